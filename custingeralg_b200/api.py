@@ -1,0 +1,111 @@
+"""Python mirror of the reference's triangle-counting entry points over the C ABI.
+
+  Graph                  the cuStinger handle subset (initializeCuStinger from a CSR)
+  count_all_triangles    callDeviceAllTriangles  (include/static_triangle_counting/cct.hpp:15-17)
+  count_all_triangles_csr callDeviceAllTrianglesCSR (tests/cct_csr.cu:279-285)
+
+Device buffers are torch CUDA tensors (plumbing only); every count runs in the native library.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import native as N
+
+
+def _stream_ptr(stream=None) -> Optional[int]:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream
+
+
+def _ptr(t) -> Optional[int]:
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+class Graph:
+    """Dynamic graph handle (tc_graph*) built from a symmetric sorted CSR."""
+
+    def __init__(self, n: int, off, ind, slack: float = 0.0, validate: bool = True, stream=None):
+        import torch
+        self._h = ctypes.c_void_p()
+        if isinstance(off, np.ndarray):
+            off = np.ascontiguousarray(off, dtype=np.int64)
+            ind = np.ascontiguousarray(ind, dtype=np.int32)
+            ind_p = ind.ctypes.data if ind.size else None
+            st = N.lib().tc_graph_create(n, off.ctypes.data, ind_p, N.TC_MEM_HOST, slack, int(validate),
+                                         _stream_ptr(stream), ctypes.byref(self._h))
+        else:
+            assert off.is_cuda and off.dtype == torch.int64 and ind.dtype == torch.int32
+            st = N.lib().tc_graph_create(n, off.data_ptr(), ind.data_ptr() if ind.numel() else None,
+                                         N.TC_MEM_DEVICE, slack, int(validate), _stream_ptr(stream),
+                                         ctypes.byref(self._h))
+        N.check(st)
+        self.n = n
+
+    @classmethod
+    def from_csr(cls, csr, **kw) -> "Graph":
+        return cls(csr.n, csr.off, csr.ind, **kw)
+
+    def close(self):
+        if self._h:
+            N.lib().tc_graph_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        nv, used, alloc = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        N.check(N.lib().tc_graph_info(self._h, ctypes.byref(nv), ctypes.byref(used), ctypes.byref(alloc)))
+        return nv.value, used.value, alloc.value
+
+    def export(self):
+        n, m, _ = self.info()
+        off = np.zeros(n + 1, np.int64)
+        ind = np.zeros(max(m, 1), np.int32)
+        N.check(N.lib().tc_graph_export(self._h, off.ctypes.data, ind.ctypes.data))
+        return off, ind[:m]
+
+    def validate(self, stream=None):
+        N.check(N.lib().tc_graph_validate(self._h, _stream_ptr(stream)))
+
+    def count(self, pv_mode: int = N.TC_PV_HANDLE, per_vertex=None, triangles_dev=None, sched=None,
+              sync: bool = True, stream=None):
+        """Static count. Returns (T, CountInfo) when sync, else None."""
+        info = N.CountInfo() if sync else None
+        st = N.lib().tc_count_static(self._h, pv_mode, _ptr(per_vertex), _ptr(triangles_dev),
+                                     ctypes.byref(info) if sync else None,
+                                     ctypes.byref(sched) if sched is not None else None, _stream_ptr(stream))
+        N.check(st)
+        return (info.triangles, info) if sync else None
+
+
+def count_all_triangles(graph: Graph, out, sched=None, stream=None):
+    """callDeviceAllTriangles: out[v] = 2 t(v) for v < nv (device int32 tensor, >= nv entries)."""
+    return graph.count(N.TC_PV_HANDLE, out, sched=sched, stream=stream)
+
+
+def count_all_triangles_csr(n: int, d_off, d_ind, out, pv_mode: int = N.TC_PV_CSR, sched=None, sync=True,
+                            stream=None, triangles_dev=None):
+    """callDeviceAllTrianglesCSR on device CSR tensors (int32 or int64 offsets)."""
+    import torch
+    info = N.CountInfo() if sync else None
+    fn = N.lib().tc_count_csr32 if d_off.dtype == torch.int32 else N.lib().tc_count_csr64
+    st = fn(n, d_off.data_ptr(), d_ind.data_ptr() if d_ind.numel() else None, pv_mode, _ptr(out),
+            _ptr(triangles_dev), ctypes.byref(info) if sync else None,
+            ctypes.byref(sched) if sched is not None else None, _stream_ptr(stream))
+    N.check(st)
+    return (info.triangles, info) if sync else None

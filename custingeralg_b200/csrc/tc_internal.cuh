@@ -1,0 +1,141 @@
+// Internal declarations shared by the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/custinger_tc.h"
+
+namespace tc {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// ---- error reporting -------------------------------------------------------------------
+
+void set_error(const char* fmt, ...);
+tc_status fail(tc_status s, const char* fmt, ...);
+
+#define TC_CUDA_TRY(call)                                                                  \
+  do {                                                                                     \
+    cudaError_t _e = (call);                                                               \
+    if (_e != cudaSuccess) {                                                               \
+      return ::tc::fail(_e == cudaErrorMemoryAllocation ? TC_ERR_OOM : TC_ERR_CUDA,        \
+                        "%s failed: %s (%s:%d)", #call, cudaGetErrorString(_e), __FILE__,  \
+                        __LINE__);                                                         \
+    }                                                                                      \
+  } while (0)
+
+#define TC_TRY(expr)                  \
+  do {                                \
+    tc_status _s = (expr);            \
+    if (_s != TC_OK) return _s;       \
+  } while (0)
+
+// ---- adjacency views -------------------------------------------------------------------
+// The orientation kernels read the input graph through one of these: a compact CSR with
+// int32 or int64 offsets (the reference's raw-CSR path) or the slack-managed handle storage
+// (per-vertex start + used length into a pool, the cuStinger layout).
+
+struct Csr32View {
+  const int32_t* off;
+  const int32_t* ind;
+  __device__ __forceinline__ int64_t start(int32_t v) const { return off[v]; }
+  __device__ __forceinline__ int32_t len(int32_t v) const { return off[v + 1] - off[v]; }
+};
+
+struct Csr64View {
+  const int64_t* off;
+  const int32_t* ind;
+  __device__ __forceinline__ int64_t start(int32_t v) const { return off[v]; }
+  __device__ __forceinline__ int32_t len(int32_t v) const { return (int32_t)(off[v + 1] - off[v]); }
+};
+
+struct SlackView {
+  const int64_t* st;
+  const int32_t* used;
+  const int32_t* ind;
+  __device__ __forceinline__ int64_t start(int32_t v) const { return st[v]; }
+  __device__ __forceinline__ int32_t len(int32_t v) const { return used[v]; }
+};
+
+// ---- device-side status of one count ---------------------------------------------------
+
+enum : unsigned { kBadRange = 1u, kBadOrder = 2u, kBadSelfLoop = 4u, kBadCapacity = 8u };
+
+struct DevStatus {
+  unsigned long long triangles;          // T
+  unsigned long long edges_intersected;  // oriented edges with deg(u) >= 2
+  unsigned long long oriented_work;      // sum over u->v of d+(u) + d+(v)
+  unsigned long long sym_checksum;       // signed edge checksum, 0 when symmetric
+  unsigned long long q_small;            // work-queue head over vertex ids
+  unsigned int bad_flags;
+  unsigned int max_dplus;
+  unsigned int n_large;                  // vertices on the block (large out-degree) queue
+  unsigned int q_large;                  // work-queue head over the large list
+};
+
+// ---- scheduler parameters as the kernels see them --------------------------------------
+
+struct SchedParams {
+  int32_t warp_max;        // <= 32
+  int32_t search_ratio_x16;
+  int32_t use_table;
+  int32_t chunk;
+  int32_t blocks_per_sm;   // 0 = occupancy limit
+  int32_t shard;           // count source vertices u with u % nshards == shard
+  int32_t nshards;
+  uint8_t table[16][16];
+};
+
+SchedParams to_params(const tc_sched* s);
+
+// ---- workspace for one static count ----------------------------------------------------
+
+struct Workspace {
+  int device = -1;
+  int64_t n_cap = 0;       // vertices
+  int64_t e_cap = 0;       // oriented edge slots
+  int64_t tiles_cap = 0;
+  int32_t* dplus = nullptr;      // [n]
+  int64_t* offp = nullptr;       // [n+1]
+  int32_t* indp = nullptr;       // [e_cap]
+  int32_t* large = nullptr;      // [n]
+  int64_t* tile_sums = nullptr;  // [tiles+1]
+  DevStatus* st = nullptr;       // [1]
+  tc_status ensure(int64_t n, int64_t m_directed);
+  void release();
+};
+
+// Device properties cached per device.
+struct DeviceInfo {
+  int sms = 148;
+  int count_blocks_per_sm = 1;
+};
+const DeviceInfo& device_info();
+
+// Static count over any view. `ws` must be sized for (n, m). Stream-ordered.
+template <class View>
+tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, int pv_mode,
+                       int32_t* per_vertex, int64_t* triangles_dev, const SchedParams& sp,
+                       cudaStream_t stream);
+
+// Structural check only (the first orientation pass). Stream-ordered; read with read_info.
+template <class View>
+tc_status validate_view(const View& view, int32_t n, Workspace& ws, cudaStream_t stream);
+
+// Phase events of the calling thread (tc_profile_enable). Each is a no-op when disabled.
+void prof_mark(int point, cudaStream_t stream);   // 0 = start, 1 = orientation done, 2 = count done
+void prof_launches(int n);
+
+// Read back a count's info (syncs the stream).
+tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* info);
+
+// Exclusive scan of int32 counts into int64 offsets: out[0..n] (out[n] = total).
+tc_status scan_counts(const int32_t* in, int64_t n, int64_t* out, int64_t* tile_sums,
+                      cudaStream_t stream);
+int64_t scan_tiles(int64_t n);
+
+}  // namespace tc

@@ -1,0 +1,752 @@
+// Static triangle count: degree orientation + vertex-grouped intersections (sm_100a).
+//
+// Replaces the reference's devicecuStingerAllTriangles (src/static_triangle_counting/cct.cu:216-270)
+// and count_all_trianglesGPU (tests/cct_csr.cu:228-276). The reference intersects the full
+// lists of every directed edge with a merge path split across 1-32 lanes and one block
+// reduction per source vertex. Here:
+//
+//  1. k_orient_count / scan / k_orient_fill build the degree orientation G+ (u -> v iff
+//     (deg u, u) < (deg v, v)) as a compact CSR whose lists stay ascending by id. Every
+//     triangle {x < y < z in that order} is found exactly once: at x, on edge x->y, as the
+//     common element z of N+(x) and N+(y). The same passes check the input (ids in range,
+//     strictly ascending lists, no self-loops, a signed edge checksum for symmetry).
+//  2. k_count runs a persistent grid over two work queues. Vertices with out-degree above
+//     the warp threshold ("large") are taken one per CTA: N+(u) is staged in shared memory
+//     as an open-addressing hash set (chunks of 2048 entries). All other vertices with
+//     d+ >= 2 are taken one per warp with a warp-private 64-slot hash set. For each group of
+//     32 out-neighbours v of u the warp streams the concatenation of their lists N+(v) with
+//     coalesced loads (segment boundaries found with one __reduce_or_sync per 32 elements)
+//     and probes every element into the hash set ("probe" strategy), or, for an edge whose
+//     N+(v) is long next to N+(u), binary-searches the elements of N+(u) into N+(v)
+//     ("search" strategy). The scheduler picks the strategy per edge.
+//  3. Per-vertex counts never take a global atomic per triangle: the three vertices of a
+//     triangle found at u are u, v = A[i] and w = A[j], both slots of the staged list A, so
+//     they accumulate in shared-memory counters and flush with at most one global atomic per
+//     oriented edge. The triangle total takes one global atomic per CTA.
+#include <algorithm>
+#include <cstring>
+
+#include "tc_internal.cuh"
+
+namespace tc {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / kWarp;
+constexpr int kChunk = 2048;      // A entries staged per pass for a large vertex
+constexpr int kHashMax = 4096;    // hash slots for a chunk (load <= 0.5)
+constexpr int kSmallSlots = 64;   // warp-private hash slots (warp_max <= 32)
+constexpr int kScanThreads = 256;
+constexpr int kScanPer = 8;
+constexpr int kScanTile = kScanThreads * kScanPer;
+
+struct WarpSmem {
+  int32_t hkeys[kSmallSlots];
+  int32_t sA[kWarp];
+  uint32_t cnt[kWarp];
+  int64_t seg_base[kWarp];
+  int32_t seg_v[kWarp];
+  uint32_t seg_cnt[kWarp];
+  int8_t hidx[kSmallSlots];
+};
+
+struct CountSmem {
+  int32_t hkeys[kHashMax];
+  int32_t sA[kChunk];
+  uint32_t cnt[kChunk];
+  int16_t hidx[kHashMax];
+  WarpSmem warp[kWarps];
+  unsigned long long tri[kWarps];
+  unsigned item;
+  int gctr;
+};
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned r;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(r));
+  return r;
+}
+
+__device__ __forceinline__ uint64_t sym_hash(uint32_t x, uint32_t y) {
+  uint64_t z = ((uint64_t)x << 32) | y;
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+__device__ __forceinline__ uint32_t hash_slot(int32_t key, int bits) {
+  return ((uint32_t)key * 0x9E3779B1u) >> (32 - bits);
+}
+
+// Insert key (unique) with payload idx; the table has 2^bits slots and load <= 0.5, so an
+// empty slot is always found within 2^bits steps.
+template <typename IdxT>
+__device__ __forceinline__ void hash_insert(int32_t* keys, IdxT* idx, int bits, int32_t key, int j) {
+  const uint32_t mask = (1u << bits) - 1;
+  uint32_t s = hash_slot(key, bits);
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const int32_t prev = atomicCAS(&keys[s], -1, key);
+    if (prev == -1) {
+      idx[s] = (IdxT)j;
+      return;
+    }
+    if (prev == key) return;
+    s = (s + 1) & mask;
+  }
+}
+
+// Slot holding key, or -1.
+__device__ __forceinline__ int hash_find(const int32_t* keys, int bits, int32_t key) {
+  const uint32_t mask = (1u << bits) - 1;
+  uint32_t s = hash_slot(key, bits);
+  for (uint32_t it = 0; it <= mask; ++it) {
+    const int32_t k = keys[s];
+    if (k == key) return (int)s;
+    if (k == -1) return -1;
+    s = (s + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ bool search_sorted(const int32_t* __restrict__ list, int len, int32_t key) {
+  int lo = 0, hi = len;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(list + mid) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo < len && __ldg(list + lo) == key;
+}
+
+__device__ __forceinline__ int log2_cell(int x) {
+  const int c = 31 - __clz(max(x, 1));
+  return min(c, 15);
+}
+
+__device__ __forceinline__ bool use_search(const SchedParams& sp, int a, int b) {
+  if (sp.use_table) return sp.table[log2_cell(a)][log2_cell(b)] == 1;
+  const int lg = 32 - __clz(b);
+  return 16LL * b > (long long)sp.search_ratio_x16 * a * lg;
+}
+
+// Weights a found triangle (u, v, w) adds to each vertex's per-vertex output.
+// TC_PV_HANDLE: 1 each (doubled at flush: out = 2 t(v)).
+// TC_PV_CSR: the reference's raw-CSR kernel counts a triangle at every edge (x, y) with
+// y > x whose lists share the third vertex, crediting x: the smallest id gets 2, the middle 1.
+template <int PV>
+__device__ __forceinline__ void tri_weights(int32_t u, int32_t v, int32_t w, uint32_t& wu, uint32_t& wv,
+                                            uint32_t& ww) {
+  if (PV == TC_PV_CSR) {
+    wu = (u < v) + (u < w);
+    wv = (v < u) + (v < w);
+    ww = (w < u) + (w < v);
+  } else {
+    wu = wv = ww = 1u;
+  }
+}
+
+template <int PV>
+constexpr uint32_t flush_mult() {
+  return PV == TC_PV_HANDLE ? 2u : 1u;
+}
+
+// One warp intersects N+(u) with N+(v) for the out-neighbours v = A[g0 .. g0+gcount) of u.
+// The current chunk of A (entries [chunk_base, chunk_base+chunk_len)) is in shared memory as
+// sA and as a hash set; cnt[] holds the chunk's per-slot counters.
+template <int PV, typename IdxT>
+__device__ __forceinline__ void process_group(
+    const int32_t u, const int32_t* __restrict__ Ag, const int32_t* sA, const int chunk_base,
+    const int chunk_len, const int32_t* hkeys, const IdxT* hidx, const int bits, uint32_t* cnt,
+    const int g0, const int gcount, const int32_t* __restrict__ dplus,
+    const int64_t* __restrict__ offp, const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
+    WarpSmem& ws, const SchedParams& sp, uint32_t& tri, uint32_t& u_acc) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const bool valid = lane < gcount;
+  const int i = g0 + lane;
+  const int li = i - chunk_base;
+  const bool in_chunk = li >= 0 && li < chunk_len;
+  const int32_t v = valid ? (in_chunk ? sA[li] : __ldg(Ag + i)) : 0;
+  const int b = valid ? __ldg(dplus + v) : 0;
+  const int64_t base = valid ? __ldg(offp + v) : 0;
+  const bool srch = valid && b > 0 && use_search(sp, chunk_len, b);
+  const int pb = (valid && !srch) ? b : 0;
+
+  // ---- probe strategy: stream the concatenated lists N+(v), probe into the hash set ----
+  int incl = pb;
+#pragma unroll
+  for (int o = 1; o < kWarp; o <<= 1) {
+    const int t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const int P = incl - pb;
+  const int total = __shfl_sync(kFull, incl, kWarp - 1);
+  const unsigned lt = lanemask_lt();
+  const unsigned segmask = __ballot_sync(kFull, pb > 0);
+  const int rank = __popc(segmask & lt);
+  if (pb > 0) {
+    ws.seg_base[rank] = base - P;
+    ws.seg_v[rank] = v;
+    ws.seg_cnt[rank] = 0;
+  }
+  __syncwarp();
+  int carry = 0;
+  for (int k0 = 0; k0 < total; k0 += kWarp) {
+    const unsigned bit = (pb > 0 && P >= k0 && P < k0 + kWarp) ? (1u << (P - k0)) : 0u;
+    const unsigned starts = __reduce_or_sync(kFull, bit);
+    const int r = carry + __popc(starts & (lt | (1u << lane))) - 1;
+    carry += __popc(starts);
+    const int k = k0 + lane;
+    if (k < total) {
+      const int32_t w = __ldg(indp + ws.seg_base[r] + k);
+      const int s = hash_find(hkeys, bits, w);
+      if (s >= 0) {
+        ++tri;
+        if (PV != TC_PV_NONE) {
+          uint32_t wu, wv, ww;
+          tri_weights<PV>(u, ws.seg_v[r], w, wu, wv, ww);
+          u_acc += wu;
+          if (ww) atomicAdd(&cnt[hidx[s]], ww);
+          if (wv) atomicAdd(&ws.seg_cnt[r], wv);
+        }
+      }
+    }
+  }
+
+  // ---- search strategy: binary-search the chunk's entries into N+(v) ----
+  unsigned sm = __ballot_sync(kFull, srch);
+  while (sm) {
+    const int sl = __ffs(sm) - 1;
+    sm &= sm - 1;
+    const int32_t sv = __shfl_sync(kFull, v, sl);
+    const int sb = __shfl_sync(kFull, b, sl);
+    const int64_t sbase = __shfl_sync(kFull, base, sl);
+    const int sli = __shfl_sync(kFull, li, sl);
+    uint32_t vacc = 0;
+    for (int j = lane; j < chunk_len; j += kWarp) {
+      const int32_t w = sA[j];
+      if (search_sorted(indp + sbase, sb, w)) {
+        ++tri;
+        if (PV != TC_PV_NONE) {
+          uint32_t wu, wv, ww;
+          tri_weights<PV>(u, sv, w, wu, wv, ww);
+          u_acc += wu;
+          vacc += wv;
+          if (ww) atomicAdd(&cnt[j], ww);
+        }
+      }
+    }
+    if (PV != TC_PV_NONE) {
+      vacc = warp_sum(vacc);
+      if (lane == 0 && vacc) {
+        if (sli >= 0 && sli < chunk_len) atomicAdd(&cnt[sli], vacc);
+        else atomicAdd(&out[sv], vacc * flush_mult<PV>());
+      }
+    }
+  }
+  __syncwarp();
+  // v-role counts of the probed edges: into the chunk counters when v is staged, else global.
+  if (PV != TC_PV_NONE && pb > 0) {
+    const uint32_t c = ws.seg_cnt[rank];
+    if (c) {
+      if (in_chunk) atomicAdd(&cnt[li], c);
+      else atomicAdd(&out[v], c * flush_mult<PV>());
+    }
+  }
+  __syncwarp();
+}
+
+template <int PV>
+__global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32_t* __restrict__ dplus,
+                                                    const int64_t* __restrict__ offp,
+                                                    const int32_t* __restrict__ indp,
+                                                    const int32_t* __restrict__ large,
+                                                    uint32_t* __restrict__ out, DevStatus* __restrict__ st,
+                                                    const SchedParams sp) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CountSmem& sm = *reinterpret_cast<CountSmem*>(smem_raw);
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int wid = threadIdx.x / kWarp;
+  uint32_t tri = 0;
+  const unsigned n_large = st->n_large;
+
+  // Phase 1: large out-degree vertices, one CTA each, in chunks of kChunk staged entries.
+  while (true) {
+    if (threadIdx.x == 0) sm.item = atomicAdd(&st->q_large, 1u);
+    __syncthreads();
+    const unsigned item = sm.item;
+    __syncthreads();
+    if (item >= n_large) break;
+    const int32_t u = large[item];
+    const int32_t a = dplus[u];
+    const int32_t* Ag = indp + offp[u];
+    uint32_t u_acc = 0;
+    for (int cb = 0; cb < a; cb += kChunk) {
+      const int clen = min(kChunk, a - cb);
+      int bits = 6;
+      while ((1 << bits) < 2 * clen) ++bits;
+      const int S = 1 << bits;
+      for (int s = threadIdx.x; s < S; s += kThreads) sm.hkeys[s] = -1;
+      for (int j = threadIdx.x; j < clen; j += kThreads) {
+        sm.sA[j] = __ldg(Ag + cb + j);
+        sm.cnt[j] = 0;
+      }
+      if (threadIdx.x == 0) sm.gctr = 0;
+      __syncthreads();
+      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(sm.hkeys, sm.hidx, bits, sm.sA[j], j);
+      __syncthreads();
+      const int ngroups = (a + kWarp - 1) / kWarp;
+      while (true) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(&sm.gctr, 1);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= ngroups) break;
+        process_group<PV>(u, Ag, sm.sA, cb, clen, sm.hkeys, sm.hidx, bits, sm.cnt, g * kWarp,
+                          min(kWarp, a - g * kWarp), dplus, offp, indp, out, sm.warp[wid], sp, tri, u_acc);
+      }
+      __syncthreads();
+      if (PV != TC_PV_NONE) {
+        for (int j = threadIdx.x; j < clen; j += kThreads) {
+          const uint32_t c = sm.cnt[j];
+          if (c) atomicAdd(&out[sm.sA[j]], c * flush_mult<PV>());
+        }
+      }
+      __syncthreads();
+    }
+    if (PV != TC_PV_NONE) {
+      u_acc = warp_sum(u_acc);
+      if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
+    }
+  }
+
+  // Phase 2: vertices with 2 <= d+ <= warp_max, one warp each, claimed in chunks.
+  WarpSmem& ws = sm.warp[wid];
+  while (true) {
+    unsigned long long c0 = 0;
+    if (lane == 0) c0 = atomicAdd(&st->q_small, (unsigned long long)sp.chunk);
+    c0 = __shfl_sync(kFull, c0, 0);
+    if (c0 >= (unsigned long long)n) break;
+    const int32_t cend = (int32_t)min((unsigned long long)n, c0 + (unsigned long long)sp.chunk);
+    for (int32_t ub = (int32_t)c0; ub < cend; ub += kWarp) {
+      const int32_t uu = ub + lane;
+      const int aa = (uu < cend) ? __ldg(dplus + uu) : 0;
+      unsigned elig = __ballot_sync(kFull, aa >= 2 && aa <= sp.warp_max && (uu % sp.nshards) == sp.shard);
+      while (elig) {
+        const int sl = __ffs(elig) - 1;
+        elig &= elig - 1;
+        const int32_t u = ub + sl;
+        const int a = __shfl_sync(kFull, aa, sl);
+        const int32_t* Ag = indp + __ldg(offp + u);
+        ws.hkeys[lane] = -1;
+        ws.hkeys[lane + kWarp] = -1;
+        ws.cnt[lane] = 0;
+        int32_t x = 0;
+        if (lane < a) {
+          x = __ldg(Ag + lane);
+          ws.sA[lane] = x;
+        }
+        __syncwarp();
+        if (lane < a) hash_insert(ws.hkeys, ws.hidx, 6, x, lane);
+        __syncwarp();
+        uint32_t u_acc = 0;
+        process_group<PV>(u, Ag, ws.sA, 0, a, ws.hkeys, ws.hidx, 6, ws.cnt, 0, a, dplus, offp, indp, out,
+                          ws, sp, tri, u_acc);
+        if (PV != TC_PV_NONE) {
+          if (lane < a) {
+            const uint32_t c = ws.cnt[lane];
+            if (c) atomicAdd(&out[x], c * flush_mult<PV>());
+          }
+          u_acc = warp_sum(u_acc);
+          if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
+        }
+        __syncwarp();
+      }
+    }
+  }
+
+  // One global atomic per CTA for the triangle total.
+  unsigned long long t = warp_sum((unsigned long long)tri);
+  if (lane == 0) sm.tri[wid] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int w = 0; w < kWarps; ++w) s += sm.tri[w];
+    if (s) atomicAdd(&st->triangles, s);
+  }
+}
+
+// ---- orientation ------------------------------------------------------------------------
+
+__device__ __forceinline__ bool precedes(int32_t du, int32_t u, int32_t dv, int32_t v) {
+  return du < dv || (du == dv && u < v);
+}
+
+template <class View>
+__global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_t n, int32_t* __restrict__ dplus,
+                                                      DevStatus* __restrict__ st) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+  unsigned long long chk = 0, ei = 0;
+  unsigned bad = 0, mx = 0;
+  for (int64_t uu = gw; uu < n; uu += nw) {
+    const int32_t u = (int32_t)uu;
+    const int64_t s = g.start(u);
+    const int32_t d = g.len(u);
+    int cnt = 0;
+    int32_t last = INT32_MIN;
+    for (int32_t k0 = 0; k0 < d; k0 += kWarp) {
+      const int32_t k = k0 + lane;
+      const bool in = k < d;
+      const int32_t v = in ? g.ind[s + k] : INT32_MAX;
+      int32_t prev = __shfl_up_sync(kFull, v, 1);
+      if (lane == 0) prev = last;
+      last = __shfl_sync(kFull, v, kWarp - 1);
+      bool pred = false;
+      if (in) {
+        if (v < 0 || v >= n) {
+          bad |= kBadRange;
+        } else {
+          if (k > 0 && prev >= v) bad |= kBadOrder;
+          if (v == u) bad |= kBadSelfLoop;
+          const int32_t dv = g.len(v);
+          pred = precedes(d, u, dv, v);
+          const uint64_t h = (u < v) ? sym_hash((uint32_t)u, (uint32_t)v) : sym_hash((uint32_t)v, (uint32_t)u);
+          chk += (u < v) ? h : (0ull - h);
+        }
+      }
+      cnt += __popc(__ballot_sync(kFull, pred));
+    }
+    if (lane == 0) {
+      dplus[u] = cnt;
+      if (d >= 2) ei += (unsigned long long)cnt;
+      mx = max(mx, (unsigned)cnt);
+    }
+  }
+  chk = warp_sum(chk);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  if (lane == 0) {
+    if (chk) atomicAdd(&st->sym_checksum, chk);
+    if (bad) atomicOr(&st->bad_flags, bad);
+    if (ei) atomicAdd(&st->edges_intersected, ei);
+    if (mx) atomicMax(&st->max_dplus, mx);
+  }
+}
+
+template <class View>
+__global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t n, const int32_t* __restrict__ dplus,
+                                                     const int64_t* __restrict__ offp, int32_t* __restrict__ indp,
+                                                     const int64_t e_cap, int32_t* __restrict__ large,
+                                                     DevStatus* __restrict__ st, const int warp_max,
+                                                     const int shard, const int nshards) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+  const unsigned lt = lanemask_lt();
+  unsigned long long work = 0;
+  int nbuf = 0;
+  int32_t buf = 0;
+  unsigned bad = 0;
+  for (int64_t uu = gw; uu < n; uu += nw) {
+    const int32_t u = (int32_t)uu;
+    const int64_t s = g.start(u);
+    const int32_t d = g.len(u);
+    const int64_t base = offp[u];
+    const int32_t a = dplus[u];
+    if (base + a > e_cap) {
+      bad |= kBadCapacity;
+      continue;
+    }
+    int pos = 0;
+    unsigned long long ws = 0;
+    for (int32_t k0 = 0; k0 < d; k0 += kWarp) {
+      const int32_t k = k0 + lane;
+      bool pred = false;
+      int32_t v = 0;
+      if (k < d) {
+        v = g.ind[s + k];
+        if (v >= 0 && v < n) pred = precedes(d, u, g.len(v), v);
+      }
+      const unsigned msk = __ballot_sync(kFull, pred);
+      const int at = pos + __popc(msk & lt);
+      if (pred && at < a) {
+        indp[base + at] = v;
+        ws += (unsigned long long)__ldg(dplus + v);
+      }
+      pos += __popc(msk);
+    }
+    ws = warp_sum(ws);
+    if (lane == 0) work += ws + (unsigned long long)a * (unsigned long long)a;
+    if (a > warp_max && (u % nshards) == shard) {
+      if (lane == nbuf) buf = u;
+      if (++nbuf == kWarp) {
+        unsigned at = 0;
+        if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)kWarp);
+        at = __shfl_sync(kFull, at, 0);
+        large[at + lane] = buf;
+        nbuf = 0;
+      }
+    }
+  }
+  if (nbuf) {
+    unsigned at = 0;
+    if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)nbuf);
+    at = __shfl_sync(kFull, at, 0);
+    if (lane < nbuf) large[at + lane] = buf;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  if (lane == 0) {
+    if (work) atomicAdd(&st->oriented_work, work);
+    if (bad) atomicOr(&st->bad_flags, bad);
+  }
+}
+
+// ---- exclusive scan of int32 counts into int64 offsets ------------------------------------
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const int32_t* __restrict__ in, const int64_t n,
+                                                                 int64_t* __restrict__ tile_sums) {
+  __shared__ long long red[kScanThreads / kWarp];
+  const int64_t base = (int64_t)blockIdx.x * kScanTile;
+  long long s = 0;
+  for (int k = 0; k < kScanPer; ++k) {
+    const int64_t i = base + (int64_t)k * kScanThreads + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x / kWarp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long t = 0;
+    for (int w = 0; w < kScanThreads / kWarp; ++w) t += red[w];
+    tile_sums[blockIdx.x] = t;
+  }
+}
+
+// Single CTA: exclusive scan of tile_sums[0..ntiles) in place, total into tile_sums[ntiles].
+__global__ void __launch_bounds__(1024) k_scan_tile_prefix(int64_t* __restrict__ tile_sums, const int64_t ntiles) {
+  __shared__ long long wsum[32];
+  __shared__ long long carry_s;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  for (int64_t b0 = 0; b0 < ntiles; b0 += 1024) {
+    const int64_t i = b0 + threadIdx.x;
+    const long long x = (i < ntiles) ? tile_sums[i] : 0;
+    long long incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      long long w = wsum[lane];
+      long long wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long t = __shfl_up_sync(kFull, wi, o);
+        if (lane >= o) wi += t;
+      }
+      wsum[lane] = wi - w;
+    }
+    __syncthreads();
+    const long long c = carry_s;
+    if (i < ntiles) tile_sums[i] = c + wsum[wid] + incl - x;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry_s = c + wsum[wid] + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) tile_sums[ntiles] = carry_s;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int32_t* __restrict__ in, const int64_t n,
+                                                             const int64_t* __restrict__ tile_sums,
+                                                             int64_t* __restrict__ out, const int64_t ntiles) {
+  __shared__ long long wsum[kScanThreads / kWarp];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
+  const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
+  long long v[kScanPer];
+  long long s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int64_t i = base + k;
+    v[k] = (i < n) ? in[i] : 0;
+    s += v[k];
+  }
+  long long incl = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  if (lane == 31) wsum[wid] = incl;
+  __syncthreads();
+  long long wpre = 0;
+  for (int w = 0; w < wid; ++w) wpre += wsum[w];
+  long long run = tile_sums[blockIdx.x] + wpre + incl - s;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    const int64_t i = base + k;
+    if (i < n) out[i] = run;
+    run += v[k];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_sums[ntiles];
+}
+
+int orient_grid(int64_t n) {
+  const int64_t want = (n + kWarps - 1) / kWarps;
+  const int64_t cap = (int64_t)device_info().sms * 16;
+  return (int)std::max<int64_t>(1, std::min(want, cap));
+}
+
+template <int PV>
+tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const SchedParams& sp,
+                       cudaStream_t stream) {
+  constexpr int kMaxDev = 64;
+  static int blocks_per_sm[kMaxDev] = {};  // 0 = not configured on that device yet
+  const size_t smem = sizeof(CountSmem);
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  if (blocks_per_sm[dev] == 0) {
+    TC_CUDA_TRY(cudaFuncSetAttribute(k_count<PV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int b = 0;
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_count<PV>, kThreads, smem));
+    blocks_per_sm[dev] = std::max(1, b);
+  }
+  const int bps = sp.blocks_per_sm > 0 ? std::min(sp.blocks_per_sm, blocks_per_sm[dev]) : blocks_per_sm[dev];
+  const int grid = device_info().sms * bps;
+  k_count<PV><<<grid, kThreads, smem, stream>>>(n, ws.dplus, ws.offp, ws.indp, ws.large, out, ws.st, sp);
+  TC_CUDA_TRY(cudaGetLastError());
+  return TC_OK;
+}
+
+}  // namespace
+
+int64_t scan_tiles(int64_t n) { return (n + kScanTile - 1) / kScanTile; }
+
+tc_status scan_counts(const int32_t* in, int64_t n, int64_t* out, int64_t* tile_sums, cudaStream_t stream) {
+  const int64_t nt = scan_tiles(n);
+  if (nt == 0) {
+    TC_CUDA_TRY(cudaMemsetAsync(out, 0, sizeof(int64_t), stream));
+    return TC_OK;
+  }
+  k_scan_tile_sums<<<(unsigned)nt, kScanThreads, 0, stream>>>(in, n, tile_sums);
+  k_scan_tile_prefix<<<1, 1024, 0, stream>>>(tile_sums, nt);
+  k_scan_tiles<<<(unsigned)nt, kScanThreads, 0, stream>>>(in, n, tile_sums, out, nt);
+  TC_CUDA_TRY(cudaGetLastError());
+  return TC_OK;
+}
+
+SchedParams to_params(const tc_sched* s) {
+  tc_sched d;
+  if (!s) {
+    tc_sched_default(&d);
+    s = &d;
+  }
+  SchedParams p;
+  p.warp_max = std::min(32, std::max(2, s->warp_max_deg));
+  p.search_ratio_x16 = std::max(0, s->search_ratio_x16);
+  p.use_table = s->use_table ? 1 : 0;
+  p.chunk = std::max(32, (s->chunk + 31) / 32 * 32);
+  p.blocks_per_sm = std::max(0, s->blocks_per_sm);
+  p.nshards = std::max(1, s->nshards);
+  p.shard = std::min(std::max(0, s->shard), p.nshards - 1);
+  memcpy(p.table, s->table, sizeof(p.table));
+  return p;
+}
+
+template <class View>
+tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, int pv_mode, int32_t* per_vertex,
+                       int64_t* triangles_dev, const SchedParams& sp, cudaStream_t stream) {
+  TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
+  if (pv_mode != TC_PV_NONE && n > 0)
+    TC_CUDA_TRY(cudaMemsetAsync(per_vertex, 0, sizeof(int32_t) * (size_t)n, stream));
+  if (n > 0) {
+    prof_mark(0, stream);
+    const int grid = orient_grid(n);
+    k_orient_count<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.st);
+    TC_CUDA_TRY(cudaGetLastError());
+    TC_TRY(scan_counts(ws.dplus, n, ws.offp, ws.tile_sums, stream));
+    k_orient_fill<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.st,
+                                                  sp.warp_max, sp.shard, sp.nshards);
+    TC_CUDA_TRY(cudaGetLastError());
+    prof_mark(1, stream);
+    uint32_t* out = reinterpret_cast<uint32_t*>(per_vertex);
+    switch (pv_mode) {
+      case TC_PV_NONE: TC_TRY(launch_count<TC_PV_NONE>(n, ws, out, sp, stream)); break;
+      case TC_PV_HANDLE: TC_TRY(launch_count<TC_PV_HANDLE>(n, ws, out, sp, stream)); break;
+      case TC_PV_CSR: TC_TRY(launch_count<TC_PV_CSR>(n, ws, out, sp, stream)); break;
+      default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
+    }
+    prof_mark(2, stream);
+    prof_launches(scan_tiles(n) > 0 ? 6 : 3);
+  }
+  (void)m;
+  if (triangles_dev)
+    TC_CUDA_TRY(cudaMemcpyAsync(triangles_dev, &ws.st->triangles, sizeof(int64_t), cudaMemcpyDeviceToDevice, stream));
+  return TC_OK;
+}
+
+template tc_status static_count<Csr32View>(const Csr32View&, int32_t, int64_t, Workspace&, int, int32_t*, int64_t*,
+                                           const SchedParams&, cudaStream_t);
+template tc_status static_count<Csr64View>(const Csr64View&, int32_t, int64_t, Workspace&, int, int32_t*, int64_t*,
+                                           const SchedParams&, cudaStream_t);
+template tc_status static_count<SlackView>(const SlackView&, int32_t, int64_t, Workspace&, int, int32_t*, int64_t*,
+                                           const SchedParams&, cudaStream_t);
+
+tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* info) {
+  DevStatus h;
+  TC_CUDA_TRY(cudaMemcpyAsync(&h, ws.st, sizeof(DevStatus), cudaMemcpyDeviceToHost, stream));
+  TC_CUDA_TRY(cudaStreamSynchronize(stream));
+  info->triangles = (int64_t)h.triangles;
+  info->edges_intersected = (int64_t)h.edges_intersected;
+  info->oriented_work = (int64_t)h.oriented_work;
+  info->max_out_degree = (int32_t)h.max_dplus;
+  if (h.bad_flags & (kBadRange | kBadOrder | kBadSelfLoop)) {
+    info->status = TC_ERR_BAD_GRAPH;
+    return fail(TC_ERR_BAD_GRAPH, "graph check failed:%s%s%s", (h.bad_flags & kBadRange) ? " id out of range" : "",
+                (h.bad_flags & kBadOrder) ? " list not strictly ascending" : "",
+                (h.bad_flags & kBadSelfLoop) ? " self-loop" : "");
+  }
+  if (h.bad_flags & kBadCapacity) {
+    info->status = TC_ERR_CAPACITY;
+    return fail(TC_ERR_CAPACITY, "oriented graph exceeded its workspace");
+  }
+  if (h.sym_checksum != 0) {
+    info->status = TC_ERR_NOT_SYMMETRIC;
+    return fail(TC_ERR_NOT_SYMMETRIC, "adjacency is not symmetric");
+  }
+  info->status = TC_OK;
+  return TC_OK;
+}
+
+}  // namespace tc
+
+namespace tc {
+
+template <class View>
+tc_status validate_view(const View& view, int32_t n, Workspace& ws, cudaStream_t stream) {
+  TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
+  if (n > 0) {
+    k_orient_count<View><<<orient_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.st);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  return TC_OK;
+}
+
+template tc_status validate_view<SlackView>(const SlackView&, int32_t, Workspace&, cudaStream_t);
+template tc_status validate_view<Csr64View>(const Csr64View&, int32_t, Workspace&, cudaStream_t);
+
+}  // namespace tc

@@ -1,0 +1,149 @@
+/* custinger_tc.h - C ABI of the B200 triangle-counting library (libcustinger_tc.so).
+ *
+ * This is the boundary below the reference's host entry points:
+ *   callDeviceAllTriangles     (include/static_triangle_counting/cct.hpp:15-17,
+ *                               src/static_triangle_counting/cct.cu:272-277)
+ *   callDeviceAllTrianglesCSR  (tests/cct_csr.cu:279-285, declared tests/cct.cpp:25-28)
+ *   callDeviceNewTriangles     (src/streaming_triangle_counting/cct_upd.cu:412-440)
+ * and the cuStinger graph handle they take (externals/cuStinger, absent from the reference
+ * tree; its use is at tests/cct.cpp:261-277 and tests/cct_upd.cpp:227-244,391-398).
+ * The C++ drop-in layer (cuStinger.hpp, static_triangle_counting/cct.hpp,
+ * streaming_triangle_counting/cct_upd.hpp) is a thin wrapper over these functions.
+ *
+ * Plain pointers and sizes only. `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream, like the reference's launches). Every function returns a tc_status;
+ * tc_last_error() gives a message for the last failure on the calling thread.
+ *
+ * Graph requirements (checked): ids in [0, nv), every adjacency list strictly ascending
+ * (sorted, no duplicates), no self-loops, symmetric (u in N(v) iff v in N(u)). These are the
+ * graphs the reference's readers produce. Asymmetry is detected with a 64-bit signed edge
+ * checksum (an asymmetric graph passes with probability about 2^-64).
+ *
+ * Count conventions (bit-exact against the reference):
+ *   TC_PV_HANDLE  per-vertex out[v] = 2 t(v) (int32, wraps mod 2^32), what
+ *                 devicecuStingerAllTriangles writes (cct.cu:216-270); sum = 6T.
+ *   TC_PV_CSR     per-vertex out[v] = sum over w in N(v), w > v of |N(v) ∩ N(w)|, what
+ *                 count_all_trianglesGPU writes (tests/cct_csr.cu:228-276); sum = 3T.
+ *   `triangles`   outputs are T, the number of triangles (int64). The reference's CPU
+ *                 counter hostCountTriangles reports 6T (tests/cct.cpp:71-89).
+ */
+#ifndef CUSTINGER_TC_H_
+#define CUSTINGER_TC_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int tc_status;
+enum {
+  TC_OK = 0,
+  TC_ERR_INVALID_ARG = 1,   /* bad pointer, size or option */
+  TC_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  TC_ERR_OOM = 3,           /* device allocation failed */
+  TC_ERR_BAD_GRAPH = 4,     /* unsorted/duplicate list, self-loop or id out of range */
+  TC_ERR_NOT_SYMMETRIC = 5, /* adjacency is not symmetric */
+  TC_ERR_CAPACITY = 6,      /* input larger than a fixed capacity (captured plans, no-alloc paths) */
+  TC_ERR_TIMEOUT = 7,       /* a bounded device-side wait gave up */
+  TC_ERR_STATE = 8          /* call out of order (e.g. counting a batch that was not applied) */
+};
+
+/* Per-vertex output conventions. */
+enum { TC_PV_NONE = 0, TC_PV_HANDLE = 1, TC_PV_CSR = 2 };
+
+/* Memory space of caller pointers. */
+enum { TC_MEM_DEVICE = 0, TC_MEM_HOST = 1 };
+
+/* Scheduler: which intersection strategy each oriented edge uses and the launch shapes.
+ * tc_sched_default() fills the fixed degree-threshold heuristic. */
+typedef struct tc_sched {
+  int32_t warp_max_deg;   /* out-degree up to which a vertex is counted by one warp (<= 32) */
+  int32_t search_ratio_x16; /* edge (u,v) uses binary search of N+(u) into N+(v) when
+                               16*d+(v) > search_ratio_x16 * d+(u) * (log2 d+(v) + 1) */
+  int32_t blocks_per_sm;  /* persistent grid = SMs x blocks_per_sm (0 = occupancy limit) */
+  int32_t chunk;          /* vertices a warp claims per work-queue grab */
+  int32_t use_table;      /* 1 = per-(log d+u, log d+v) strategy table below overrides the ratio */
+  uint8_t table[16][16];  /* strategy per degree-cell: 0 = hash probe, 1 = binary search */
+  int32_t shard;          /* count only triangles whose lowest vertex u has u % nshards == shard */
+  int32_t nshards;        /* (multi-GPU work split; 1 = everything) */
+} tc_sched;
+
+typedef struct tc_graph tc_graph;
+
+const char* tc_last_error(void);
+const char* tc_status_string(tc_status s);
+void tc_sched_default(tc_sched* s);
+
+/* Build a graph from a CSR (off: nv+1 int64 offsets, ind: off[nv] int32 ids) in host or
+ * device memory. The graph owns a copy in slack-managed device storage: each adjacency list
+ * gets capacity for ceil(slack * degree) extra entries (rounded to 16 bytes) for streaming
+ * insertions. With validate=1 the graph is checked (requirements above); the call then
+ * synchronises `stream`. Replaces initializeCuStinger with eInitStateCSR. */
+tc_status tc_graph_create(int32_t nv, const int64_t* off, const int32_t* ind, int mem, double slack,
+                          int validate, void* stream, tc_graph** out);
+tc_status tc_graph_destroy(tc_graph* g);
+/* nv, directed edges in use, directed edge slots allocated. */
+tc_status tc_graph_info(const tc_graph* g, int32_t* nv, int64_t* edges_used, int64_t* edges_alloc);
+/* Copy the graph back as a compact CSR into host arrays (off: nv+1, ind: edges_used). Syncs. */
+tc_status tc_graph_export(tc_graph* g, int64_t* off_host, int32_t* ind_host);
+/* Full structural check (sorted, no duplicates, no self-loops, ids in range, symmetric). Syncs. */
+tc_status tc_graph_validate(tc_graph* g, void* stream);
+/* Device pointers of the live structure: per-vertex list start (int64[nv]), used length
+ * (int32[nv]) and the adjacency pool. Valid until the next structural update. */
+tc_status tc_graph_device_view(tc_graph* g, const int64_t** start, const int32_t** used, const int32_t** pool);
+
+/* What a count measured, read back to the host on request. */
+typedef struct tc_count_info {
+  int64_t triangles;         /* T */
+  int64_t edges_intersected; /* undirected edges {u,v} with deg(u), deg(v) >= 2 */
+  int64_t oriented_work;     /* sum over oriented edges u->v of d+(u) + d+(v) (list elements a
+                                merge-based intersection reads) */
+  int32_t max_out_degree;    /* max d+ in the degree orientation */
+  int32_t status;            /* structural check made during the count: TC_OK,
+                                TC_ERR_BAD_GRAPH or TC_ERR_NOT_SYMMETRIC */
+} tc_count_info;
+
+/* Static count over a graph handle.
+ *   pv_mode:       TC_PV_NONE, TC_PV_HANDLE or TC_PV_CSR
+ *   per_vertex:    device int32[nv] (required unless TC_PV_NONE), entries [0, nv) overwritten
+ *   triangles_dev: optional device int64 receiving T (stream-ordered, no sync)
+ *   info:          optional host struct; when given the call synchronises `stream` and returns
+ *                  the structural status found during the count as its own status
+ *   sched:         NULL = default heuristic
+ * Stream-ordered and allocation-free after the first call on a graph of this size, so it can
+ * be captured in a CUDA graph once warmed up (with info == NULL). */
+tc_status tc_count_static(tc_graph* g, int pv_mode, int32_t* per_vertex, int64_t* triangles_dev,
+                          tc_count_info* info, const tc_sched* sched, void* stream);
+
+/* Stateless static count on a caller CSR in device memory (int32 offsets: the raw-CSR path
+ * of the reference; int64 offsets for graphs past 2^31 edges). The structural checks run on
+ * the fly; their result is in info->status (or in tc_workspace_status() when info == NULL).
+ * Uses a per-device workspace owned by the library (grown on demand, freed at exit); calls
+ * on one device must not overlap. */
+tc_status tc_count_csr32(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode,
+                         int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
+                         const tc_sched* sched, void* stream);
+tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind, int pv_mode,
+                         int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
+                         const tc_sched* sched, void* stream);
+
+/* Read back the info of the last stateless count on the current device. Syncs `stream`. */
+tc_status tc_workspace_status(void* stream, tc_count_info* info);
+
+/* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching
+ * stream around the orientation passes and around the intersection kernel (off by default;
+ * recording adds no synchronisation). */
+typedef struct tc_phase_times {
+  float orient_ms;   /* orientation: out-degree pass, scan, fill */
+  float count_ms;    /* the intersection kernel (k_count) */
+  int32_t launches;  /* kernels the last count launched */
+} tc_phase_times;
+tc_status tc_profile_enable(int on);
+/* Times of the last profiled count on this thread; waits for its events. */
+tc_status tc_profile_last(tc_phase_times* t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUSTINGER_TC_H_ */
