@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-streaming", action="store_true")
+    ap.add_argument("--stream-scale", type=int, default=22)
+    ap.add_argument("--stream-batches", type=int, default=200)
+    ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
     return ap.parse_args()
 
 
@@ -359,10 +363,94 @@ def run_ours(a, rank, world, local_rank):
                          "path": "tc_count_csr64 (callDeviceAllTrianglesCSR boundary), pinned host CSR in, "
                                  "per-vertex counts out"}
 
+    if rank == 0 and world == 1 and not a.no_streaming:
+        result["streaming"] = run_streaming(a, dev)
+
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         v, nt, desc, kind, _, _ = cpu_reference_sample(g, e_int, a.cpu_seconds)
         result["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": nt, "kind": kind, "sample": desc}
     return result
+
+
+def streaming_batches(scale, nbatch, base, seed=4):
+    """Batch sizes log-uniform on [1, 2^20]; 70% insertions with R-MAT endpoints, 30% deletions
+    sampled from the base graph's edges (an already-deleted pick is a no-op)."""
+    from custingeralg_b200 import generators as G
+    rng = np.random.default_rng(seed)
+    sizes = np.floor(np.exp(rng.uniform(0.0, np.log(2.0 ** 20), nbatch))).astype(np.int64)
+    sizes = np.clip(sizes, 1, 1 << 20)
+    src_of = np.repeat(np.arange(base.n, dtype=np.int32), np.diff(base.off))
+    out = []
+    for i, b in enumerate(sizes.tolist()):
+        n_del = int(round(0.3 * b))
+        n_ins = b - n_del
+        s_ins, d_ins = G.rmat_pairs(scale, n_ins, seed=seed, stream=i + 1)
+        pick = rng.integers(0, base.m, n_del)
+        s = np.concatenate([s_ins, src_of[pick]]).astype(np.int32)
+        d = np.concatenate([d_ins, base.ind[pick]]).astype(np.int32)
+        dl = np.concatenate([np.zeros(n_ins, np.uint8), np.ones(n_del, np.uint8)])
+        perm = rng.permutation(b)
+        out.append((s[perm], d[perm], dl[perm]))
+    return out
+
+
+def run_streaming(a, dev):
+    """Update edges per second on R-MAT scale 22 (seed 4) with 200 uneven batches; the running
+    count is checked against a full static recount after every batch (outside the timing)."""
+    import torch
+    from custingeralg_b200 import api, generators as G, native as N
+    base = G.rmat(a.stream_scale, 16, 0.57, 0.19, 0.19, seed=4)
+    graph = api.Graph.from_csr(base, slack=0.25)
+    pv = torch.zeros(base.n + 1, dtype=torch.int32, device=dev)
+    delta = torch.zeros(1, dtype=torch.int64, device=dev)
+    scratch = torch.zeros(base.n + 1, dtype=torch.int32, device=dev)
+    T0, _ = graph.count(N.TC_PV_HANDLE, scratch)
+    batches = streaming_batches(a.stream_scale, a.stream_batches, base)
+    dbat = [(torch.from_numpy(s).to(dev), torch.from_numpy(d).to(dev), torch.from_numpy(x).to(dev))
+            for s, d, x in batches]
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    total_ms, updates, checked = 0.0, 0, 0
+    for i, (s, d, x) in enumerate(dbat):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        graph.apply_batch(s, d, x, per_vertex=pv, delta_dev=delta, sync=False)
+        e1.record(stream)
+        e1.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        updates += s.numel()
+        if a.stream_verify and (i % a.stream_verify == 0 or i == len(dbat) - 1):
+            T, _ = graph.count(N.TC_PV_HANDLE, scratch)
+            if T != T0 + int(delta.item()):
+                raise SystemExit(f"streaming mismatch after batch {i}: recount {T} vs running {T0 + int(delta.item())}")
+            if not torch.equal(scratch[: base.n], (pv[: base.n].to(torch.int64) +
+                                                  _static_pv_cache(graph, base, T0, dev)).to(torch.int32)):
+                raise SystemExit(f"per-vertex streaming mismatch after batch {i}")
+            checked += 1
+    return {"value": updates / (total_ms / 1e3), "unit": "update edges/s", "batches": len(dbat),
+            "updates": updates, "ms_total": total_ms, "recount_checks": checked,
+            "workload": f"R-MAT scale {a.stream_scale} ef 16 seed 4 base (slack 0.25), {len(dbat)} batches of "
+                        "log-uniform size in [1, 2^20], 70% R-MAT insertions / 30% deletions of base edges; "
+                        "timed per batch over sort + classify + structure update + delta count, batches resident "
+                        "on the device",
+            "final_triangles": T0 + int(delta.item())}
+
+
+_PV0 = {}
+
+
+def _static_pv_cache(graph, base, T0, dev):
+    """Per-vertex 2t(v) of the base graph (computed once on a fresh handle)."""
+    import torch
+    from custingeralg_b200 import api, native as N
+    key = id(base)
+    if key not in _PV0:
+        g0 = api.Graph.from_csr(base)
+        out = torch.zeros(base.n + 1, dtype=torch.int32, device=dev)
+        g0.count(N.TC_PV_HANDLE, out)
+        _PV0[key] = out[: base.n].to(torch.int64)
+        g0.close()
+    return _PV0[key]
 
 
 def run_reference(a, rank, world):

@@ -93,6 +93,34 @@ class Graph:
         return (info.triangles, info) if sync else None
 
 
+def _apply_batch(self, src, dst, is_delete=None, per_vertex=None, delta_dev=None, sched=None, sync=True,
+                 stream=None):
+    """tc_apply_batch: undirected updates {src[i], dst[i]}; numpy arrays (host) or CUDA tensors.
+    Returns BatchInfo when sync."""
+    import torch
+    info = N.BatchInfo() if sync else None
+    if isinstance(src, np.ndarray):
+        s = np.ascontiguousarray(src, dtype=np.int32)
+        d = np.ascontiguousarray(dst, dtype=np.int32)
+        dl = None if is_delete is None else np.ascontiguousarray(is_delete, dtype=np.uint8)
+        b = s.size
+        args = (s.ctypes.data if b else None, d.ctypes.data if b else None,
+                dl.ctypes.data if (dl is not None and b) else None, b, N.TC_MEM_HOST)
+    else:
+        assert src.is_cuda and src.dtype == torch.int32 and dst.dtype == torch.int32
+        b = src.numel()
+        args = (src.data_ptr() if b else None, dst.data_ptr() if b else None,
+                is_delete.data_ptr() if (is_delete is not None and b) else None, b, N.TC_MEM_DEVICE)
+    st = N.lib().tc_apply_batch(self._h, *args, _ptr(per_vertex), _ptr(delta_dev),
+                                ctypes.byref(info) if sync else None,
+                                ctypes.byref(sched) if sched is not None else None, _stream_ptr(stream))
+    N.check(st)
+    return info
+
+
+Graph.apply_batch = _apply_batch
+
+
 def count_all_triangles(graph: Graph, out, sched=None, stream=None):
     """callDeviceAllTriangles: out[v] = 2 t(v) for v < nv (device int32 tensor, >= nv entries)."""
     return graph.count(N.TC_PV_HANDLE, out, sched=sched, stream=stream)

@@ -62,6 +62,11 @@ void free_graph(tc_graph* g) {
   cudaFree(g->used);
   cudaFree(g->cap);
   cudaFree(g->pool);
+  cudaFree(g->d_pool_top);
+  cudaFree(g->mark);
+  cudaFree(g->pv_scratch);
+  release_stream_ws(g->sw);
+  g->sw = nullptr;
   g->ws.release();
 }
 
@@ -163,6 +168,8 @@ tc_status tc_graph_create(int32_t nv, const int64_t* off, const int32_t* ind, in
   // Headroom for lists that move when they outgrow their slack.
   g->pool_cap = top + (g->slack_q10 > 0 ? std::max<int64_t>(top / 4, 1 << 16) : 0);
   G_TRY(cudaMalloc(&g->pool, sizeof(int32_t) * (size_t)std::max<int64_t>(g->pool_cap, 1)));
+  G_TRY(cudaMalloc(&g->d_pool_top, sizeof(unsigned long long)));
+  G_TRY(cudaMemcpyAsync(g->d_pool_top, &g->pool_top, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
   if (nv > 0) {
     k_copy_lists<<<warp_grid(nv), 256, 0, s>>>(nv, d_off, d_ind, g->start, g->used, g->pool);
     G_TRY(cudaGetLastError());

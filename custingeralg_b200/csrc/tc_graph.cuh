@@ -3,6 +3,11 @@
 
 #include "tc_internal.cuh"
 
+namespace tc {
+struct StreamWs;
+void release_stream_ws(StreamWs* w);
+}  // namespace tc
+
 // Slack-managed adjacency: vertex v owns pool[start[v] .. start[v] + cap[v]); its first used[v]
 // entries are its neighbours, strictly ascending. Capacities are multiples of 4 entries so
 // every list starts on a 16-byte boundary. Lists that outgrow their capacity move to fresh
@@ -19,6 +24,11 @@ struct tc_graph {
   int32_t* cap = nullptr;
   int32_t* pool = nullptr;
   tc::Workspace ws;       // static-count workspace (oriented CSR etc.)
+  unsigned long long* d_pool_top = nullptr;  // device bump pointer (authoritative)
+  uint8_t* mark = nullptr;        // per-slot change marks, parallel to pool (streaming)
+  tc::StreamWs* sw = nullptr;     // streaming workspace
+  void* pv_scratch = nullptr;     // per-vertex sink when a batch call passes none
+  uint64_t view_version = 0;      // bumped by every structural update
 };
 
 namespace tc {

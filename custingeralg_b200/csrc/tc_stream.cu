@@ -1,0 +1,940 @@
+// Streaming triangle counting: batch preparation, structural updates of the slack-managed
+// adjacency and the triangle delta of a batch (sm_100a).
+//
+// Replaces the reference's three streaming kernels devicecuStingerNewTriangles,
+// deviceBUThreeTriangles and deviceBUTwoCUOneTriangles (src/streaming_triangle_counting/
+// cct_upd.cu:231-410), whose inclusion-exclusion nets +2 per vertex of every new triangle on a
+// symmetric batch (K1 counts a triangle with k new edges k times, K2 and K3 correct the
+// overcount). Here a triangle is attributed once, to the smallest of its changed edges in the
+// (min id, max id) order: k_delta intersects N(x) and N(y) for each changed edge {x, y} and keeps
+// a common neighbour w unless (x, w) or (y, w) is a changed edge with a smaller key. Whether an
+// edge is changed comes either from a per-slot mark array parallel to the adjacency pool
+// (tc_apply_batch) or from a lookup in the sorted batch (the cuStinger-style path).
+//
+// Per changed edge the warp intersects the two full lists with one of two strategies chosen by
+// their lengths: binary search of the shorter list's entries into the longer ("search", for
+// skewed pairs) or a partitioned merge in which each lane owns a contiguous slice of the shorter
+// list and merges it against the longer one from a binary-searched start ("merge", for balanced
+// pairs).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "tc_graph.cuh"
+
+namespace tc {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr uint64_t kSentinel = ~0ull;
+
+enum : unsigned { kErrRange = 1u, kErrPool = 2u };
+
+struct BatchStatus {
+  unsigned long long n_uniq;      // unique undirected edges
+  unsigned long long n_del;       // effective deletions
+  unsigned long long n_ins;       // effective insertions
+  unsigned long long n_dir;       // directed insert entries (2 n_ins)
+  unsigned long long n_runs;      // affected source vertices of insertions
+  unsigned long long demand;      // pool slots relocations may take
+  unsigned long long tri_removed;
+  unsigned long long tri_added;
+  unsigned long long pool_top;    // device copy of the bump pointer
+  unsigned long long dir_added;   // directed entries inserted (cuStinger path)
+  unsigned long long dir_removed; // directed entries deleted (cuStinger path)
+  unsigned long long not_fitting;
+  unsigned int err;
+  unsigned int pad;
+};
+
+__device__ __forceinline__ uint64_t ekey(int32_t a, int32_t b) {
+  const uint32_t lo = (uint32_t)min(a, b), hi = (uint32_t)max(a, b);
+  return ((uint64_t)lo << 32) | hi;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(kFull, x, o);
+  return x;
+}
+
+// First index in [lo, hi) of list with list[i] >= key.
+__device__ __forceinline__ int64_t lower_bound(const int32_t* __restrict__ list, int64_t lo, int64_t hi, int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = lo + ((hi - lo) >> 1);
+    if (__ldg(list + mid) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+int grid_for(int64_t items, int per_block) {
+  const int64_t want = std::max<int64_t>(1, (items + per_block - 1) / per_block);
+  return (int)std::min<int64_t>(want, (int64_t)device_info().sms * 16);
+}
+
+// ---- batch preparation (canonical undirected updates) --------------------------------------
+
+// key = (min << (L+1)) | (max << 1) | is_insert; self-loops and bad ids become the sentinel.
+__global__ void k_make_keys(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                            const uint8_t* __restrict__ is_del, const int64_t b, const int32_t n, const int L,
+                            uint64_t* __restrict__ keys, BatchStatus* __restrict__ st) {
+  const uint64_t sent = (1ull << (2 * L + 1)) - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t s = src[i], d = dst[i];
+    uint64_t k = sent;
+    if (s < 0 || s >= n || d < 0 || d >= n) {
+      atomicOr(&st->err, kErrRange);
+    } else if (s != d) {
+      const uint64_t lo = (uint64_t)min(s, d), hi = (uint64_t)max(s, d);
+      k = (lo << (L + 1)) | (hi << 1) | (uint64_t)((is_del && is_del[i]) ? 0 : 1);
+    }
+    keys[i] = k;
+  }
+}
+
+__global__ void k_run_heads(const uint64_t* __restrict__ keys, const int64_t b, const uint64_t sent,
+                            int32_t* __restrict__ head) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    head[i] = (k != sent) && (i == 0 || (keys[i - 1] >> 1) != (k >> 1));
+  }
+}
+
+// Each unique undirected edge: classify against the graph and append to the deletion or the
+// insertion list. A deletion records the slots of the edge in both lists.
+__global__ void k_classify(const SlackView g, const uint64_t* __restrict__ keys, const int64_t b, const int L,
+                           const int32_t* __restrict__ head, int4* __restrict__ dlist, int2* __restrict__ ilist,
+                           uint64_t* __restrict__ dirkeys, BatchStatus* __restrict__ st) {
+  const uint64_t maxmask = (1ull << L) - 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    if (!head[i]) continue;
+    const uint64_t e = keys[i] >> 1;
+    int64_t j = i;
+    while (j + 1 < b && (keys[j + 1] >> 1) == e) ++j;
+    const bool del_any = (keys[i] & 1ull) == 0;  // deletions sort before insertions of the same edge
+    const bool ins_any = (keys[j] & 1ull) == 1;
+    const int32_t x = (int32_t)(e >> L), y = (int32_t)(e & maxmask);
+    atomicAdd(&st->n_uniq, 1ull);
+    // presence: search the shorter list
+    const int32_t lx = g.len(x), ly = g.len(y);
+    const int64_t sx = g.start(x), sy = g.start(y);
+    int64_t px = -1, py = -1;
+    if (lx <= ly) {
+      const int64_t p = lower_bound(g.ind, sx, sx + lx, y);
+      if (p < sx + lx && g.ind[p] == y) px = p - sx;
+    } else {
+      const int64_t p = lower_bound(g.ind, sy, sy + ly, x);
+      if (p < sy + ly && g.ind[p] == x) py = p - sy;
+    }
+    const bool present = px >= 0 || py >= 0;
+    if (del_any && !ins_any && present) {
+      if (px < 0) px = lower_bound(g.ind, sx, sx + lx, y) - sx;
+      if (py < 0) py = lower_bound(g.ind, sy, sy + ly, x) - sy;
+      const unsigned long long at = atomicAdd(&st->n_del, 1ull);
+      dlist[at] = make_int4(x, y, (int32_t)px, (int32_t)py);
+    } else if (ins_any && !present) {
+      const unsigned long long at = atomicAdd(&st->n_ins, 1ull);
+      ilist[at] = make_int2(x, y);
+      dirkeys[2 * at] = ((uint64_t)(uint32_t)x << 32) | (uint32_t)y;
+      dirkeys[2 * at + 1] = ((uint64_t)(uint32_t)y << 32) | (uint32_t)x;
+    }
+  }
+}
+
+// ---- insertion planning / application ------------------------------------------------------
+
+// Heads of source-vertex runs in the sorted directed entries, and the pool slots the lists that
+// must move could take (computed on the pre-deletion lengths, an upper bound).
+__global__ void k_dir_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ used,
+                           const int32_t* __restrict__ cap, const int32_t slack_q10, int32_t* __restrict__ run_start,
+                           BatchStatus* __restrict__ st) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd_cap; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = dk[i];
+    if (k == kSentinel) continue;
+    const uint32_t v = (uint32_t)(k >> 32);
+    if (i > 0 && (uint32_t)(dk[i - 1] >> 32) == v) continue;
+    int64_t j = i;
+    while (j + 1 < nd_cap && dk[j + 1] != kSentinel && (uint32_t)(dk[j + 1] >> 32) == v) ++j;
+    const int32_t c = (int32_t)(j - i + 1);
+    const unsigned long long r = atomicAdd(&st->n_runs, 1ull);
+    run_start[r] = (int32_t)i;
+    const int32_t need = used[v] + c;
+    if (need > cap[v]) atomicAdd(&st->demand, (unsigned long long)slack_capacity(need, max(slack_q10, 256)));
+  }
+}
+
+// One warp per affected source vertex: merge its sorted new neighbours into its list, in place
+// (backwards) when the capacity allows, else into a fresh block at the pool top. New slots are
+// marked (mark = 1) when `mark` is given; their absolute slots go to slot[].
+__global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ run_start,
+                              int64_t* __restrict__ start, int32_t* __restrict__ used, int32_t* __restrict__ cap,
+                              int32_t* __restrict__ pool, const int64_t pool_cap, uint8_t* __restrict__ mark,
+                              int64_t* __restrict__ slot, unsigned long long* __restrict__ pool_top,
+                              const int32_t slack_q10, BatchStatus* __restrict__ st) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nruns = (int64_t)st->n_runs;
+  for (int64_t r = gw; r < nruns; r += nw) {
+    const int64_t i0 = run_start[r];
+    const int32_t v = (int32_t)(dk[i0] >> 32);
+    int64_t i1 = i0;  // run end (exclusive), found cooperatively
+    {
+      int64_t k = i0 + lane;
+      while (true) {
+        const bool same = k < nd_cap && dk[k] != kSentinel && (int32_t)(dk[k] >> 32) == v;
+        const unsigned m = __ballot_sync(kFull, same);
+        if (m != kFull) {
+          i1 = k - lane + __ffs(~m) - 1;
+          break;
+        }
+        k += 32;
+      }
+      i1 = __shfl_sync(kFull, i1, 0);
+    }
+    const int32_t c = (int32_t)(i1 - i0);
+    const int32_t a = used[v];
+    const int64_t s_old = start[v];
+    int64_t s_new = s_old;
+    bool moved = false;
+    if (a + c > cap[v]) {
+      const int32_t nc = slack_capacity(a + c, max(slack_q10, 256));
+      unsigned long long at = 0;
+      if (lane == 0) at = atomicAdd(pool_top, (unsigned long long)nc);
+      at = __shfl_sync(kFull, at, 0);
+      if ((int64_t)at + nc > pool_cap) {
+        if (lane == 0) atomicOr(&st->err, kErrPool);
+        continue;  // cannot happen when the host sized the pool from the demand pass
+      }
+      s_new = (int64_t)at;
+      moved = true;
+      if (lane == 0) {
+        cap[v] = nc;
+        atomicAdd(&st->not_fitting, (unsigned long long)c);
+      }
+    }
+    const int32_t* A = pool + s_old;
+    // New entries first, while A is intact: final position j + #(old < B[j]) (relative).
+    for (int64_t j = i0 + lane; j < i1; j += 32) {
+      const int32_t val = (int32_t)(uint32_t)dk[j];
+      int32_t lo = 0, hi = a;
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (A[mid] < val) lo = mid + 1;
+        else hi = mid;
+      }
+      slot[j] = (j - i0) + lo;
+    }
+    __syncwarp();
+    // Old entries: final position i + #(new < A[i]); backwards in chunks so that, in place, no
+    // unread entry is overwritten (targets never precede sources).
+    for (int32_t base = ((a - 1) / 32) * 32; base >= 0 && a > 0; base -= 32) {
+      const int32_t i = base + lane;
+      int32_t val = 0;
+      int64_t pos = 0;
+      if (i < a) {
+        val = A[i];
+        int64_t lo = i0, hi = i1;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if ((int32_t)(uint32_t)dk[mid] < val) lo = mid + 1;
+          else hi = mid;
+        }
+        pos = i + (lo - i0);
+      }
+      __syncwarp();
+      if (i < a) {
+        pool[s_new + pos] = val;
+        if (mark) mark[s_new + pos] = 0;
+      }
+      __syncwarp();
+    }
+    // New entries into the holes.
+    for (int64_t j = i0 + lane; j < i1; j += 32) {
+      const int64_t pos = s_new + slot[j];
+      pool[pos] = (int32_t)(uint32_t)dk[j];
+      if (mark) mark[pos] = 1;
+      slot[j] = pos;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      used[v] = a + c;
+      if (moved) start[v] = s_new;
+      atomicAdd(&st->dir_added, (unsigned long long)c);
+    }
+  }
+}
+
+__global__ void k_clear_slots(const int64_t* __restrict__ slot, const int64_t n, uint8_t* __restrict__ mark) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = slot[i];
+    if (s >= 0) mark[s] = 0;
+  }
+}
+
+// ---- deletion -------------------------------------------------------------------------------
+
+__global__ void k_mark_deletions(const int4* __restrict__ dlist, const BatchStatus* __restrict__ st,
+                                 const int64_t* __restrict__ start, uint8_t* __restrict__ mark) {
+  const int64_t nd = (int64_t)st->n_del;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += (int64_t)gridDim.x * blockDim.x) {
+    const int4 d = dlist[i];
+    mark[start[d.x] + d.z] = 1;
+    mark[start[d.y] + d.w] = 1;
+  }
+}
+
+// Remove marked slots from the lists of the vertices in vlist (each vertex once: the first warp
+// to claim it with this epoch compacts it), then clear the marks of the old range.
+__global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
+                                 const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start,
+                                 int32_t* __restrict__ used, int32_t* __restrict__ pool, uint8_t* __restrict__ mark,
+                                 unsigned* __restrict__ claim, const unsigned epoch, BatchStatus* __restrict__ st) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t cnt = nv_dev ? (int64_t)(*nv_dev) * stride : nv_list;
+  const unsigned lt = (1u << lane) - 1u;
+  for (int64_t k = gw; k < cnt; k += nw) {
+    const int32_t v = vlist[k];
+    unsigned old = 0;
+    if (lane == 0) old = atomicMax(&claim[v], epoch);
+    old = __shfl_sync(kFull, old, 0);
+    if (old >= epoch) continue;
+    const int64_t s = start[v];
+    const int32_t a = used[v];
+    int32_t wp = 0;
+    for (int32_t base = 0; base < a; base += 32) {
+      const int32_t i = base + lane;
+      int32_t val = 0;
+      bool keep = false;
+      if (i < a) {
+        val = pool[s + i];
+        keep = mark[s + i] == 0;
+      }
+      const unsigned m = __ballot_sync(kFull, keep);
+      __syncwarp();
+      if (keep) pool[s + wp + __popc(m & lt)] = val;
+      wp += __popc(m);
+      __syncwarp();
+    }
+    for (int32_t i = lane; i < a; i += 32) mark[s + i] = 0;
+    if (lane == 0) {
+      used[v] = wp;
+      atomicAdd(&st->dir_removed, (unsigned long long)(a - wp));
+    }
+  }
+}
+
+// ---- the triangle delta of changed edges -----------------------------------------------------
+
+enum { kPredMark = 0, kPredBatch = 1 };
+
+struct BatchLists {
+  const int32_t* src;    // sorted directed entries (cuStinger path)
+  const int32_t* dst;
+  const int32_t* off;    // batch CSR over src, int32[nv+1]
+  const int32_t* dup;
+};
+
+struct DeltaArgs {
+  SlackView g;
+  const uint8_t* mark;
+  // entries: either int2/int4 canonical lists (mark predicate) or the batch arrays
+  const int2* ilist;
+  const int4* dlist;
+  const unsigned long long* count_dev;  // number of entries (device), or NULL with count_host
+  int64_t count_host;
+  BatchLists bl;
+  int sign;          // +1 insertions, -1 deletions
+  uint32_t weight;   // per-vertex increment per counted triangle
+  int search_ratio_x16;
+  int only_present;  // skip entries whose edge is absent (cuStinger deletion count)
+};
+
+template <int PRED>
+__device__ __forceinline__ bool changed(const DeltaArgs& A, int32_t owner, int64_t slot_abs, int32_t w) {
+  if (PRED == kPredMark) return A.mark[slot_abs] != 0;
+  const int32_t lo = A.bl.off[owner], hi = A.bl.off[owner + 1];
+  int32_t l = lo, h = hi;
+  while (l < h) {
+    const int32_t mid = (l + h) >> 1;
+    if (A.bl.dst[mid] < w) l = mid + 1;
+    else h = mid;
+  }
+  return l < hi && A.bl.dst[l] == w && A.bl.dup[l] == 0;
+}
+
+template <int PRED>
+__global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
+                                                    unsigned long long* __restrict__ tri_out) {
+  __shared__ unsigned long long s_tri[kThreads / 32];
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
+  unsigned long long tri_acc = 0;
+  for (int64_t e = gw; e < cnt; e += nw) {
+    int32_t x, y;
+    bool count_total = true;
+    if (PRED == kPredMark) {
+      if (A.dlist) {
+        const int4 d = A.dlist[e];
+        x = d.x;
+        y = d.y;
+      } else {
+        const int2 d = A.ilist[e];
+        x = d.x;
+        y = d.y;
+      }
+    } else {
+      if (A.bl.dup[e]) continue;
+      x = A.bl.src[e];
+      y = A.bl.dst[e];
+      if (x == y) continue;
+      count_total = x < y;  // symmetric batch: each undirected edge appears in both directions
+    }
+    const int32_t lx = A.g.len(x), ly = A.g.len(y);
+    if (lx < 2 || ly < 2) continue;
+    const int64_t sx = A.g.start(x), sy = A.g.start(y);
+    if (PRED == kPredBatch && A.only_present) {
+      // the edge must exist for its triangles to be destroyed
+      bool pres = false;
+      if (lane == 0) {
+        const int64_t p = lower_bound(A.g.ind, sx, sx + lx, y);
+        pres = p < sx + lx && A.g.ind[p] == y;
+      }
+      if (!__shfl_sync(kFull, pres, 0)) continue;
+    }
+    const uint64_t key = ekey(x, y);
+    // A = shorter list, B = longer.
+    const bool xs = lx <= ly;
+    const int32_t oa = xs ? x : y, ob = xs ? y : x;
+    const int64_t sa = xs ? sx : sy, sb = xs ? sy : sx;
+    const int32_t la = xs ? lx : ly, lb = xs ? ly : lx;
+    const int32_t* L = A.g.ind;
+    uint32_t c = 0;
+    auto on_match = [&](int64_t ia, int64_t ib, int32_t w) {
+      const bool ca = changed<PRED>(A, oa, sa + ia, w);
+      const bool cb = changed<PRED>(A, ob, sb + ib, w);
+      const bool keep = (!ca || key < ekey(oa, w)) && (!cb || key < ekey(ob, w));
+      if (keep) {
+        ++c;
+        atomicAdd(&pv[w], A.weight * (uint32_t)A.sign);
+      }
+    };
+    const int lg = 32 - __clz(lb);
+    const bool search = 16LL * lb > (long long)A.search_ratio_x16 * la * lg;
+    if (search) {
+      for (int32_t i = lane; i < la; i += 32) {
+        const int32_t w = L[sa + i];
+        const int64_t p = lower_bound(L, sb, sb + lb, w);
+        if (p < sb + lb && L[p] == w) on_match(i, p - sb, w);
+      }
+    } else {
+      const int32_t per = (la + 31) / 32;
+      const int32_t i0 = min(la, lane * per), i1 = min(la, i0 + per);
+      if (i0 < i1) {
+        int64_t p = lower_bound(L, sb, sb + lb, L[sa + i0]);
+        for (int32_t i = i0; i < i1 && p < sb + lb; ++i) {
+          const int32_t w = L[sa + i];
+          while (p < sb + lb && L[p] < w) ++p;
+          if (p < sb + lb && L[p] == w) on_match(i, p - sb, w);
+        }
+      }
+    }
+    c = warp_sum(c);
+    if (lane == 0 && c) {
+      atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
+      atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
+      if (count_total) tri_acc += c;
+    }
+  }
+  if (lane == 0) s_tri[wid] = tri_acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int w = 0; w < kThreads / 32; ++w) s += s_tri[w];
+    if (s) atomicAdd(tri_out, s);
+  }
+}
+
+// ---- cuStinger-style batch helpers ------------------------------------------------------------
+
+__global__ void k_pack_dir(const int32_t* __restrict__ s, const int32_t* __restrict__ d, const int64_t b,
+                           uint64_t* __restrict__ keys) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x)
+    keys[i] = ((uint64_t)(uint32_t)s[i] << 32) | (uint32_t)d[i];
+}
+
+__global__ void k_unpack_dir(const uint64_t* __restrict__ keys, const int64_t b, const int32_t nv, int32_t* __restrict__ s,
+                             int32_t* __restrict__ d, int32_t* __restrict__ dup, int32_t* __restrict__ cnt,
+                             unsigned* __restrict__ err) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    const int32_t a = (int32_t)(k >> 32), c = (int32_t)(uint32_t)k;
+    s[i] = a;
+    d[i] = c;
+    const bool bad = a < 0 || a >= nv || c < 0 || c >= nv;
+    if (bad) {
+      atomicOr(err, kErrRange);
+      dup[i] = 1;
+      continue;
+    }
+    dup[i] = (a == c) || (i > 0 && keys[i - 1] == k);
+    atomicAdd(&cnt[a], 1);
+  }
+}
+
+// Entries with dup == 0 that are already in the graph become duplicates; the rest are packed
+// as directed insertion keys (sentinel elsewhere).
+__global__ void k_flag_present(const SlackView g, const int32_t* __restrict__ s, const int32_t* __restrict__ d,
+                               int32_t* __restrict__ dup, const int64_t b, uint64_t* __restrict__ dk) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = kSentinel;
+    if (!dup[i]) {
+      const int32_t x = s[i], y = d[i];
+      const int64_t sx = g.start(x);
+      const int32_t lx = g.len(x);
+      const int64_t p = lower_bound(g.ind, sx, sx + lx, y);
+      if (p < sx + lx && g.ind[p] == y) dup[i] = 1;
+      else k = ((uint64_t)(uint32_t)x << 32) | (uint32_t)y;
+    }
+    dk[i] = k;
+  }
+}
+
+// Mark the slots of present, non-duplicate entries for deletion; list their source vertices.
+__global__ void k_mark_dir_deletions(const SlackView g, const int32_t* __restrict__ s, const int32_t* __restrict__ d,
+                                     const int32_t* __restrict__ dup, const int64_t b, uint8_t* __restrict__ mark,
+                                     int32_t* __restrict__ vlist, unsigned long long* __restrict__ nvl) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    if (dup[i]) continue;
+    const int32_t x = s[i], y = d[i];
+    const int64_t sx = g.start(x);
+    const int32_t lx = g.len(x);
+    const int64_t p = lower_bound(g.ind, sx, sx + lx, y);
+    if (p < sx + lx && g.ind[p] == y) {
+      mark[p] = 1;
+      vlist[atomicAdd(nvl, 1ull)] = x;
+    }
+  }
+}
+
+__global__ void k_endpoints(const int4* __restrict__ dlist, const BatchStatus* __restrict__ st, int32_t* __restrict__ vlist) {
+  const int64_t nd = (int64_t)st->n_del;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += (int64_t)gridDim.x * blockDim.x) {
+    vlist[2 * i] = dlist[i].x;
+    vlist[2 * i + 1] = dlist[i].y;
+  }
+}
+
+__global__ void k_add_delta(int64_t* __restrict__ delta, const unsigned long long* __restrict__ add,
+                            const unsigned long long* __restrict__ sub) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *delta += (int64_t)(add ? *add : 0ull) - (int64_t)(sub ? *sub : 0ull);
+}
+
+__global__ void k_to_int32(const int64_t* __restrict__ in, const int64_t n, int32_t* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (int32_t)in[i];
+}
+
+}  // namespace
+
+// ---- per-graph streaming workspace -----------------------------------------------------------
+
+struct StreamWs {
+  int64_t b_cap = 0;
+  int64_t n_cap = 0;
+  int32_t* src = nullptr;       // host batches staged here
+  int32_t* dst = nullptr;
+  uint8_t* isdel = nullptr;
+  uint64_t* keys = nullptr;     // [b]
+  uint64_t* keys2 = nullptr;    // [b]
+  int32_t* head = nullptr;      // [b]
+  int4* dlist = nullptr;        // [b]
+  int2* ilist = nullptr;        // [b]
+  uint64_t* dk = nullptr;       // [2b]
+  uint64_t* dk2 = nullptr;      // [2b]
+  int32_t* run_start = nullptr; // [2b]
+  int64_t* ins_slot = nullptr;  // [2b]
+  int32_t* vlist = nullptr;     // [2b]
+  unsigned* claim = nullptr;    // [n]
+  unsigned epoch = 0;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+  BatchStatus* st = nullptr;
+  BatchStatus* st_host = nullptr;  // pinned
+  unsigned long long* counter = nullptr;
+  int32_t* cnt = nullptr;       // [n+1] per-source counts (cuStinger sort)
+  int64_t* scan64 = nullptr;    // [n+1]
+  int64_t* tiles = nullptr;
+  void release();
+};
+
+void StreamWs::release() {
+  cudaFree(src); cudaFree(dst); cudaFree(isdel); cudaFree(keys); cudaFree(keys2); cudaFree(head);
+  cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(ins_slot);
+  cudaFree(vlist); cudaFree(claim); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
+  cudaFree(cnt); cudaFree(scan64); cudaFree(tiles);
+  *this = StreamWs();
+}
+
+void release_stream_ws(StreamWs* w) {
+  if (!w) return;
+  w->release();
+  delete w;
+}
+
+namespace {
+
+tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
+  if (!g->sw) g->sw = new StreamWs();
+  StreamWs& w = *g->sw;
+  if (!g->mark) {
+    TC_CUDA_TRY(cudaMalloc(&g->mark, (size_t)std::max<int64_t>(g->pool_cap, 1)));
+    TC_CUDA_TRY(cudaMemset(g->mark, 0, (size_t)std::max<int64_t>(g->pool_cap, 1)));
+  }
+  if (w.n_cap < (int64_t)g->n + 1) {
+    cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles);
+    TC_CUDA_TRY(cudaMalloc(&w.claim, sizeof(unsigned) * ((size_t)g->n + 1)));
+    TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * ((size_t)g->n + 1)));
+    TC_CUDA_TRY(cudaMalloc(&w.cnt, sizeof(int32_t) * ((size_t)g->n + 1)));
+    TC_CUDA_TRY(cudaMalloc(&w.scan64, sizeof(int64_t) * ((size_t)g->n + 2)));
+    TC_CUDA_TRY(cudaMalloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)));
+    w.n_cap = g->n + 1;
+    w.epoch = 0;
+  }
+  if (!w.st) {
+    TC_CUDA_TRY(cudaMalloc(&w.st, sizeof(BatchStatus)));
+    TC_CUDA_TRY(cudaMallocHost(&w.st_host, sizeof(BatchStatus)));
+    TC_CUDA_TRY(cudaMalloc(&w.counter, sizeof(unsigned long long)));
+  }
+  if (b <= w.b_cap) return TC_OK;
+  const int64_t nb = std::max<int64_t>(b, 1024);
+  cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
+  cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
+  cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
+  w.cub_tmp = nullptr;
+  TC_CUDA_TRY(cudaMalloc(&w.src, sizeof(int32_t) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.dst, sizeof(int32_t) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.isdel, nb));
+  TC_CUDA_TRY(cudaMalloc(&w.keys, sizeof(uint64_t) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.keys2, sizeof(uint64_t) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.head, sizeof(int32_t) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.dlist, sizeof(int4) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.ilist, sizeof(int2) * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.dk, sizeof(uint64_t) * 2 * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.dk2, sizeof(uint64_t) * 2 * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.run_start, sizeof(int32_t) * 2 * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.ins_slot, sizeof(int64_t) * 2 * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.vlist, sizeof(int32_t) * 2 * nb));
+  size_t t1 = 0, t2 = 0;
+  TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t1, w.keys, w.keys2, (int)(2 * nb)));
+  TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t2, w.dk, w.dk2, (int)(2 * nb)));
+  w.cub_bytes = std::max(t1, t2);
+  TC_CUDA_TRY(cudaMalloc(&w.cub_tmp, w.cub_bytes));
+  w.b_cap = nb;
+  return TC_OK;
+}
+
+// Make room for `extra` slots past pool_top (grow the pool and the mark array by copying).
+tc_status ensure_pool(tc_graph* g, int64_t extra, cudaStream_t s) {
+  const int64_t need = g->pool_top + extra;
+  if (need <= g->pool_cap) return TC_OK;
+  const int64_t ncap = std::max<int64_t>(need + need / 4, g->pool_cap * 3 / 2);
+  int32_t* np = nullptr;
+  uint8_t* nm = nullptr;
+  TC_CUDA_TRY(cudaMalloc(&np, sizeof(int32_t) * (size_t)ncap));
+  TC_CUDA_TRY(cudaMalloc(&nm, (size_t)ncap));
+  TC_CUDA_TRY(cudaMemcpyAsync(np, g->pool, sizeof(int32_t) * (size_t)g->pool_top, cudaMemcpyDeviceToDevice, s));
+  TC_CUDA_TRY(cudaMemsetAsync(nm, 0, (size_t)ncap, s));
+  if (g->mark) TC_CUDA_TRY(cudaMemcpyAsync(nm, g->mark, (size_t)g->pool_top, cudaMemcpyDeviceToDevice, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaFree(g->pool);
+  cudaFree(g->mark);
+  g->pool = np;
+  g->mark = nm;
+  g->pool_cap = ncap;
+  g->view_version++;
+  return TC_OK;
+}
+
+int bits_for(int32_t n) {
+  int L = 1;
+  while (L < 31 && ((int64_t)1 << L) < (int64_t)n) ++L;
+  return L;
+}
+
+DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
+  DeltaArgs A;
+  memset(&A, 0, sizeof(A));
+  A.g = SlackView{g->start, g->used, g->pool};
+  A.mark = g->mark;
+  A.search_ratio_x16 = sp.search_ratio_x16;
+  return A;
+}
+
+int delta_grid() { return device_info().sms * 8; }
+
+}  // namespace
+}  // namespace tc
+
+using namespace tc;
+
+extern "C" {
+
+tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, const uint8_t* is_delete, int64_t b,
+                         int mem, int32_t* per_vertex, int64_t* delta_dev, tc_batch_info* info, const tc_sched* sched,
+                         void* stream) {
+  if (!g) return fail(TC_ERR_INVALID_ARG, "graph is NULL");
+  if (b < 0 || (b > 0 && (!src || !dst)) || (mem != TC_MEM_HOST && mem != TC_MEM_DEVICE))
+    return fail(TC_ERR_INVALID_ARG, "invalid batch arguments");
+  if (b > (int64_t)INT32_MAX / 2) return fail(TC_ERR_CAPACITY, "batch of %lld pairs exceeds 2^30", (long long)b);
+  cudaStream_t s = (cudaStream_t)stream;
+  TC_TRY(ensure_stream_ws(g, b));
+  StreamWs& w = *g->sw;
+  const SchedParams sp = to_params(sched);
+  TC_CUDA_TRY(cudaMemsetAsync(w.st, 0, sizeof(BatchStatus), s));
+  const int32_t* d_src = src;
+  const int32_t* d_dst = dst;
+  const uint8_t* d_del = is_delete;
+  if (mem == TC_MEM_HOST && b > 0) {
+    TC_CUDA_TRY(cudaMemcpyAsync(w.src, src, sizeof(int32_t) * b, cudaMemcpyHostToDevice, s));
+    TC_CUDA_TRY(cudaMemcpyAsync(w.dst, dst, sizeof(int32_t) * b, cudaMemcpyHostToDevice, s));
+    if (is_delete) TC_CUDA_TRY(cudaMemcpyAsync(w.isdel, is_delete, b, cudaMemcpyHostToDevice, s));
+    d_src = w.src;
+    d_dst = w.dst;
+    d_del = is_delete ? w.isdel : nullptr;
+  }
+  const int L = bits_for(std::max(g->n, 2));
+  const uint64_t sent = (1ull << (2 * L + 1)) - 1;
+  SlackView view{g->start, g->used, g->pool};
+  const int gb = grid_for(std::max<int64_t>(b, 1), kThreads);
+  // 1. canonical keys, sort, unique + classify
+  if (b > 0) {
+    k_make_keys<<<gb, kThreads, 0, s>>>(d_src, d_dst, d_del, b, g->n, L, w.keys, w.st);
+    size_t tb = w.cub_bytes;
+    TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb, w.keys, w.keys2, (int)b, 0, 2 * L + 1, s));
+    k_run_heads<<<gb, kThreads, 0, s>>>(w.keys2, b, sent, w.head);
+    TC_CUDA_TRY(cudaMemsetAsync(w.dk, 0xff, sizeof(uint64_t) * 2 * b, s));
+    k_classify<<<gb, kThreads, 0, s>>>(view, w.keys2, b, L, w.head, w.dlist, w.ilist, w.dk, w.st);
+    size_t tb2 = w.cub_bytes;
+    TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * b), 0, 64, s));
+    k_dir_runs<<<grid_for(2 * b, kThreads), kThreads, 0, s>>>(w.dk2, 2 * b, g->used, g->cap, g->slack_q10, w.run_start,
+                                                               w.st);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  // 2. one synchronisation: sizes and the pool demand
+  TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(&w.st_host->pool_top, g->d_pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  const BatchStatus h = *w.st_host;
+  g->pool_top = (int64_t)h.pool_top;
+  if (h.err & kErrRange) return fail(TC_ERR_INVALID_ARG, "batch has vertex ids outside [0, %d)", g->n);
+  TC_TRY(ensure_pool(g, (int64_t)h.demand, s));
+  uint32_t* pv = reinterpret_cast<uint32_t*>(per_vertex);
+  uint32_t* pv_use = pv;
+  uint32_t* scratch_pv = nullptr;
+  if (!pv_use) {
+    // counts only: route per-vertex updates to a scratch array
+    if (!g->pv_scratch) TC_CUDA_TRY(cudaMalloc(&g->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)));
+    scratch_pv = reinterpret_cast<uint32_t*>(g->pv_scratch);
+    pv_use = scratch_pv;
+  }
+  view = SlackView{g->start, g->used, g->pool};
+  // 3. deletions: mark, count on the pre-deletion graph, compact
+  if (h.n_del > 0) {
+    const int gd = grid_for((int64_t)h.n_del, kThreads);
+    k_mark_deletions<<<gd, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
+    DeltaArgs A = delta_args(g, sp);
+    A.dlist = w.dlist;
+    A.count_dev = &w.st->n_del;
+    A.sign = -1;
+    A.weight = 2;
+    k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
+    k_endpoints<<<gd, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
+    ++w.epoch;
+    k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
+        w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.epoch, w.st);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  // 4. insertions: merge into the lists, count on the post-insertion graph, clear marks
+  if (h.n_ins > 0) {
+    k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
+        w.dk2, 2 * b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, g->mark, w.ins_slot,
+        g->d_pool_top, g->slack_q10, w.st);
+    DeltaArgs A = delta_args(g, sp);
+    A.ilist = w.ilist;
+    A.count_dev = &w.st->n_ins;
+    A.sign = 1;
+    A.weight = 2;
+    k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
+    k_clear_slots<<<grid_for(2 * (int64_t)h.n_ins, kThreads), kThreads, 0, s>>>(w.ins_slot, 2 * (int64_t)h.n_ins,
+                                                                                  g->mark);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  g->m += 2 * ((int64_t)h.n_ins - (int64_t)h.n_del);
+  g->pool_top += (int64_t)h.demand;  // host bound until the next read of the device counter
+  g->view_version++;
+  if (delta_dev) k_add_delta<<<1, 32, 0, s>>>(delta_dev, &w.st->tri_added, &w.st->tri_removed);
+  if (info) {
+    TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+    TC_CUDA_TRY(cudaStreamSynchronize(s));
+    const BatchStatus& f = *w.st_host;
+    if (f.err & kErrPool) return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+    info->updates = b;
+    info->inserted = (int64_t)f.n_ins;
+    info->deleted = (int64_t)f.n_del;
+    info->ignored = b - (int64_t)f.n_ins - (int64_t)f.n_del;
+    info->triangles_added = (int64_t)f.tri_added;
+    info->triangles_removed = (int64_t)f.tri_removed;
+    info->status = TC_OK;
+  }
+  return TC_OK;
+}
+
+tc_status tc_batch_sort(int32_t nv, int32_t* d_src, int32_t* d_dst, int64_t b, int32_t* d_offsets, int32_t* d_dup,
+                        void* stream) {
+  if (nv < 0 || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup)) || !d_offsets)
+    return fail(TC_ERR_INVALID_ARG, "invalid batch arguments");
+  if (b > (int64_t)INT32_MAX / 2) return fail(TC_ERR_CAPACITY, "batch too large");
+  cudaStream_t s = (cudaStream_t)stream;
+  uint64_t *k1 = nullptr, *k2 = nullptr;
+  void* tmp = nullptr;
+  size_t tb = 0;
+  int32_t* cnt = nullptr;
+  int64_t *off64 = nullptr, *tiles = nullptr;
+  unsigned* err = nullptr;
+  tc_status rc = TC_OK;
+  unsigned herr = 0;
+  do {
+    if (cudaMalloc(&k1, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
+        cudaMalloc(&k2, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
+        cudaMalloc(&cnt, sizeof(int32_t) * ((size_t)nv + 1)) != cudaSuccess ||
+        cudaMalloc(&off64, sizeof(int64_t) * ((size_t)nv + 2)) != cudaSuccess ||
+        cudaMalloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(nv) + 1)) != cudaSuccess ||
+        cudaMalloc(&err, sizeof(unsigned)) != cudaSuccess) {
+      rc = fail(TC_ERR_OOM, "batch sort: allocation failed");
+      break;
+    }
+    cudaMemsetAsync(cnt, 0, sizeof(int32_t) * ((size_t)nv + 1), s);
+    cudaMemsetAsync(err, 0, sizeof(unsigned), s);
+    if (b > 0) {
+      k_pack_dir<<<grid_for(b, kThreads), kThreads, 0, s>>>(d_src, d_dst, b, k1);
+      cub::DeviceRadixSort::SortKeys(nullptr, tb, k1, k2, (int)b, 0, 64, s);
+      if (cudaMalloc(&tmp, std::max<size_t>(tb, 1)) != cudaSuccess) {
+        rc = fail(TC_ERR_OOM, "batch sort: allocation failed");
+        break;
+      }
+      cub::DeviceRadixSort::SortKeys(tmp, tb, k1, k2, (int)b, 0, 64, s);
+      k_unpack_dir<<<grid_for(b, kThreads), kThreads, 0, s>>>(k2, b, nv, d_src, d_dst, d_dup, cnt, err);
+    }
+    rc = scan_counts(cnt, nv, off64, tiles, s);
+    if (rc != TC_OK) break;
+    k_to_int32<<<grid_for((int64_t)nv + 1, kThreads), kThreads, 0, s>>>(off64, nv, d_offsets);
+    cudaMemcpyAsync(&herr, err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = fail(TC_ERR_CUDA, "batch sort: %s", cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    if (herr) rc = fail(TC_ERR_INVALID_ARG, "batch has vertex ids outside [0, %d)", nv);
+  } while (0);
+  cudaFree(k1); cudaFree(k2); cudaFree(tmp); cudaFree(cnt); cudaFree(off64); cudaFree(tiles); cudaFree(err);
+  return rc;
+}
+
+tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, int64_t b, int32_t* d_dup,
+                           int64_t* not_fitting, void* stream) {
+  if (!g || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup))) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  TC_TRY(ensure_stream_ws(g, (b + 1) / 2 + 1));
+  StreamWs& w = *g->sw;
+  TC_CUDA_TRY(cudaMemsetAsync(w.st, 0, sizeof(BatchStatus), s));
+  if (not_fitting) *not_fitting = 0;
+  if (b == 0) return TC_OK;
+  SlackView view{g->start, g->used, g->pool};
+  // entries come sorted by (src, dst): the packed keys of the new ones stay sorted, sentinel
+  // elsewhere; sort once more to push the sentinels to the end.
+  k_flag_present<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, w.dk);
+  size_t tb = w.cub_bytes;
+  TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb, w.dk, w.dk2, (int)b, 0, 64, s));
+  k_dir_runs<<<grid_for(b, kThreads), kThreads, 0, s>>>(w.dk2, b, g->used, g->cap, g->slack_q10, w.run_start, w.st);
+  TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(&w.st_host->pool_top, g->d_pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  const BatchStatus h = *w.st_host;
+  g->pool_top = (int64_t)h.pool_top;
+  TC_TRY(ensure_pool(g, (int64_t)h.demand, s));
+  if (h.n_runs > 0) {
+    k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
+        w.dk2, b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, nullptr, w.ins_slot, g->d_pool_top,
+        g->slack_q10, w.st);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  if (w.st_host->err & kErrPool) return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+  g->m += (int64_t)w.st_host->dir_added;
+  g->pool_top += (int64_t)h.demand;  // host bound until the next read of the device counter
+  g->view_version++;
+  if (not_fitting) *not_fitting = (int64_t)w.st_host->not_fitting;
+  return TC_OK;
+}
+
+tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, const int32_t* d_dup, int64_t b,
+                           void* stream) {
+  if (!g || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup))) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  TC_TRY(ensure_stream_ws(g, (b + 1) / 2 + 1));
+  StreamWs& w = *g->sw;
+  TC_CUDA_TRY(cudaMemsetAsync(w.st, 0, sizeof(BatchStatus), s));
+  if (b == 0) return TC_OK;
+  TC_CUDA_TRY(cudaMemsetAsync(w.counter, 0, sizeof(unsigned long long), s));
+  SlackView view{g->start, g->used, g->pool};
+  k_mark_dir_deletions<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, g->mark, w.vlist,
+                                                                   w.counter);
+  ++w.epoch;
+  k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
+                                                                   g->pool, g->mark, w.claim, w.epoch, w.st);
+  TC_CUDA_TRY(cudaGetLastError());
+  TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
+  TC_CUDA_TRY(cudaStreamSynchronize(s));
+  g->m -= (int64_t)w.st_host->dir_removed;
+  g->view_version++;
+  return TC_OK;
+}
+
+tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, const int32_t* d_offsets,
+                         const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
+                         const tc_sched* sched, void* stream) {
+  if (!g || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup || !d_offsets)) || (sign != 1 && sign != -1) || !per_vertex)
+    return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  cudaStream_t s = (cudaStream_t)stream;
+  TC_TRY(ensure_stream_ws(g, 1));
+  StreamWs& w = *g->sw;
+  TC_CUDA_TRY(cudaMemsetAsync(w.counter, 0, sizeof(unsigned long long), s));
+  if (b > 0) {
+    DeltaArgs A = delta_args(g, to_params(sched));
+    A.bl = BatchLists{d_src, d_dst, d_offsets, d_dup};
+    A.count_host = b;
+    A.sign = sign;
+    A.weight = 1;
+    A.only_present = sign < 0;
+    k_delta<kPredBatch><<<delta_grid(), kThreads, 0, s>>>(A, reinterpret_cast<uint32_t*>(per_vertex), w.counter);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  if (delta_dev) {
+    if (sign > 0) k_add_delta<<<1, 32, 0, s>>>(delta_dev, w.counter, nullptr);
+    else k_add_delta<<<1, 32, 0, s>>>(delta_dev, nullptr, w.counter);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
+  return TC_OK;
+}
+
+}  // extern "C"

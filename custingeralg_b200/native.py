@@ -21,6 +21,11 @@ TC_ERR_CAPACITY = 6
 TC_ERR_TIMEOUT = 7
 TC_ERR_STATE = 8
 
+MLP_IN = 4
+MLP_HIDDEN = 64
+MLP_OUT = 3
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
+
 TC_PV_NONE = 0
 TC_PV_HANDLE = 1
 TC_PV_CSR = 2
@@ -46,6 +51,11 @@ class CountInfo(ctypes.Structure):
 
 class PhaseTimes(ctypes.Structure):
     _fields_ = [("orient_ms", ctypes.c_float), ("count_ms", ctypes.c_float), ("launches", _i32)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("updates", _i64), ("inserted", _i64), ("deleted", _i64), ("ignored", _i64),
+                ("triangles_added", _i64), ("triangles_removed", _i64), ("status", _i32)]
 
 
 class TcError(RuntimeError):
@@ -74,6 +84,22 @@ SIGNATURES = {
     "tc_count_csr64": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
                                       ctypes.POINTER(Sched), _P]),
     "tc_workspace_status": (ctypes.c_int, [_P, ctypes.POINTER(CountInfo)]),
+    "tc_apply_batch": (ctypes.c_int, [_P, _P, _P, _P, _i64, ctypes.c_int, _P, _P, ctypes.POINTER(BatchInfo),
+                                      ctypes.POINTER(Sched), _P]),
+    "tc_batch_sort": (ctypes.c_int, [_i32, _P, _P, _i64, _P, _P, _P]),
+    "tc_insert_sorted": (ctypes.c_int, [_P, _P, _P, _i64, _P, ctypes.POINTER(_i64), _P]),
+    "tc_delete_sorted": (ctypes.c_int, [_P, _P, _P, _P, _i64, _P]),
+    "tc_count_batch": (ctypes.c_int, [_P, _P, _P, _P, _P, _i64, ctypes.c_int, _P, _P, ctypes.POINTER(Sched), _P]),
+    "tc_autotune_static": (ctypes.c_int, [_P, ctypes.c_int, _P, _i32, ctypes.POINTER(Sched),
+                                          ctypes.POINTER(ctypes.c_float), _P]),
+    "tc_autotune_lookup": (ctypes.c_int, [_i32, _i64, _i32, ctypes.POINTER(Sched)]),
+    "tc_autotune_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "tc_autotune_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "tc_mlp_init": (ctypes.c_int, [_P, ctypes.c_uint64]),
+    "tc_mlp_forward": (ctypes.c_int, [_P, _P, _i32, _P, _P]),
+    "tc_mlp_backward": (ctypes.c_int, [_P, _P, _P, _P, _i32, _P, _P, _P]),
+    "tc_mlp_adam_step": (ctypes.c_int, [_P, _P, _P, _P, _i32, ctypes.c_float, _P]),
+    "tc_mlp_train": (ctypes.c_int, [_P, _P, _P, _P, _i32, _i32, ctypes.c_float, _P, _P]),
     "tc_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "tc_profile_last": (ctypes.c_int, [ctypes.POINTER(PhaseTimes)]),
 }

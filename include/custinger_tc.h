@@ -131,6 +131,94 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
 /* Read back the info of the last stateless count on the current device. Syncs `stream`. */
 tc_status tc_workspace_status(void* stream, tc_count_info* info);
 
+/* ---- streaming updates ------------------------------------------------------------------ */
+
+/* What one batch did, read back on request. */
+typedef struct tc_batch_info {
+  int64_t updates;           /* pairs submitted */
+  int64_t inserted;          /* undirected edges inserted */
+  int64_t deleted;           /* undirected edges deleted */
+  int64_t ignored;           /* self-loops, repeats, inserts of present / deletes of absent edges */
+  int64_t triangles_added;   /* triangles created by the insertions */
+  int64_t triangles_removed; /* triangles destroyed by the deletions */
+  int32_t status;
+} tc_batch_info;
+
+/* Apply a batch of b undirected edge updates {src[i], dst[i]} (host or device arrays per `mem`;
+ * is_delete[i] != 0 marks a deletion, NULL = all insertions) and count the triangles they
+ * create and destroy. Set semantics: an edge is present or absent; repeats, self-loops,
+ * insertions of present edges and deletions of absent edges are ignored; within a batch all
+ * deletions apply before all insertions.
+ *   per_vertex:  optional device int32[nv], accumulated: += 2 (t_after(v) - t_before(v))
+ *   delta_dev:   optional device int64, accumulated: += T_after - T_before
+ *   info:        optional host struct (the call then synchronises `stream`)
+ * The call synchronises once per batch to size list relocations. */
+tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, const uint8_t* is_delete, int64_t b,
+                         int mem, int32_t* per_vertex, int64_t* delta_dev, tc_batch_info* info, const tc_sched* sched,
+                         void* stream);
+
+/* The cuStinger batch steps on directed entries in device memory (a batch is expected to be
+ * symmetric: both directions of every edge).
+ * tc_batch_sort:     sort (src, dst) in place by (src, dst); offsets[nv+1] = batch CSR over src;
+ *                    dup[i] = 1 for self-loops and repeats of an earlier entry (sortDeviceBUD).
+ * tc_insert_sorted:  insert the entries with dup == 0, flagging (dup = 1) those already present
+ *                    (edgeInsertionsSorted); *not_fitting = entries whose list had to move.
+ * tc_delete_sorted:  delete the entries with dup == 0 that are present (edgeDeletionsSorted).
+ * tc_count_batch:    after an insertion (sign = +1): per_vertex[v] += 2 for each vertex of each
+ *                    triangle containing a batch entry with dup == 0 (callDeviceNewTriangles);
+ *                    before a deletion (sign = -1): the same for the triangles the deletion
+ *                    destroys, subtracted. delta_dev (optional) += sign * triangles. */
+tc_status tc_batch_sort(int32_t nv, int32_t* d_src, int32_t* d_dst, int64_t b, int32_t* d_offsets, int32_t* d_dup,
+                        void* stream);
+tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, int64_t b, int32_t* d_dup,
+                           int64_t* not_fitting, void* stream);
+tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, const int32_t* d_dup, int64_t b,
+                           void* stream);
+tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, const int32_t* d_offsets,
+                         const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
+                         const tc_sched* sched, void* stream);
+
+/* ---- autotuner --------------------------------------------------------------------------- */
+
+/* Time the candidate scheduler settings (out-degree threshold of the warp path, search ratio,
+ * work-queue chunk, CTAs per SM) on this graph, `reps` timed runs each after one warm-up, and
+ * return the fastest in *best (its median time in *best_ms). The result is also cached under
+ * the graph's (log2 n, log2 m, log2 max out-degree) bucket. */
+tc_status tc_autotune_static(tc_graph* g, int pv_mode, int32_t* per_vertex, int32_t reps, tc_sched* best,
+                             float* best_ms, void* stream);
+/* Cached setting for a graph bucket (TC_ERR_STATE and the default heuristic when none). */
+tc_status tc_autotune_lookup(int32_t nv, int64_t edges, int32_t max_out_degree, tc_sched* out);
+/* Save / load the cache as text (one line per bucket). */
+tc_status tc_autotune_save(const char* path);
+tc_status tc_autotune_load(const char* path);
+
+/* ---- learned scheduler: a 3-layer FP32 MLP trained and evaluated on the GPU ------------------ */
+
+/* features (log2(1+d_a), log2(1+d_b), d_min/d_max, cell id / 255) -> 64 -> 64 -> one predicted
+ * log2 cost (ns per edge) per strategy. Parameters are TC_MLP_PARAMS floats, layout
+ * W1[64][4] b1[64] W2[64][64] b2[64] W3[3][64] b3[3]. */
+#define TC_MLP_IN 4
+#define TC_MLP_HIDDEN 64
+#define TC_MLP_OUT 3
+#define TC_MLP_PARAMS                                                                                 \
+  (TC_MLP_HIDDEN * TC_MLP_IN + TC_MLP_HIDDEN + TC_MLP_HIDDEN * TC_MLP_HIDDEN + TC_MLP_HIDDEN +         \
+   TC_MLP_OUT * TC_MLP_HIDDEN + TC_MLP_OUT)
+
+/* Deterministic He-uniform initialisation into a host array of TC_MLP_PARAMS floats. */
+tc_status tc_mlp_init(float* params_host, uint64_t seed);
+/* y[n][TC_MLP_OUT] = MLP(x[n][TC_MLP_IN]) (device arrays). */
+tc_status tc_mlp_forward(const float* d_params, const float* d_x, int32_t n, float* d_y, void* stream);
+/* Gradient of the masked MSE mean_i (y_i[strategy_i] - label_i)^2 into d_grad (TC_MLP_PARAMS
+ * floats, overwritten) and the loss into d_loss[0]. */
+tc_status tc_mlp_backward(const float* d_params, const float* d_x, const int32_t* d_strategy, const float* d_label,
+                          int32_t n, float* d_grad, float* d_loss, void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8; step counts from 1). */
+tc_status tc_mlp_adam_step(float* d_params, const float* d_grad, float* d_m, float* d_v, int32_t step, float lr,
+                           void* stream);
+/* Full-batch Adam for `epochs` steps; the final loss goes to *loss_host (optional, syncs). */
+tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strategy, const float* d_label, int32_t n,
+                       int32_t epochs, float lr, float* loss_host, void* stream);
+
 /* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching
  * stream around the orientation passes and around the intersection kernel (off by default;
  * recording adds no synchronisation). */

@@ -40,6 +40,8 @@ def lib():
         L.oracle_new_triangles.argtypes = [i32, _P, _P, _P, _P]
         L.oracle_sort_batch.argtypes = [i32, _P, _P, i64, _P, _P, _P, _P]
         L.oracle_fast_count.argtypes = [i32, _P, _P, ctypes.c_int, _P, _P]
+        L.oracle_fast_count_shard.argtypes = [i32, _P, _P, ctypes.c_int, i32, i32, _P, _P]
+        L.oracle_fast_count_shard.restype = None
         L.oracle_host_count_sample.argtypes = [i32, _P, _P, _P, i32, ctypes.c_int]
         L.oracle_host_count_sample.restype = i64
         for f in ("oracle_host_count_triangles", "oracle_static_per_vertex", "oracle_csr_per_vertex",
@@ -185,3 +187,12 @@ def sample_count(n, off, ind, verts, nthreads=0):
     verts = np.ascontiguousarray(verts, dtype=np.int32)
     return int(lib().oracle_host_count_sample(n, _ptr(off), _ptr(ind), _ptr(verts) if verts.size else None,
                                               verts.size, nthreads))
+
+
+def fast_count_shard(n, off, ind, shard, nshards, nthreads=0):
+    """Total (6T share) and per-vertex counts of one vertex shard of the oriented count."""
+    off, ind = _g(off, ind)
+    tot = np.zeros(1, np.int64)
+    pv = np.zeros(max(n, 1), np.int32)
+    lib().oracle_fast_count_shard(n, _ptr(off), _ptr(ind), nthreads, shard, nshards, _ptr(tot), _ptr(pv))
+    return int(tot[0]), pv[:n]

@@ -214,6 +214,11 @@ static inline int precedes(const int64_t* off, int32_t u, int32_t v) {
 
 void oracle_fast_count(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads,
                        int64_t* total, int32_t* per_vertex) {
+  oracle_fast_count_shard(nv, off, ind, nthreads, 0, 1, total, per_vertex);
+}
+
+void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
+                             int32_t nshards, int64_t* total, int32_t* per_vertex) {
 #ifdef _OPENMP
   int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
 #else
@@ -242,6 +247,7 @@ void oracle_fast_count(int32_t nv, const int64_t* off, const int32_t* ind, int n
   int64_t tri = 0;
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 64) reduction(+ : tri)
   for (int32_t u = 0; u < nv; ++u) {
+    if (nshards > 1 && u % nshards != shard) continue;
     const int32_t* a = pind + poff[u];
     int64_t al = poff[u + 1] - poff[u];
     uint32_t tu = 0;

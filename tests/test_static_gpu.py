@@ -163,3 +163,22 @@ def test_export_roundtrip():
     assert np.array_equal(off, g.off) and np.array_equal(ind, g.ind)
     n, used, alloc = graph.info()
     assert n == g.n and used == g.m and alloc >= used
+
+
+@pytest.mark.parametrize("nshards", [2, 3])
+def test_shards_sum_to_full(nshards):
+    torch = _torch()
+    g = golden_graph("rmat12_ef16_s2")
+    rec = GOLD["rmat12_ef16_s2"]
+    graph = api.Graph.from_csr(g)
+    total = 0
+    acc = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    for sh in range(nshards):
+        out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+        T, _ = graph.count(N.TC_PV_HANDLE, out, sched=sched(shard=sh, nshards=nshards))
+        tot_o, pv_o = O.fast_count_shard(g.n, g.off, g.ind, sh, nshards)
+        assert 6 * T == tot_o and np.array_equal(out[: g.n].cpu().numpy(), pv_o)
+        total += T
+        acc += out
+    assert total == rec["triangles"]
+    assert digest(acc[: g.n].cpu().numpy()) == rec["per_vertex_handle_digest"]
