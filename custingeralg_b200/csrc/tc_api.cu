@@ -133,6 +133,13 @@ GlobalWs& global_ws() {
   return *g;
 }
 
+#ifdef TC_DEBUG_PROGRESS
+extern "C" volatile int tc_dbg_host_stage;
+#define TC_DBG_STAGE(x) (tc_dbg_host_stage = (x))
+#else
+#define TC_DBG_STAGE(x) ((void)0)
+#endif
+
 template <class View, typename OffT>
 tc_status count_csr(int32_t nv, const OffT* d_off, const int32_t* d_ind, int pv_mode, int32_t* per_vertex,
                     int64_t* triangles_dev, tc_count_info* info, const tc_sched* sched, void* stream) {
@@ -146,18 +153,26 @@ tc_status count_csr(int32_t nv, const OffT* d_off, const int32_t* d_ind, int pv_
   TC_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
   OffT m_h = 0;
+  TC_DBG_STAGE(101);
   if (nv > 0) {
     TC_CUDA_TRY(cudaMemcpyAsync(&m_h, d_off + nv, sizeof(OffT), cudaMemcpyDeviceToHost, s));
     TC_CUDA_TRY(cudaStreamSynchronize(s));
   }
+  TC_DBG_STAGE(102);
   if (m_h < 0) return fail(TC_ERR_BAD_GRAPH, "negative edge count");
   GlobalWs& g = global_ws();
   std::lock_guard<std::mutex> lk(g.mu);
   Workspace& ws = g.ws[dev];
   TC_TRY(ws.ensure(nv, (int64_t)m_h));
   View view{d_off, d_ind};
+  TC_DBG_STAGE(103);
   TC_TRY(static_count(view, nv, (int64_t)m_h, ws, pv_mode, per_vertex, triangles_dev, to_params(sched), s));
-  if (info) return read_info(ws, s, info);
+  TC_DBG_STAGE(104);
+  if (info) {
+    tc_status r = read_info(ws, s, info);
+    TC_DBG_STAGE(105);
+    return r;
+  }
   return TC_OK;
 }
 }  // namespace
@@ -199,6 +214,7 @@ void tc_sched_default(tc_sched* s) {
   s->use_table = 0;
   s->shard = 0;
   s->nshards = 1;
+  s->cell_filter = -1;
 }
 
 tc_status tc_count_csr32(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode, int32_t* per_vertex,

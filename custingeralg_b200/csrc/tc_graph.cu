@@ -272,11 +272,27 @@ tc_status tc_count_static(tc_graph* g, int pv_mode, int32_t* per_vertex, int64_t
   if (pv_mode != TC_PV_NONE && g->n > 0 && !per_vertex)
     return fail(TC_ERR_INVALID_ARG, "per_vertex output required for mode %d", pv_mode);
   cudaStream_t s = (cudaStream_t)stream;
+#ifdef TC_DEBUG_PROGRESS
+  extern volatile int tc_dbg_host_stage;
+  tc_dbg_host_stage = 201;
+#endif
   TC_TRY(g->ws.ensure(g->n, g->m));
   SlackView view{g->start, g->used, g->pool};
   TC_TRY(static_count(view, g->n, g->m, g->ws, pv_mode, per_vertex, triangles_dev, to_params(sched), s));
+#ifdef TC_DEBUG_PROGRESS
+  tc_dbg_host_stage = 202;
+#endif
   if (info) return read_info(g->ws, s, info);
   return TC_OK;
 }
 
 }  // extern "C"
+
+extern "C" tc_status tc_cell_stats(tc_graph* g, double* out_host, void* stream) {
+  if (!g || !out_host) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  tc_sched none;
+  tc_sched_default(&none);
+  none.cell_filter = -2;  // build the orientation, intersect nothing
+  TC_TRY(tc_count_static(g, TC_PV_NONE, nullptr, nullptr, nullptr, &none, stream));
+  return cell_stats(g->n, g->ws, out_host, (cudaStream_t)stream);
+}

@@ -87,6 +87,7 @@ struct SchedParams {
   int32_t blocks_per_sm;   // 0 = occupancy limit
   int32_t shard;           // count source vertices u with u % nshards == shard
   int32_t nshards;
+  int32_t cell_filter;     // -1 all edges, -2 none, >= 0 only that degree cell
   uint8_t table[16][16];
 };
 
@@ -129,6 +130,9 @@ tc_status validate_view(const View& view, int32_t n, Workspace& ws, cudaStream_t
 // Phase events of the calling thread (tc_profile_enable). Each is a no-op when disabled.
 void prof_mark(int point, cudaStream_t stream);   // 0 = start, 1 = orientation done, 2 = count done
 void prof_launches(int n);
+
+// Oriented-edge statistics per degree cell (needs the orientation in ws): 256 x 4 doubles.
+tc_status cell_stats(int32_t n, Workspace& ws, double* out_host, cudaStream_t stream);
 
 // Read back a count's info (syncs the stream).
 tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* info);

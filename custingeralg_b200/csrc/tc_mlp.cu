@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "tc_internal.cuh"
 
@@ -258,6 +259,45 @@ tc_status tc_mlp_adam_step(float* d_params, const float* d_grad, float* d_m, flo
   k_adam<<<(kParams + 255) / 256, 256, 0, (cudaStream_t)stream>>>(d_params, d_grad, d_m, d_v, kParams, lr, b1, b2, eps,
                                                                   c1, c2);
   TC_CUDA_TRY(cudaGetLastError());
+  return TC_OK;
+}
+
+tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* sch, void* stream) {
+  if (!d_params || !sch || (kind != 0 && kind != 1)) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  std::vector<float> feat(256 * kIn);
+  for (int c = 0; c < 256; ++c) {
+    if (cell_features) {
+      for (int k = 0; k < kIn; ++k) feat[c * kIn + k] = cell_features[c * kIn + k];
+    } else {
+      const double a = 1.5 * (double)(1 << (c / 16)), b = 1.5 * (double)(1 << (c % 16));
+      feat[c * kIn + 0] = (float)std::log2(1.0 + a);
+      feat[c * kIn + 1] = (float)std::log2(1.0 + b);
+      feat[c * kIn + 2] = (float)(std::min(a, b) / std::max(a, b));
+      feat[c * kIn + 3] = (float)c / 255.f;
+    }
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  float *dx = nullptr, *dy = nullptr;
+  TC_CUDA_TRY(cudaMalloc(&dx, sizeof(float) * feat.size()));
+  TC_CUDA_TRY(cudaMalloc(&dy, sizeof(float) * 256 * kOut));
+  std::vector<float> y(256 * kOut);
+  tc_status rc = TC_OK;
+  if (cudaMemcpyAsync(dx, feat.data(), sizeof(float) * feat.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = fail(TC_ERR_CUDA, "copy failed");
+  if (rc == TC_OK) rc = tc_mlp_forward(d_params, dx, 256, dy, stream);
+  if (rc == TC_OK && (cudaMemcpyAsync(y.data(), dy, sizeof(float) * y.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+    rc = fail(TC_ERR_CUDA, "copy failed");
+  cudaFree(dx);
+  cudaFree(dy);
+  if (rc != TC_OK) return rc;
+  // strategy ids: 0 = hash probe, 1 = binary search, 2 = merge; static chooses {0, 1}, streaming {1, 2}
+  const int s0 = kind == 0 ? 0 : 1, s1 = kind == 0 ? 1 : 2;
+  for (int c = 0; c < 256; ++c) {
+    const float c0 = y[c * kOut + s0], c1 = y[c * kOut + s1];
+    sch->table[c / 16][c % 16] = (uint8_t)(c1 < c0 ? 1 : 0);
+  }
+  sch->use_table = 1;
   return TC_OK;
 }
 

@@ -15,8 +15,8 @@
 //     as an open-addressing hash set (chunks of 2048 entries). All other vertices with
 //     d+ >= 2 are taken one per warp with a warp-private 64-slot hash set. For each group of
 //     32 out-neighbours v of u the warp streams the concatenation of their lists N+(v) with
-//     coalesced loads (segment boundaries found with one __reduce_or_sync per 32 elements)
-//     and probes every element into the hash set ("probe" strategy), or, for an edge whose
+//     coalesced loads (each lane walks its own segment pointer; no warp collective inside the
+//     data-dependent loop) and probes every element into the hash set ("probe" strategy), or, for an edge whose
 //     N+(v) is long next to N+(u), binary-searches the elements of N+(u) into N+(v)
 //     ("search" strategy). The scheduler picks the strategy per edge.
 //  3. Per-vertex counts never take a global atomic per triangle: the three vertices of a
@@ -27,6 +27,11 @@
 #include <cstring>
 
 #include "tc_internal.cuh"
+
+#ifdef TC_DEBUG_PROGRESS
+extern "C" void* tc_dbg_progress_host_dev;
+extern "C" size_t tc_dbg_progress_bytes;
+#endif
 
 namespace tc {
 
@@ -48,6 +53,7 @@ struct WarpSmem {
   int64_t seg_base[kWarp];
   int32_t seg_v[kWarp];
   uint32_t seg_cnt[kWarp];
+  int32_t seg_start[kWarp];
   int8_t hidx[kSmallSlots];
 };
 
@@ -61,6 +67,35 @@ struct CountSmem {
   unsigned item;
   int gctr;
 };
+
+#ifdef TC_DEBUG_PROGRESS
+// Debug builds only: per-warp progress words and per-kernel entry/exit counters in host-mapped
+// memory, readable while a kernel runs.
+__device__ unsigned long long* tc_dbg_progress = nullptr;
+__device__ unsigned long long* tc_dbg_kern = nullptr;
+#define TC_DBG_MARK(idx, val)                                                              \
+  do {                                                                                     \
+    if (tc_dbg_progress) ((volatile unsigned long long*)tc_dbg_progress)[(idx)] = (val);  \
+  } while (0)
+#define TC_DBG_ENTER(id)                                                                   \
+  do {                                                                                     \
+    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id)], 1ull);    \
+  } while (0)
+#define TC_DBG_EXIT(id)                                                                    \
+  do {                                                                                     \
+    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id) + 1], 1ull); \
+  } while (0)
+#else
+#define TC_DBG_MARK(idx, val) \
+  do {                        \
+  } while (0)
+#define TC_DBG_ENTER(id) \
+  do {                   \
+  } while (0)
+#define TC_DBG_EXIT(id) \
+  do {                  \
+  } while (0)
+#endif
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned r;
@@ -177,8 +212,10 @@ __device__ __forceinline__ void process_group(
   const int32_t v = valid ? (in_chunk ? sA[li] : __ldg(Ag + i)) : 0;
   const int b = valid ? __ldg(dplus + v) : 0;
   const int64_t base = valid ? __ldg(offp + v) : 0;
-  const bool srch = valid && b > 0 && use_search(sp, chunk_len, b);
-  const int pb = (valid && !srch) ? b : 0;
+  const bool active = valid && b > 0 &&
+                      (sp.cell_filter == -1 || (sp.cell_filter >= 0 && log2_cell(chunk_len) * 16 + log2_cell(b) == sp.cell_filter));
+  const bool srch = active && use_search(sp, chunk_len, b);
+  const int pb = (active && !srch) ? b : 0;
 
   // ---- probe strategy: stream the concatenated lists N+(v), probe into the hash set ----
   int incl = pb;
@@ -196,30 +233,31 @@ __device__ __forceinline__ void process_group(
     ws.seg_base[rank] = base - P;
     ws.seg_v[rank] = v;
     ws.seg_cnt[rank] = 0;
+    ws.seg_start[rank] = P;
   }
   __syncwarp();
-  int carry = 0;
-  for (int k0 = 0; k0 < total; k0 += kWarp) {
-    const unsigned bit = (pb > 0 && P >= k0 && P < k0 + kWarp) ? (1u << (P - k0)) : 0u;
-    const unsigned starts = __reduce_or_sync(kFull, bit);
-    const int r = carry + __popc(starts & (lt | (1u << lane))) - 1;
-    carry += __popc(starts);
-    const int k = k0 + lane;
-    if (k < total) {
-      const int32_t w = __ldg(indp + ws.seg_base[r] + k);
-      const int s = hash_find(hkeys, bits, w);
-      if (s >= 0) {
-        ++tri;
-        if (PV != TC_PV_NONE) {
-          uint32_t wu, wv, ww;
-          tri_weights<PV>(u, ws.seg_v[r], w, wu, wv, ww);
-          u_acc += wu;
-          if (ww) atomicAdd(&cnt[hidx[s]], ww);
-          if (wv) atomicAdd(&ws.seg_cnt[r], wv);
-        }
+  // Each lane walks the flat index k = lane, lane + 32, ... and advances its own segment
+  // pointer (segments are contiguous and ascending), so the loop holds no warp collective.
+  const int nseg = __popc(segmask);
+  int r = 0;
+  for (int k = lane; k < total; k += kWarp) {
+    if (lane == 0) TC_DBG_MARK(((blockIdx.x * kWarps + threadIdx.x / kWarp) * 4 + 2),
+                               ((unsigned long long)(unsigned)total << 32) | (unsigned)k);
+    while (r + 1 < nseg && ws.seg_start[r + 1] <= k) ++r;
+    const int32_t w = __ldg(indp + ws.seg_base[r] + k);
+    const int s = hash_find(hkeys, bits, w);
+    if (s >= 0) {
+      ++tri;
+      if (PV != TC_PV_NONE) {
+        uint32_t wu, wv, ww;
+        tri_weights<PV>(u, ws.seg_v[r], w, wu, wv, ww);
+        u_acc += wu;
+        if (ww) atomicAdd(&cnt[hidx[s]], ww);
+        if (wv) atomicAdd(&ws.seg_cnt[r], wv);
       }
     }
   }
+  __syncwarp();
 
   // ---- search strategy: binary-search the chunk's entries into N+(v) ----
   unsigned sm = __ballot_sync(kFull, srch);
@@ -244,6 +282,7 @@ __device__ __forceinline__ void process_group(
         }
       }
     }
+    __syncwarp();
     if (PV != TC_PV_NONE) {
       vacc = warp_sum(vacc);
       if (lane == 0 && vacc) {
@@ -271,6 +310,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
                                                     const int32_t* __restrict__ large,
                                                     uint32_t* __restrict__ out, DevStatus* __restrict__ st,
                                                     const SchedParams sp) {
+  TC_DBG_ENTER(6);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CountSmem& sm = *reinterpret_cast<CountSmem*>(smem_raw);
   const int lane = threadIdx.x & (kWarp - 1);
@@ -281,11 +321,13 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
   // Phase 1: large out-degree vertices, one CTA each, in chunks of kChunk staged entries.
   while (true) {
     if (threadIdx.x == 0) sm.item = atomicAdd(&st->q_large, 1u);
+    __syncwarp();
     __syncthreads();
     const unsigned item = sm.item;
     __syncthreads();
     if (item >= n_large) break;
     const int32_t u = large[item];
+    if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (1ull << 60) | ((unsigned long long)item << 32) | (unsigned)u);
     const int32_t a = dplus[u];
     const int32_t* Ag = indp + offp[u];
     uint32_t u_acc = 0;
@@ -300,18 +342,23 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
         sm.cnt[j] = 0;
       }
       if (threadIdx.x == 0) sm.gctr = 0;
+      __syncwarp();
       __syncthreads();
       for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(sm.hkeys, sm.hidx, bits, sm.sA[j], j);
+      __syncwarp();
       __syncthreads();
       const int ngroups = (a + kWarp - 1) / kWarp;
       while (true) {
         int g = 0;
         if (lane == 0) g = atomicAdd(&sm.gctr, 1);
+        __syncwarp();
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
+        if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4 + 1, ((unsigned long long)cb << 32) | (unsigned)g);
         process_group<PV>(u, Ag, sm.sA, cb, clen, sm.hkeys, sm.hidx, bits, sm.cnt, g * kWarp,
                           min(kWarp, a - g * kWarp), dplus, offp, indp, out, sm.warp[wid], sp, tri, u_acc);
       }
+      __syncwarp();
       __syncthreads();
       if (PV != TC_PV_NONE) {
         for (int j = threadIdx.x; j < clen; j += kThreads) {
@@ -319,6 +366,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
           if (c) atomicAdd(&out[sm.sA[j]], c * flush_mult<PV>());
         }
       }
+      __syncwarp();
       __syncthreads();
     }
     if (PV != TC_PV_NONE) {
@@ -332,6 +380,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
   while (true) {
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(&st->q_small, (unsigned long long)sp.chunk);
+    __syncwarp();
     c0 = __shfl_sync(kFull, c0, 0);
     if (c0 >= (unsigned long long)n) break;
     const int32_t cend = (int32_t)min((unsigned long long)n, c0 + (unsigned long long)sp.chunk);
@@ -344,6 +393,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
         elig &= elig - 1;
         const int32_t u = ub + sl;
         const int a = __shfl_sync(kFull, aa, sl);
+        if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (2ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
         const int32_t* Ag = indp + __ldg(offp + u);
         ws.hkeys[lane] = -1;
         ws.hkeys[lane + kWarp] = -1;
@@ -364,6 +414,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
             const uint32_t c = ws.cnt[lane];
             if (c) atomicAdd(&out[x], c * flush_mult<PV>());
           }
+          __syncwarp();
           u_acc = warp_sum(u_acc);
           if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
         }
@@ -372,7 +423,9 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
     }
   }
 
+  if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4 + 3, 1ull);
   // One global atomic per CTA for the triangle total.
+  __syncwarp();
   unsigned long long t = warp_sum((unsigned long long)tri);
   if (lane == 0) sm.tri[wid] = t;
   __syncthreads();
@@ -381,6 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
     for (int w = 0; w < kWarps; ++w) s += sm.tri[w];
     if (s) atomicAdd(&st->triangles, s);
   }
+  TC_DBG_EXIT(6);
 }
 
 // ---- orientation ------------------------------------------------------------------------
@@ -392,6 +446,7 @@ __device__ __forceinline__ bool precedes(int32_t du, int32_t u, int32_t dv, int3
 template <class View>
 __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_t n, int32_t* __restrict__ dplus,
                                                       DevStatus* __restrict__ st) {
+  TC_DBG_ENTER(1);
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
@@ -423,6 +478,7 @@ __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_
           chk += (u < v) ? h : (0ull - h);
         }
       }
+      __syncwarp();
       cnt += __popc(__ballot_sync(kFull, pred));
     }
     if (lane == 0) {
@@ -431,6 +487,7 @@ __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_
       mx = max(mx, (unsigned)cnt);
     }
   }
+  __syncwarp();
   chk = warp_sum(chk);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
@@ -440,6 +497,7 @@ __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_
     if (ei) atomicAdd(&st->edges_intersected, ei);
     if (mx) atomicMax(&st->max_dplus, mx);
   }
+  TC_DBG_EXIT(1);
 }
 
 template <class View>
@@ -448,6 +506,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
                                                      const int64_t e_cap, int32_t* __restrict__ large,
                                                      DevStatus* __restrict__ st, const int warp_max,
                                                      const int shard, const int nshards) {
+  TC_DBG_ENTER(5);
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
@@ -476,6 +535,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
         v = g.ind[s + k];
         if (v >= 0 && v < n) pred = precedes(d, u, g.len(v), v);
       }
+      __syncwarp();
       const unsigned msk = __ballot_sync(kFull, pred);
       const int at = pos + __popc(msk & lt);
       if (pred && at < a) {
@@ -484,6 +544,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
       }
       pos += __popc(msk);
     }
+    __syncwarp();
     ws = warp_sum(ws);
     if (lane == 0) work += ws + (unsigned long long)a * (unsigned long long)a;
     if (a > warp_max && (u % nshards) == shard) {
@@ -491,6 +552,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
       if (++nbuf == kWarp) {
         unsigned at = 0;
         if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)kWarp);
+        __syncwarp();
         at = __shfl_sync(kFull, at, 0);
         large[at + lane] = buf;
         nbuf = 0;
@@ -500,6 +562,7 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
   if (nbuf) {
     unsigned at = 0;
     if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)nbuf);
+    __syncwarp();
     at = __shfl_sync(kFull, at, 0);
     if (lane < nbuf) large[at + lane] = buf;
   }
@@ -509,12 +572,14 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
     if (work) atomicAdd(&st->oriented_work, work);
     if (bad) atomicOr(&st->bad_flags, bad);
   }
+  TC_DBG_EXIT(5);
 }
 
 // ---- exclusive scan of int32 counts into int64 offsets ------------------------------------
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const int32_t* __restrict__ in, const int64_t n,
                                                                  int64_t* __restrict__ tile_sums) {
+  TC_DBG_ENTER(2);
   __shared__ long long red[kScanThreads / kWarp];
   const int64_t base = (int64_t)blockIdx.x * kScanTile;
   long long s = 0;
@@ -530,10 +595,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tile_sums(const int32_t* 
     for (int w = 0; w < kScanThreads / kWarp; ++w) t += red[w];
     tile_sums[blockIdx.x] = t;
   }
+  TC_DBG_EXIT(2);
 }
 
 // Single CTA: exclusive scan of tile_sums[0..ntiles) in place, total into tile_sums[ntiles].
 __global__ void __launch_bounds__(1024) k_scan_tile_prefix(int64_t* __restrict__ tile_sums, const int64_t ntiles) {
+  TC_DBG_ENTER(3);
   __shared__ long long wsum[32];
   __shared__ long long carry_s;
   const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
@@ -568,11 +635,13 @@ __global__ void __launch_bounds__(1024) k_scan_tile_prefix(int64_t* __restrict__
     __syncthreads();
   }
   if (threadIdx.x == 0) tile_sums[ntiles] = carry_s;
+  TC_DBG_EXIT(3);
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int32_t* __restrict__ in, const int64_t n,
                                                              const int64_t* __restrict__ tile_sums,
                                                              int64_t* __restrict__ out, const int64_t ntiles) {
+  TC_DBG_ENTER(4);
   __shared__ long long wsum[kScanThreads / kWarp];
   const int lane = threadIdx.x & 31, wid = threadIdx.x / 32;
   const int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanPer;
@@ -602,6 +671,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_tiles(const int32_t* __re
     run += v[k];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) out[n] = tile_sums[ntiles];
+  TC_DBG_EXIT(4);
 }
 
 int orient_grid(int64_t n) {
@@ -627,6 +697,9 @@ tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const Sche
   }
   const int bps = sp.blocks_per_sm > 0 ? std::min(sp.blocks_per_sm, blocks_per_sm[dev]) : blocks_per_sm[dev];
   const int grid = device_info().sms * bps;
+#ifdef TC_DEBUG_PROGRESS
+  if (tc_dbg_progress_host_dev) cudaMemsetAsync(tc_dbg_progress_host_dev, 0, tc_dbg_progress_bytes, stream);
+#endif
   k_count<PV><<<grid, kThreads, smem, stream>>>(n, ws.dplus, ws.offp, ws.indp, ws.large, out, ws.st, sp);
   TC_CUDA_TRY(cudaGetLastError());
   return TC_OK;
@@ -662,6 +735,7 @@ SchedParams to_params(const tc_sched* s) {
   p.chunk = std::max(32, (s->chunk + 31) / 32 * 32);
   p.blocks_per_sm = std::max(0, s->blocks_per_sm);
   p.nshards = std::max(1, s->nshards);
+  p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
   p.shard = std::min(std::max(0, s->shard), p.nshards - 1);
   memcpy(p.table, s->table, sizeof(p.table));
   return p;
@@ -736,6 +810,49 @@ tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* inf
 
 namespace tc {
 
+namespace {
+// Warp per source vertex: per degree-cell sums over its oriented edges, in shared memory, then
+// one atomic per touched cell per CTA.
+__global__ void __launch_bounds__(256) k_cell_stats(const int32_t n, const int32_t* __restrict__ dplus,
+                                                    const int64_t* __restrict__ offp, const int32_t* __restrict__ indp,
+                                                    double* __restrict__ out) {
+  __shared__ double acc[256 * 4];
+  for (int i = threadIdx.x; i < 256 * 4; i += blockDim.x) acc[i] = 0.0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t uu = gw; uu < n; uu += nw) {
+    const int32_t a = dplus[uu];
+    const int64_t s = offp[uu];
+    const double la = log2(1.0 + a);
+    for (int32_t k = lane; k < a; k += 32) {
+      const int32_t b = dplus[indp[s + k]];
+      const int c = log2_cell(a) * 16 + log2_cell(b);
+      atomicAdd(&acc[4 * c + 0], 1.0);
+      atomicAdd(&acc[4 * c + 1], la);
+      atomicAdd(&acc[4 * c + 2], log2(1.0 + b));
+      atomicAdd(&acc[4 * c + 3], (double)min(a, b) / (double)max(max(a, b), 1));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256 * 4; i += blockDim.x)
+    if (acc[i] != 0.0) atomicAdd(&out[i], acc[i]);
+}
+}  // namespace
+
+tc_status cell_stats(int32_t n, Workspace& ws, double* out_host, cudaStream_t stream) {
+  double* d = nullptr;
+  TC_CUDA_TRY(cudaMalloc(&d, sizeof(double) * 1024));
+  cudaMemsetAsync(d, 0, sizeof(double) * 1024, stream);
+  if (n > 0) k_cell_stats<<<orient_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.offp, ws.indp, d);
+  cudaError_t e = cudaMemcpyAsync(out_host, d, sizeof(double) * 1024, cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(TC_ERR_CUDA, "cell stats: %s", cudaGetErrorString(e));
+  return TC_OK;
+}
+
 template <class View>
 tc_status validate_view(const View& view, int32_t n, Workspace& ws, cudaStream_t stream) {
   TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
@@ -750,3 +867,21 @@ template tc_status validate_view<SlackView>(const SlackView&, int32_t, Workspace
 template tc_status validate_view<Csr64View>(const Csr64View&, int32_t, Workspace&, cudaStream_t);
 
 }  // namespace tc
+
+#ifdef TC_DEBUG_PROGRESS
+extern "C" {
+volatile int tc_dbg_host_stage = 0;
+void* tc_dbg_progress_host_dev = nullptr;
+size_t tc_dbg_progress_bytes = 0;
+int tc_debug_get_stage(void) { return tc_dbg_host_stage; }
+int tc_debug_set_progress(void* dev_ptr, size_t bytes, void* kern_dev_ptr) {
+  unsigned long long* p = (unsigned long long*)dev_ptr;
+  unsigned long long* k = (unsigned long long*)kern_dev_ptr;
+  tc_dbg_progress_host_dev = dev_ptr;
+  tc_dbg_progress_bytes = bytes;
+  int e = (int)cudaMemcpyToSymbol(tc::tc_dbg_progress, &p, sizeof(p));
+  if (e) return e;
+  return (int)cudaMemcpyToSymbol(tc::tc_dbg_kern, &k, sizeof(k));
+}
+}
+#endif

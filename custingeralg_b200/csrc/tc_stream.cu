@@ -187,6 +187,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
       int64_t k = i0 + lane;
       while (true) {
         const bool same = k < nd_cap && dk[k] != kSentinel && (int32_t)(dk[k] >> 32) == v;
+        __syncwarp();
         const unsigned m = __ballot_sync(kFull, same);
         if (m != kFull) {
           i1 = k - lane + __ffs(~m) - 1;
@@ -205,7 +206,9 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
       const int32_t nc = slack_capacity(a + c, max(slack_q10, 256));
       unsigned long long at = 0;
       if (lane == 0) at = atomicAdd(pool_top, (unsigned long long)nc);
+      __syncwarp();
       at = __shfl_sync(kFull, at, 0);
+      __syncwarp();
       if ((int64_t)at + nc > pool_cap) {
         if (lane == 0) atomicOr(&st->err, kErrPool);
         continue;  // cannot happen when the host sized the pool from the demand pass
@@ -303,6 +306,7 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
     const int32_t v = vlist[k];
     unsigned old = 0;
     if (lane == 0) old = atomicMax(&claim[v], epoch);
+    __syncwarp();
     old = __shfl_sync(kFull, old, 0);
     if (old >= epoch) continue;
     const int64_t s = start[v];
@@ -316,6 +320,7 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
         val = pool[s + i];
         keep = mark[s + i] == 0;
       }
+      __syncwarp();
       const unsigned m = __ballot_sync(kFull, keep);
       __syncwarp();
       if (keep) pool[s + wp + __popc(m & lt)] = val;
@@ -354,7 +359,15 @@ struct DeltaArgs {
   uint32_t weight;   // per-vertex increment per counted triangle
   int search_ratio_x16;
   int only_present;  // skip entries whose edge is absent (cuStinger deletion count)
+  int use_table;     // per-cell strategy table: 0 = search, 1 = merge
+  int cell_filter;   // -1 all, -2 none, c >= 0 only edges of cell c (timing mode)
+  uint8_t table[256];
 };
+
+__device__ __forceinline__ int cell_of(int a, int b) {
+  const int ca = min(31 - __clz(max(a, 1)), 15), cb = min(31 - __clz(max(b, 1)), 15);
+  return ca * 16 + cb;
+}
 
 template <int PRED>
 __device__ __forceinline__ bool changed(const DeltaArgs& A, int32_t owner, int64_t slot_abs, int32_t w) {
@@ -409,6 +422,7 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
         const int64_t p = lower_bound(A.g.ind, sx, sx + lx, y);
         pres = p < sx + lx && A.g.ind[p] == y;
       }
+      __syncwarp();
       if (!__shfl_sync(kFull, pres, 0)) continue;
     }
     const uint64_t key = ekey(x, y);
@@ -428,8 +442,10 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
         atomicAdd(&pv[w], A.weight * (uint32_t)A.sign);
       }
     };
+    const int cell = cell_of(la, lb);
+    if (A.cell_filter == -2 || (A.cell_filter >= 0 && cell != A.cell_filter)) continue;
     const int lg = 32 - __clz(lb);
-    const bool search = 16LL * lb > (long long)A.search_ratio_x16 * la * lg;
+    const bool search = A.use_table ? A.table[cell] == 0 : 16LL * lb > (long long)A.search_ratio_x16 * la * lg;
     if (search) {
       for (int32_t i = lane; i < la; i += 32) {
         const int32_t w = L[sa + i];
@@ -448,6 +464,7 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
         }
       }
     }
+    __syncwarp();
     c = warp_sum(c);
     if (lane == 0 && c) {
       atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
@@ -456,6 +473,7 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
     }
   }
   if (lane == 0) s_tri[wid] = tri_acc;
+  __syncwarp();
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned long long s = 0;
@@ -677,6 +695,9 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
   A.g = SlackView{g->start, g->used, g->pool};
   A.mark = g->mark;
   A.search_ratio_x16 = sp.search_ratio_x16;
+  A.use_table = sp.use_table;
+  A.cell_filter = sp.cell_filter;
+  memcpy(A.table, sp.table, sizeof(A.table));
   return A;
 }
 

@@ -41,7 +41,7 @@ _i64 = ctypes.c_int64
 class Sched(ctypes.Structure):
     _fields_ = [("warp_max_deg", _i32), ("search_ratio_x16", _i32), ("blocks_per_sm", _i32),
                 ("chunk", _i32), ("use_table", _i32), ("table", (ctypes.c_uint8 * 16) * 16),
-                ("shard", _i32), ("nshards", _i32)]
+                ("shard", _i32), ("nshards", _i32), ("cell_filter", _i32)]
 
 
 class CountInfo(ctypes.Structure):
@@ -95,6 +95,8 @@ SIGNATURES = {
     "tc_autotune_lookup": (ctypes.c_int, [_i32, _i64, _i32, ctypes.POINTER(Sched)]),
     "tc_autotune_save": (ctypes.c_int, [ctypes.c_char_p]),
     "tc_autotune_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "tc_cell_stats": (ctypes.c_int, [_P, _P, _P]),
+    "tc_sched_learned": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(Sched), _P]),
     "tc_mlp_init": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "tc_mlp_forward": (ctypes.c_int, [_P, _P, _i32, _P, _P]),
     "tc_mlp_backward": (ctypes.c_int, [_P, _P, _P, _P, _i32, _P, _P, _P]),

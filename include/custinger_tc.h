@@ -67,6 +67,9 @@ typedef struct tc_sched {
   uint8_t table[16][16];  /* strategy per degree-cell: 0 = hash probe, 1 = binary search */
   int32_t shard;          /* count only triangles whose lowest vertex u has u % nshards == shard */
   int32_t nshards;        /* (multi-GPU work split; 1 = everything) */
+  int32_t cell_filter;    /* timing mode for scheduler training: -1 = intersect every edge (normal),
+                             -2 = none, c >= 0 = only edges of degree cell c (16*log2 d_a + log2 d_b);
+                             counts are partial unless -1 */
 } tc_sched;
 
 typedef struct tc_graph tc_graph;
@@ -178,6 +181,11 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
                          const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
                          const tc_sched* sched, void* stream);
 
+/* Per degree-cell statistics of the oriented edges u->v (cell = 16*min(15, log2 d+u) +
+ * min(15, log2 d+v)): out[4*c + 0..3] = edge count, sum of log2(1 + d+u), sum of log2(1 + d+v),
+ * sum of min/max of the two. Host array of 1024 doubles. Syncs. */
+tc_status tc_cell_stats(tc_graph* g, double* out_host, void* stream);
+
 /* ---- autotuner --------------------------------------------------------------------------- */
 
 /* Time the candidate scheduler settings (out-degree threshold of the warp path, search ratio,
@@ -218,6 +226,13 @@ tc_status tc_mlp_adam_step(float* d_params, const float* d_grad, float* d_m, flo
 /* Full-batch Adam for `epochs` steps; the final loss goes to *loss_host (optional, syncs). */
 tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strategy, const float* d_label, int32_t n,
                        int32_t epochs, float lr, float* loss_host, void* stream);
+
+/* Fill a scheduler from a trained MLP (device parameters): for every degree cell the
+ * strategy with the lowest predicted cost among those of `kind` (0 = static count: hash probe
+ * or search; 1 = streaming delta: search or merge) goes into s->table and s->use_table = 1.
+ * cell_features (host, 256 x TC_MLP_IN floats) are the features of each cell, e.g. from
+ * tc_cell_stats; NULL uses the cells' nominal degrees. */
+tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* s, void* stream);
 
 /* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching
  * stream around the orientation passes and around the intersection kernel (off by default;
