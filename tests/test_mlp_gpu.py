@@ -36,7 +36,8 @@ def test_forward_matches_oracle(n):
     p = init_params(3)
     X, _, _ = data(n)
     y = torch.zeros(n, N.MLP_OUT, dtype=torch.float32, device="cuda")
-    N.check(N.lib().tc_mlp_forward(_t(p).data_ptr(), _t(X).data_ptr(), n, y.data_ptr(), None))
+    dp, dx = _t(p), _t(X)  # keep the device tensors alive across the call
+    N.check(N.lib().tc_mlp_forward(dp.data_ptr(), dx.data_ptr(), n, y.data_ptr(), None))
     ref, _ = M.forward(p, X)
     np.testing.assert_allclose(y.cpu().numpy(), ref, rtol=1e-4, atol=1e-4)
 
@@ -48,8 +49,8 @@ def test_gradient_matches_oracle(n):
     X, s, lab = data(n, seed=n)
     g = torch.zeros(N.MLP_PARAMS, dtype=torch.float32, device="cuda")
     loss = torch.zeros(1, dtype=torch.float32, device="cuda")
-    dp = _t(p)
-    N.check(N.lib().tc_mlp_backward(dp.data_ptr(), _t(X).data_ptr(), _t(s).data_ptr(), _t(lab).data_ptr(), n,
+    dp, dx, ds, dl = _t(p), _t(X), _t(s), _t(lab)
+    N.check(N.lib().tc_mlp_backward(dp.data_ptr(), dx.data_ptr(), ds.data_ptr(), dl.data_ptr(), n,
                                     g.data_ptr(), loss.data_ptr(), None))
     ref_loss, ref_g = M.loss_and_grad(p, X, s, lab)
     assert abs(loss.item() - ref_loss) <= 1e-4 * max(1.0, abs(ref_loss))
@@ -62,10 +63,10 @@ def test_training_reduces_loss():
     import torch
     p = init_params(7)
     X, s, lab = data(4000, seed=11)
-    dp = _t(p)
+    dp, dx, ds, dl = _t(p), _t(X), _t(s), _t(lab)
     l0, _ = M.loss_and_grad(p, X, s, lab)
     out = ctypes.c_float()
-    N.check(N.lib().tc_mlp_train(dp.data_ptr(), _t(X).data_ptr(), _t(s).data_ptr(), _t(lab).data_ptr(), 4000, 400,
+    N.check(N.lib().tc_mlp_train(dp.data_ptr(), dx.data_ptr(), ds.data_ptr(), dl.data_ptr(), 4000, 400,
                                  3e-3, ctypes.byref(out), None))
     l1, _ = M.loss_and_grad(dp.cpu().numpy(), X, s, lab)
     assert abs(out.value - l1) < 1e-3 * max(1, l1)
