@@ -1,0 +1,113 @@
+// Static triangle count with no device allocation: the stateless raw-CSR count
+// (tc_count_csr32) with its working memory in a fixed array of this library's own device
+// memory instead of cudaMalloc'd buffers.
+//
+// Who needs it: code that runs where it cannot call cudaMalloc -- inside a captured CUDA
+// graph region, under an allocator that forbids device allocation after start-up, or from a
+// host that pre-plans every byte of device memory (a serving process with a fixed budget).
+// They still pass their own input CSR and output buffers.
+//
+// The array is sized for graphs of up to TC_NOALLOC_MAX_NV vertices and TC_NOALLOC_MAX_EDGES
+// directed edges (about 32 MB); every GPU that loads the library holds it until the process
+// exits. All calls share it: two calls that overlap on the GPU race and corrupt each other, so
+// serialise them (one stream, or events). The first call on a device looks up the array's
+// device address (cudaGetSymbolAddress) with that device current; make that first call before
+// any stream capture.
+#include <cstring>
+#include <mutex>
+
+#include "tc_internal.cuh"
+
+namespace tc {
+namespace {
+
+constexpr int64_t kMaxNv = TC_NOALLOC_MAX_NV;
+constexpr int64_t kMaxEdges = TC_NOALLOC_MAX_EDGES;
+constexpr int64_t kScanTile = 2048;  // scan tile of tc_static.cu (scan_tiles rounds by it)
+constexpr int64_t kMaxTiles = (kMaxNv + kScanTile - 1) / kScanTile + 1;
+
+// Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | tile_sums int64[tiles+1]
+// | dplus int32[maxnv+1] | large int32[maxnv+1] | indp int32[max_edges]
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t kOffStatus = 0;
+constexpr size_t kOffOffp = align256(kOffStatus + sizeof(DevStatus));
+constexpr size_t kOffTiles = align256(kOffOffp + sizeof(int64_t) * (kMaxNv + 1));
+constexpr size_t kOffDplus = align256(kOffTiles + sizeof(int64_t) * (kMaxTiles + 1));
+constexpr size_t kOffLarge = align256(kOffDplus + sizeof(int32_t) * (kMaxNv + 1));
+constexpr size_t kOffIndp = align256(kOffLarge + sizeof(int32_t) * (kMaxNv + 1));
+constexpr size_t kScratchBytes = align256(kOffIndp + sizeof(int32_t) * kMaxEdges);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+struct DevScratch {
+  std::mutex mu;
+  unsigned char* ptr[64] = {};
+};
+DevScratch& dev_scratch() {
+  static DevScratch* d = new DevScratch();
+  return *d;
+}
+
+// Device address of the scratch array on the current device (looked up once per device).
+tc_status scratch_address(unsigned char** out) {
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  DevScratch& d = dev_scratch();
+  std::lock_guard<std::mutex> lk(d.mu);
+  if (!d.ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(TC_ERR_CUDA, "cudaGetSymbolAddress of the no-alloc scratch failed: %s", cudaGetErrorString(e));
+    d.ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  *out = d.ptr[dev];
+  return TC_OK;
+}
+
+}  // namespace
+}  // namespace tc
+
+using namespace tc;
+
+extern "C" tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode,
+                                            int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
+                                            const tc_sched* sched, void* stream) {
+  if (nv < 0 || (nv > 0 && (!d_off || !d_ind))) return fail(TC_ERR_INVALID_ARG, "invalid CSR (nv=%d)", nv);
+  if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_CSR) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
+  if (pv_mode != TC_PV_NONE && nv > 0 && !per_vertex)
+    return fail(TC_ERR_INVALID_ARG, "per_vertex output required for mode %d", pv_mode);
+  if ((int64_t)nv > kMaxNv)
+    return fail(TC_ERR_CAPACITY, "no-alloc count: %d vertices exceed the fixed limit of %lld", nv, (long long)kMaxNv);
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t m = 0;
+  if (nv > 0) {
+    TC_CUDA_TRY(cudaMemcpyAsync(&m, d_off + nv, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    TC_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (m < 0) return fail(TC_ERR_BAD_GRAPH, "negative edge count");
+  if ((int64_t)m > kMaxEdges)
+    return fail(TC_ERR_CAPACITY, "no-alloc count: %d directed edges exceed the fixed limit of %lld", m,
+                (long long)kMaxEdges);
+  unsigned char* base = nullptr;
+  TC_TRY(scratch_address(&base));
+  // A workspace view onto the fixed array; nothing is allocated or freed.
+  Workspace ws;
+  ws.device = -1;
+  ws.n_cap = kMaxNv + 1;
+  ws.e_cap = kMaxEdges;
+  ws.tiles_cap = kMaxTiles + 1;
+  ws.st = reinterpret_cast<DevStatus*>(base + kOffStatus);
+  ws.offp = reinterpret_cast<int64_t*>(base + kOffOffp);
+  ws.tile_sums = reinterpret_cast<int64_t*>(base + kOffTiles);
+  ws.dplus = reinterpret_cast<int32_t*>(base + kOffDplus);
+  ws.large = reinterpret_cast<int32_t*>(base + kOffLarge);
+  ws.indp = reinterpret_cast<int32_t*>(base + kOffIndp);
+  if (scan_tiles(nv) + 1 > ws.tiles_cap) return fail(TC_ERR_CAPACITY, "scan tiles exceed the fixed limit");
+  Csr32View view{d_off, d_ind};
+  // static_count clears the status word (the only scratch that must start at zero) itself.
+  TC_TRY(static_count(view, nv, (int64_t)m, ws, pv_mode, per_vertex, triangles_dev, to_params(sched), s));
+  if (info) return read_info(ws, s, info);
+  return TC_OK;
+}

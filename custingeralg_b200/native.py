@@ -26,6 +26,9 @@ MLP_HIDDEN = 64
 MLP_OUT = 3
 MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
 
+NOALLOC_MAX_NV = 1 << 20
+NOALLOC_MAX_EDGES = 1 << 22
+
 TC_PV_NONE = 0
 TC_PV_HANDLE = 1
 TC_PV_CSR = 2
@@ -84,6 +87,8 @@ SIGNATURES = {
     "tc_count_csr64": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
                                       ctypes.POINTER(Sched), _P]),
     "tc_workspace_status": (ctypes.c_int, [_P, ctypes.POINTER(CountInfo)]),
+    "tc_count_csr32_noalloc": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
+                                              ctypes.POINTER(Sched), _P]),
     "tc_apply_batch": (ctypes.c_int, [_P, _P, _P, _P, _i64, ctypes.c_int, _P, _P, ctypes.POINTER(BatchInfo),
                                       ctypes.POINTER(Sched), _P]),
     "tc_batch_sort": (ctypes.c_int, [_i32, _P, _P, _i64, _P, _P, _P]),

@@ -131,6 +131,24 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
                          int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
                          const tc_sched* sched, void* stream);
 
+/* Allocation-free variant of tc_count_csr32 (no counterpart in the reference): same inputs,
+ * outputs and conventions, but it never calls cudaMalloc or cudaFree. It is for callers that
+ * cannot allocate device memory at count time: code running inside a captured CUDA graph
+ * region, processes whose allocator forbids device allocation after start-up, or services
+ * that budget every byte of device memory up front. Its working memory is a fixed array inside
+ * this library's device image, sized for at most TC_NOALLOC_MAX_NV vertices and
+ * TC_NOALLOC_MAX_EDGES directed edges (about 32 MB, held by every GPU that loads the library
+ * until the process exits); larger graphs are rejected with TC_ERR_CAPACITY. All calls share
+ * that array, so calls that overlap on the GPU race: issue them on one stream or order them
+ * with events. The first call on a device looks up the array's device address with that
+ * device current; make it before any stream capture. The edge count d_off[nv] is read back to
+ * the host, so the call synchronises `stream` once. */
+#define TC_NOALLOC_MAX_NV (1 << 20)
+#define TC_NOALLOC_MAX_EDGES (1 << 22)
+tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode,
+                                 int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
+                                 const tc_sched* sched, void* stream);
+
 /* Read back the info of the last stateless count on the current device. Syncs `stream`. */
 tc_status tc_workspace_status(void* stream, tc_count_info* info);
 
