@@ -190,7 +190,7 @@ class ClockSampler:
 
 def traffic_from_profile(scale):
     """DRAM bytes per k_count launch from the committed ncu summary, scaled to this graph."""
-    path = os.path.join(ROOT, "profiles", "k_count_rmat.md")
+    path = os.path.join(ROOT, "profiles", f"k_count_rmat{scale}.md")
     if not os.path.exists(path):
         return None
     vals = {}
