@@ -90,17 +90,31 @@ tc_status Workspace::ensure(int64_t n, int64_t m) {
   if (device >= 0 && device != dev) return fail(TC_ERR_INVALID_ARG, "workspace used on device %d, created on %d", dev, device);
   device = dev;
   if (n + 1 > n_cap) {
-    int64_t c1 = 0, c2 = 0, c3 = 0;
+    int64_t c1 = 0, c2 = 0, c3 = 0, c4 = 0;
     if (dplus) { cudaFree(dplus); dplus = nullptr; }
     if (offp) { cudaFree(offp); offp = nullptr; }
     if (large) { cudaFree(large); large = nullptr; }
+    if (medium) { cudaFree(medium); medium = nullptr; }
     TC_TRY(grow(dplus, c1, n + 1));
     TC_TRY(grow(offp, c2, n + 1));
     TC_TRY(grow(large, c3, n + 1));
+    TC_TRY(grow(medium, c4, n + 1));
     n_cap = n + 1;
   }
   TC_TRY(grow(indp, e_cap, m));
   TC_TRY(grow(tile_sums, tiles_cap, scan_tiles(n) + 1));
+  if (hubs_for(m) > hub_cap) {
+    int64_t c1 = 0;
+    if (hub_base) { cudaFree(hub_base); hub_base = nullptr; }
+    TC_TRY(grow(hub_u, hub_cap, hubs_for(m)));
+    TC_TRY(grow(hub_base, c1, hubs_for(m)));
+  }
+  if (chunks_for(m) > chunk_cap) {
+    int64_t c1 = 0;
+    if (chunk_hub) { cudaFree(chunk_hub); chunk_hub = nullptr; }
+    TC_TRY(grow(hub_cnt, chunk_cap, chunks_for(m)));
+    TC_TRY(grow(chunk_hub, c1, chunks_for(m)));
+  }
   if (!st) TC_CUDA_TRY(cudaMalloc(&st, sizeof(DevStatus)));
   return TC_OK;
 }
@@ -110,16 +124,14 @@ void Workspace::release() {
   cudaFree(offp);
   cudaFree(indp);
   cudaFree(large);
+  cudaFree(medium);
   cudaFree(tile_sums);
+  cudaFree(hub_u);
+  cudaFree(hub_base);
+  cudaFree(hub_cnt);
+  cudaFree(chunk_hub);
   cudaFree(st);
-  dplus = nullptr;
-  offp = nullptr;
-  indp = nullptr;
-  large = nullptr;
-  tile_sums = nullptr;
-  st = nullptr;
-  n_cap = e_cap = tiles_cap = 0;
-  device = -1;
+  *this = Workspace();
 }
 
 namespace {
@@ -207,8 +219,8 @@ const char* tc_status_string(tc_status s) {
 void tc_sched_default(tc_sched* s) {
   if (!s) return;
   memset(s, 0, sizeof(*s));
-  s->warp_max_deg = 32;
-  s->search_ratio_x16 = 32;  // search when d+(v) > 2 d+(u) (log2 d+(v) + 1)
+  s->warp_max_deg = 256;     // out-degree up to which one warp counts a vertex alone
+  s->search_ratio_x16 = 16;  // search when d+(v) > d+(u) (log2 d+(v) + 1)
   s->blocks_per_sm = 0;
   s->chunk = 64;
   s->use_table = 0;

@@ -12,6 +12,8 @@ namespace tc {
 
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kHubChunk = 2048;     // orientation: list entries per warp work item of a hub
+constexpr int kWarpTierMax = 256;   // largest out-degree a single warp counts on its own
 
 // ---- error reporting -------------------------------------------------------------------
 
@@ -73,8 +75,14 @@ struct DevStatus {
   unsigned long long q_small;            // work-queue head over vertex ids
   unsigned int bad_flags;
   unsigned int max_dplus;
-  unsigned int n_large;                  // vertices on the block (large out-degree) queue
+  unsigned int n_large;                  // vertices on the CTA (large out-degree) queue
   unsigned int q_large;                  // work-queue head over the large list
+  unsigned int n_medium;                 // vertices on the warp (medium out-degree) queue
+  unsigned int q_medium;
+  unsigned int n_hubs;                   // vertices whose list is split into chunks
+  unsigned int n_hub_chunks;
+  unsigned int q_hub_count;              // work-queue heads of the two hub kernels
+  unsigned int q_hub_fill;
 };
 
 // ---- scheduler parameters as the kernels see them --------------------------------------
@@ -104,10 +112,20 @@ struct Workspace {
   int64_t* offp = nullptr;       // [n+1]
   int32_t* indp = nullptr;       // [e_cap]
   int32_t* large = nullptr;      // [n]
+  int32_t* medium = nullptr;     // [n]
   int64_t* tile_sums = nullptr;  // [tiles+1]
+  int32_t* hub_u = nullptr;      // [hub_cap] vertices split into chunks
+  int32_t* hub_base = nullptr;   // [hub_cap] their first chunk index
+  int32_t* hub_cnt = nullptr;    // [chunk_cap] out-neighbours found per chunk
+  int32_t* chunk_hub = nullptr;  // [chunk_cap] hub of each chunk
+  int64_t hub_cap = 0;
+  int64_t chunk_cap = 0;
   DevStatus* st = nullptr;       // [1]
   tc_status ensure(int64_t n, int64_t m_directed);
   void release();
+  // Hub arrays needed for a graph of m directed edges.
+  static int64_t hubs_for(int64_t m) { return m / kHubChunk + 1; }
+  static int64_t chunks_for(int64_t m) { return 2 * (m / kHubChunk) + 2; }
 };
 
 // Device properties cached per device.

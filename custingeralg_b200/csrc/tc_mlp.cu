@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(kHid) k_mlp_backward(const float* __restrict__
   for (int o = 0; o < kOut; ++o) atomicAdd(&grad[oW3 + o * kHid + j], gW3[o]);
   if (j < kOut) atomicAdd(&grad[oB3 + j], gb3);
   // loss: warp sums then one atomic per warp
+  __syncwarp();
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(kFull, lsum, o);
   if ((j & 31) == 0) atomicAdd(loss, lsum * inv_n);
 }

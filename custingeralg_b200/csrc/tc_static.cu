@@ -5,25 +5,32 @@
 // lists of every directed edge with a merge path split across 1-32 lanes and one block
 // reduction per source vertex. Here:
 //
-//  1. k_orient_count / scan / k_orient_fill build the degree orientation G+ (u -> v iff
-//     (deg u, u) < (deg v, v)) as a compact CSR whose lists stay ascending by id. Every
-//     triangle {x < y < z in that order} is found exactly once: at x, on edge x->y, as the
-//     common element z of N+(x) and N+(y). The same passes check the input (ids in range,
-//     strictly ascending lists, no self-loops, a signed edge checksum for symmetry).
-//  2. k_count runs a persistent grid over two work queues. Vertices with out-degree above
-//     the warp threshold ("large") are taken one per CTA: N+(u) is staged in shared memory
-//     as an open-addressing hash set (chunks of 2048 entries). All other vertices with
-//     d+ >= 2 are taken one per warp with a warp-private 64-slot hash set. For each group of
-//     32 out-neighbours v of u the warp streams the concatenation of their lists N+(v) with
-//     coalesced loads (each lane walks its own segment pointer; no warp collective inside the
-//     data-dependent loop) and probes every element into the hash set ("probe" strategy), or, for an edge whose
-//     N+(v) is long next to N+(u), binary-searches the elements of N+(u) into N+(v)
-//     ("search" strategy). The scheduler picks the strategy per edge.
-//  3. Per-vertex counts never take a global atomic per triangle: the three vertices of a
-//     triangle found at u are u, v = A[i] and w = A[j], both slots of the staged list A, so
-//     they accumulate in shared-memory counters and flush with at most one global atomic per
-//     oriented edge. The triangle total takes one global atomic per CTA.
+//  1. Orientation. k_orient_count / k_orient_count_hub / scan / k_orient_fill /
+//     k_orient_fill_hub build the degree orientation G+ (u -> v iff (deg u, u) < (deg v, v)) as
+//     a compact CSR whose lists stay ascending by id. Every triangle {x < y < z in that order}
+//     is found exactly once: at x, on edge x->y, as the common element z of N+(x) and N+(y).
+//     One warp takes a vertex; a vertex with more than kHubChunk neighbours is split into
+//     chunks of kHubChunk that separate warps take (the hub kernels), so a degree-64k hub is
+//     not one warp's serial tail. The same passes check the input (ids in range, strictly
+//     ascending lists, no self-loops, a signed edge checksum for symmetry).
+//  2. Counting. k_count is a persistent grid over three tiers of source vertex u by its
+//     out-degree a = d+(u):
+//       L  a > warp_max:    one CTA per vertex; N+(u) staged in shared memory as an
+//                           open-addressing hash set (2048 entries per pass);
+//       M  32 < a <= warp_max (<= 256): one warp per vertex with a warp-private hash set;
+//       S  2 <= a <= 32:    one warp per vertex, claimed in chunks of vertex ids.
+//     For each group of 32 out-neighbours v of u the warp walks the concatenation of their
+//     lists N+(v) with coalesced loads; each lane advances its own segment pointer, held in
+//     registers (no warp collective inside the data-dependent loop), and probes every element
+//     into the hash set ("probe" strategy). For an edge whose N+(v) is long next to N+(u) the
+//     warp binary-searches the entries of N+(u) into N+(v) instead ("search" strategy). The
+//     scheduler (threshold or learned per-degree-cell table) picks the strategy per edge.
+//  3. Attribution. Per-vertex counts never take a global atomic per triangle: the three
+//     vertices of a triangle found at u are u, v = A[i] and w = A[j], all in the staged list
+//     A, so they accumulate in registers / shared-memory counters and flush with at most one
+//     global atomic per oriented edge. The triangle total takes one global atomic per CTA.
 #include <algorithm>
+#include <climits>
 #include <cstring>
 
 #include "tc_internal.cuh"
@@ -37,36 +44,18 @@ namespace tc {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;     // 4 warps: small CTAs keep more warps resident per SM
 constexpr int kWarps = kThreads / kWarp;
-constexpr int kChunk = 2048;      // A entries staged per pass for a large vertex
-constexpr int kHashMax = 4096;    // hash slots for a chunk (load <= 0.5)
-constexpr int kSmallSlots = 64;   // warp-private hash slots (warp_max <= 32)
+constexpr int kChunk = 1024;      // A entries staged per pass for an L-tier vertex
+constexpr int kHashMax = 2048;    // hash slots for such a chunk (load <= 0.5)
+constexpr int kUnroll = 4;        // list elements a lane loads before probing (independent loads)
+constexpr int kSmallMax = 32;     // S tier: out-degree up to one warp group
+constexpr int kMedSlots = 2 * kWarpTierMax;  // warp-private hash slots (load <= 0.25 up to a = 128, else <= 0.5)
+// Hash sets are bucketized: 4 slots per 16-byte bucket, probed with one 128-bit shared load,
+// so a lookup ends after one bucket unless that bucket is full (rare at these loads).
 constexpr int kScanThreads = 256;
 constexpr int kScanPer = 8;
 constexpr int kScanTile = kScanThreads * kScanPer;
-
-struct WarpSmem {
-  int32_t hkeys[kSmallSlots];
-  int32_t sA[kWarp];
-  uint32_t cnt[kWarp];
-  int64_t seg_base[kWarp];
-  int32_t seg_v[kWarp];
-  uint32_t seg_cnt[kWarp];
-  int32_t seg_start[kWarp];
-  int8_t hidx[kSmallSlots];
-};
-
-struct CountSmem {
-  int32_t hkeys[kHashMax];
-  int32_t sA[kChunk];
-  uint32_t cnt[kChunk];
-  int16_t hidx[kHashMax];
-  WarpSmem warp[kWarps];
-  unsigned long long tri[kWarps];
-  unsigned item;
-  int gctr;
-};
 
 #ifdef TC_DEBUG_PROGRESS
 // Debug builds only: per-warp progress words and per-kernel entry/exit counters in host-mapped
@@ -77,13 +66,13 @@ __device__ unsigned long long* tc_dbg_kern = nullptr;
   do {                                                                                     \
     if (tc_dbg_progress) ((volatile unsigned long long*)tc_dbg_progress)[(idx)] = (val);  \
   } while (0)
-#define TC_DBG_ENTER(id)                                                                   \
-  do {                                                                                     \
-    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id)], 1ull);    \
+#define TC_DBG_ENTER(id)                                                                     \
+  do {                                                                                       \
+    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id)], 1ull);      \
   } while (0)
-#define TC_DBG_EXIT(id)                                                                    \
-  do {                                                                                     \
-    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id) + 1], 1ull); \
+#define TC_DBG_EXIT(id)                                                                      \
+  do {                                                                                       \
+    if (tc_dbg_kern && threadIdx.x == 0) atomicAdd_system(&tc_dbg_kern[2 * (id) + 1], 1ull);  \
   } while (0)
 #else
 #define TC_DBG_MARK(idx, val) \
@@ -96,6 +85,32 @@ __device__ unsigned long long* tc_dbg_kern = nullptr;
   do {                  \
   } while (0)
 #endif
+
+// Warp-private staging of one vertex (S and M tiers).
+struct WarpTable {
+  alignas(16) int32_t hkeys[kMedSlots];
+  int32_t sA[kWarpTierMax];
+  uint32_t cnt[kWarpTierMax];
+  uint8_t hidx[kMedSlots];
+};
+
+// CTA-shared staging of one chunk of an L-tier vertex.
+struct BlockTable {
+  alignas(16) int32_t hkeys[kHashMax];
+  int32_t sA[kChunk];
+  uint32_t cnt[kChunk];
+  int16_t hidx[kHashMax];
+};
+
+struct CountSmem {
+  union {
+    BlockTable L;
+    WarpTable W[kWarps];
+  } t;
+  unsigned long long tri[kWarps];
+  unsigned item;
+  int gctr;
+};
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned r;
@@ -118,36 +133,51 @@ __device__ __forceinline__ T warp_sum(T x) {
   return x;
 }
 
-__device__ __forceinline__ uint32_t hash_slot(int32_t key, int bits) {
-  return ((uint32_t)key * 0x9E3779B1u) >> (32 - bits);
+__device__ __forceinline__ uint32_t hash_bucket(int32_t key, int bbits) {
+  return ((uint32_t)key * 0x9E3779B1u) >> (32 - bbits);
 }
 
-// Insert key (unique) with payload idx; the table has 2^bits slots and load <= 0.5, so an
-// empty slot is always found within 2^bits steps.
+// Insert key (unique) with payload idx into a table of 2^bbits buckets of 4 slots (load <= 0.5,
+// so a bucket with a free slot is always found within 2^bbits steps). Slots of a bucket fill in
+// order and are never freed, so a key that moved on found every slot before it taken.
 template <typename IdxT>
-__device__ __forceinline__ void hash_insert(int32_t* keys, IdxT* idx, int bits, int32_t key, int j) {
-  const uint32_t mask = (1u << bits) - 1;
-  uint32_t s = hash_slot(key, bits);
-  for (uint32_t it = 0; it <= mask; ++it) {
-    const int32_t prev = atomicCAS(&keys[s], -1, key);
-    if (prev == -1) {
-      idx[s] = (IdxT)j;
-      return;
+__device__ __forceinline__ void hash_insert(int32_t* keys, IdxT* idx, int bbits, int32_t key, int j) {
+  const uint32_t bmask = (1u << bbits) - 1;
+  uint32_t b = hash_bucket(key, bbits);
+  for (uint32_t it = 0; it <= bmask; ++it) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int32_t prev = atomicCAS(&keys[4 * b + t], -1, key);
+      if (prev == -1) {
+        idx[4 * b + t] = (IdxT)j;
+        return;
+      }
+      if (prev == key) return;
     }
-    if (prev == key) return;
-    s = (s + 1) & mask;
+    b = (b + 1) & bmask;
   }
 }
 
-// Slot holding key, or -1.
-__device__ __forceinline__ int hash_find(const int32_t* keys, int bits, int32_t key) {
-  const uint32_t mask = (1u << bits) - 1;
-  uint32_t s = hash_slot(key, bits);
-  for (uint32_t it = 0; it <= mask; ++it) {
-    const int32_t k = keys[s];
-    if (k == key) return (int)s;
-    if (k == -1) return -1;
-    s = (s + 1) & mask;
+// Slot holding key, or -1. One 128-bit load per bucket visited; the first bucket is resolved
+// without branches, the chain continues only when that bucket is full and lacks the key.
+__device__ __forceinline__ int hash_find(const int32_t* keys, int bbits, int32_t key) {
+  const uint32_t bmask = (1u << bbits) - 1;
+  uint32_t b = hash_bucket(key, bbits);
+  int4 q = *reinterpret_cast<const int4*>(keys + 4 * b);
+  int pos = q.w == key ? 3 : -1;
+  pos = q.z == key ? 2 : pos;
+  pos = q.y == key ? 1 : pos;
+  pos = q.x == key ? 0 : pos;
+  if (pos >= 0) return 4 * b + pos;
+  if (q.w == -1) return -1;  // slots fill in order: a free last slot means the bucket is not full
+  for (uint32_t it = 0; it < bmask; ++it) {
+    b = (b + 1) & bmask;
+    q = *reinterpret_cast<const int4*>(keys + 4 * b);
+    if (q.x == key) return 4 * b;
+    if (q.y == key) return 4 * b + 1;
+    if (q.z == key) return 4 * b + 2;
+    if (q.w == key) return 4 * b + 3;
+    if (q.w == -1) return -1;
   }
   return -1;
 }
@@ -190,99 +220,93 @@ __device__ __forceinline__ void tri_weights(int32_t u, int32_t v, int32_t w, uin
 }
 
 template <int PV>
-constexpr uint32_t flush_mult() {
+__host__ __device__ constexpr uint32_t flush_mult() {
   return PV == TC_PV_HANDLE ? 2u : 1u;
 }
 
 // One warp intersects N+(u) with N+(v) for the out-neighbours v = A[g0 .. g0+gcount) of u.
 // The current chunk of A (entries [chunk_base, chunk_base+chunk_len)) is in shared memory as
-// sA and as a hash set; cnt[] holds the chunk's per-slot counters.
+// sA and as a hash set of 2^bits buckets (hidx[slot] = entry); cnt[] holds the chunk's
+// per-entry counters.
+//
+// The out-neighbours are taken one at a time (warp-uniform). For each, either the warp streams
+// N+(v) with coalesced loads, kUnroll elements per lane in flight, and probes the hash set
+// (probe strategy), or it binary-searches the chunk's entries in N+(v) (search strategy).
+// Almost all probe work lies in lists of 32 or more entries, so walking one list at a time
+// wastes few lanes and keeps v, its list pointer and its v-role count warp-uniform.
 template <int PV, typename IdxT>
 __device__ __forceinline__ void process_group(
     const int32_t u, const int32_t* __restrict__ Ag, const int32_t* sA, const int chunk_base,
     const int chunk_len, const int32_t* hkeys, const IdxT* hidx, const int bits, uint32_t* cnt,
     const int g0, const int gcount, const int32_t* __restrict__ dplus,
     const int64_t* __restrict__ offp, const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
-    WarpSmem& ws, const SchedParams& sp, uint32_t& tri, uint32_t& u_acc) {
+    const SchedParams& sp, uint32_t& tri, uint32_t& u_acc) {
   const int lane = threadIdx.x & (kWarp - 1);
   const bool valid = lane < gcount;
   const int i = g0 + lane;
   const int li = i - chunk_base;
-  const bool in_chunk = li >= 0 && li < chunk_len;
-  const int32_t v = valid ? (in_chunk ? sA[li] : __ldg(Ag + i)) : 0;
+  const int32_t v = valid ? ((li >= 0 && li < chunk_len) ? sA[li] : __ldg(Ag + i)) : 0;
   const int b = valid ? __ldg(dplus + v) : 0;
   const int64_t base = valid ? __ldg(offp + v) : 0;
-  const bool active = valid && b > 0 &&
-                      (sp.cell_filter == -1 || (sp.cell_filter >= 0 && log2_cell(chunk_len) * 16 + log2_cell(b) == sp.cell_filter));
-  const bool srch = active && use_search(sp, chunk_len, b);
-  const int pb = (active && !srch) ? b : 0;
-
-  // ---- probe strategy: stream the concatenated lists N+(v), probe into the hash set ----
-  int incl = pb;
-#pragma unroll
-  for (int o = 1; o < kWarp; o <<= 1) {
-    const int t = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += t;
-  }
-  const int P = incl - pb;
-  const int total = __shfl_sync(kFull, incl, kWarp - 1);
-  const unsigned lt = lanemask_lt();
-  const unsigned segmask = __ballot_sync(kFull, pb > 0);
-  const int rank = __popc(segmask & lt);
-  if (pb > 0) {
-    ws.seg_base[rank] = base - P;
-    ws.seg_v[rank] = v;
-    ws.seg_cnt[rank] = 0;
-    ws.seg_start[rank] = P;
-  }
-  __syncwarp();
-  // Each lane walks the flat index k = lane, lane + 32, ... and advances its own segment
-  // pointer (segments are contiguous and ascending), so the loop holds no warp collective.
-  const int nseg = __popc(segmask);
-  int r = 0;
-  for (int k = lane; k < total; k += kWarp) {
-    if (lane == 0) TC_DBG_MARK(((blockIdx.x * kWarps + threadIdx.x / kWarp) * 4 + 2),
-                               ((unsigned long long)(unsigned)total << 32) | (unsigned)k);
-    while (r + 1 < nseg && ws.seg_start[r + 1] <= k) ++r;
-    const int32_t w = __ldg(indp + ws.seg_base[r] + k);
-    const int s = hash_find(hkeys, bits, w);
-    if (s >= 0) {
-      ++tri;
-      if (PV != TC_PV_NONE) {
-        uint32_t wu, wv, ww;
-        tri_weights<PV>(u, ws.seg_v[r], w, wu, wv, ww);
-        u_acc += wu;
-        if (ww) atomicAdd(&cnt[hidx[s]], ww);
-        if (wv) atomicAdd(&ws.seg_cnt[r], wv);
-      }
-    }
-  }
-  __syncwarp();
-
-  // ---- search strategy: binary-search the chunk's entries into N+(v) ----
-  unsigned sm = __ballot_sync(kFull, srch);
-  while (sm) {
-    const int sl = __ffs(sm) - 1;
-    sm &= sm - 1;
+  const bool active =
+      valid && b > 0 &&
+      (sp.cell_filter == -1 || (sp.cell_filter >= 0 && log2_cell(chunk_len) * 16 + log2_cell(b) == sp.cell_filter));
+  unsigned todo = __ballot_sync(kFull, active);
+  while (todo) {
+    const int sl = __ffs(todo) - 1;
+    todo &= todo - 1;
     const int32_t sv = __shfl_sync(kFull, v, sl);
     const int sb = __shfl_sync(kFull, b, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
     const int sli = __shfl_sync(kFull, li, sl);
-    uint32_t vacc = 0;
-    for (int j = lane; j < chunk_len; j += kWarp) {
-      const int32_t w = sA[j];
-      if (search_sorted(indp + sbase, sb, w)) {
-        ++tri;
-        if (PV != TC_PV_NONE) {
-          uint32_t wu, wv, ww;
-          tri_weights<PV>(u, sv, w, wu, wv, ww);
-          u_acc += wu;
-          vacc += wv;
-          if (ww) atomicAdd(&cnt[j], ww);
+    const int32_t* __restrict__ lst = indp + sbase;
+    uint32_t vacc = 0;  // v-role weight found by this lane
+    if (use_search(sp, chunk_len, sb)) {
+      // ---- search strategy: binary-search the chunk's entries into N+(v) ----
+      for (int j = lane; j < chunk_len; j += kWarp) {
+        const int32_t w = sA[j];
+        if (search_sorted(lst, sb, w)) {
+          ++tri;
+          if (PV != TC_PV_NONE) {
+            uint32_t wu, wv, ww;
+            tri_weights<PV>(u, sv, w, wu, wv, ww);
+            u_acc += wu;
+            vacc += wv;
+            if (ww) atomicAdd(&cnt[j], ww);
+          }
         }
       }
+    } else {
+      // ---- probe strategy: stream N+(v) and probe each element into the hash set ----
+      for (int k0 = lane; k0 < sb; k0 += kUnroll * kWarp) {
+        int32_t w[kUnroll];
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+          const int k = k0 + j * kWarp;
+          w[j] = k < sb ? __ldg(lst + k) : -1;
+        }
+#pragma unroll
+        for (int j = 0; j < kUnroll; ++j) {
+          if (w[j] < 0) continue;
+          const int s = hash_find(hkeys, bits, w[j]);
+          if (s >= 0) {
+            ++tri;
+            if (PV == TC_PV_HANDLE) {
+              ++vacc;
+              atomicAdd(&cnt[hidx[s]], 1u);
+            } else if (PV == TC_PV_CSR) {
+              uint32_t wu, wv, ww;
+              tri_weights<PV>(u, sv, w[j], wu, wv, ww);
+              u_acc += wu;
+              vacc += wv;
+              if (ww) atomicAdd(&cnt[hidx[s]], ww);
+            }
+          }
+        }
+      }
+      if (PV == TC_PV_HANDLE) u_acc += vacc;
     }
-    __syncwarp();
+    // v-role count: into the chunk counter when v is staged, else global.
     if (PV != TC_PV_NONE) {
       vacc = warp_sum(vacc);
       if (lane == 0 && vacc) {
@@ -292,22 +316,49 @@ __device__ __forceinline__ void process_group(
     }
   }
   __syncwarp();
-  // v-role counts of the probed edges: into the chunk counters when v is staged, else global.
-  if (PV != TC_PV_NONE && pb > 0) {
-    const uint32_t c = ws.seg_cnt[rank];
-    if (c) {
-      if (in_chunk) atomicAdd(&cnt[li], c);
-      else atomicAdd(&out[v], c * flush_mult<PV>());
+}
+
+// One warp counts the triangles whose lowest vertex is u (S and M tiers, a <= kWarpTierMax).
+template <int PV>
+__device__ __forceinline__ void warp_vertex(const int32_t u, const int a, WarpTable& t,
+                                            const int32_t* __restrict__ dplus, const int64_t* __restrict__ offp,
+                                            const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
+                                            const SchedParams& sp, uint32_t& tri) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int32_t* Ag = indp + __ldg(offp + u);
+  int bits = 4;  // buckets: 4 * 2^bits slots >= 4a (load <= 0.25) while they fit in kMedSlots
+  while ((1 << bits) < a && (8 << bits) <= kMedSlots) ++bits;
+  const int S = 4 << bits;
+  for (int s = lane; s < S; s += kWarp) t.hkeys[s] = -1;
+  for (int j = lane; j < a; j += kWarp) {
+    t.sA[j] = __ldg(Ag + j);
+    t.cnt[j] = 0;
+  }
+  __syncwarp();
+  for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, t.hidx, bits, t.sA[j], j);
+  __syncwarp();
+  uint32_t u_acc = 0;
+  for (int g0 = 0; g0 < a; g0 += kWarp)
+    process_group<PV>(u, Ag, t.sA, 0, a, t.hkeys, t.hidx, bits, t.cnt, g0, min(kWarp, a - g0), dplus, offp, indp, out,
+                      sp, tri, u_acc);
+  if (PV != TC_PV_NONE) {
+    for (int j = lane; j < a; j += kWarp) {
+      const uint32_t c = t.cnt[j];
+      if (c) atomicAdd(&out[t.sA[j]], c * flush_mult<PV>());
     }
+    __syncwarp();
+    u_acc = warp_sum(u_acc);
+    if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
   }
   __syncwarp();
 }
 
 template <int PV>
-__global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32_t* __restrict__ dplus,
+__global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const int32_t* __restrict__ dplus,
                                                     const int64_t* __restrict__ offp,
                                                     const int32_t* __restrict__ indp,
                                                     const int32_t* __restrict__ large,
+                                                    const int32_t* __restrict__ medium,
                                                     uint32_t* __restrict__ out, DevStatus* __restrict__ st,
                                                     const SchedParams sp) {
   TC_DBG_ENTER(6);
@@ -317,8 +368,10 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
   const int wid = threadIdx.x / kWarp;
   uint32_t tri = 0;
   const unsigned n_large = st->n_large;
+  const unsigned n_medium = st->n_medium;
 
-  // Phase 1: large out-degree vertices, one CTA each, in chunks of kChunk staged entries.
+  // Tier L: one CTA per vertex, in chunks of kChunk staged entries.
+  BlockTable& L = sm.t.L;
   while (true) {
     if (threadIdx.x == 0) sm.item = atomicAdd(&st->q_large, 1u);
     __syncwarp();
@@ -333,18 +386,18 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
     uint32_t u_acc = 0;
     for (int cb = 0; cb < a; cb += kChunk) {
       const int clen = min(kChunk, a - cb);
-      int bits = 6;
-      while ((1 << bits) < 2 * clen) ++bits;
-      const int S = 1 << bits;
-      for (int s = threadIdx.x; s < S; s += kThreads) sm.hkeys[s] = -1;
+      int bits = 4;  // buckets: 4 * 2^bits slots >= 2 clen, load <= 0.5
+      while ((4 << bits) < 2 * clen) ++bits;
+      const int S = 4 << bits;
+      for (int s = threadIdx.x; s < S; s += kThreads) L.hkeys[s] = -1;
       for (int j = threadIdx.x; j < clen; j += kThreads) {
-        sm.sA[j] = __ldg(Ag + cb + j);
-        sm.cnt[j] = 0;
+        L.sA[j] = __ldg(Ag + cb + j);
+        L.cnt[j] = 0;
       }
       if (threadIdx.x == 0) sm.gctr = 0;
       __syncwarp();
       __syncthreads();
-      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(sm.hkeys, sm.hidx, bits, sm.sA[j], j);
+      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, L.hidx, bits, L.sA[j], j);
       __syncwarp();
       __syncthreads();
       const int ngroups = (a + kWarp - 1) / kWarp;
@@ -354,16 +407,15 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
         __syncwarp();
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
-        if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4 + 1, ((unsigned long long)cb << 32) | (unsigned)g);
-        process_group<PV>(u, Ag, sm.sA, cb, clen, sm.hkeys, sm.hidx, bits, sm.cnt, g * kWarp,
-                          min(kWarp, a - g * kWarp), dplus, offp, indp, out, sm.warp[wid], sp, tri, u_acc);
+        process_group<PV>(u, Ag, L.sA, cb, clen, L.hkeys, L.hidx, bits, L.cnt, g * kWarp, min(kWarp, a - g * kWarp),
+                          dplus, offp, indp, out, sp, tri, u_acc);
       }
       __syncwarp();
       __syncthreads();
       if (PV != TC_PV_NONE) {
         for (int j = threadIdx.x; j < clen; j += kThreads) {
-          const uint32_t c = sm.cnt[j];
-          if (c) atomicAdd(&out[sm.sA[j]], c * flush_mult<PV>());
+          const uint32_t c = L.cnt[j];
+          if (c) atomicAdd(&out[L.sA[j]], c * flush_mult<PV>());
         }
       }
       __syncwarp();
@@ -375,8 +427,24 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
     }
   }
 
-  // Phase 2: vertices with 2 <= d+ <= warp_max, one warp each, claimed in chunks.
-  WarpSmem& ws = sm.warp[wid];
+  // From here every warp works alone, on its own slice of the (now free) staging area.
+  WarpTable& W = sm.t.W[wid];
+
+  // Tier M: one warp per vertex with 32 < d+ <= warp_max, from the medium queue.
+  while (true) {
+    unsigned idx = 0;
+    if (lane == 0) idx = atomicAdd(&st->q_medium, 1u);
+    __syncwarp();
+    idx = __shfl_sync(kFull, idx, 0);
+    if (idx >= n_medium) break;
+    const int32_t u = medium[idx];
+    const int a = __ldg(dplus + u);
+    if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (3ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
+    warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri);
+  }
+
+  // Tier S: vertices with 2 <= d+ <= 32 (and <= warp_max), one warp each, claimed in chunks.
+  const int smax = min(kSmallMax, sp.warp_max);
   while (true) {
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(&st->q_small, (unsigned long long)sp.chunk);
@@ -387,38 +455,14 @@ __global__ void __launch_bounds__(kThreads) k_count(const int32_t n, const int32
     for (int32_t ub = (int32_t)c0; ub < cend; ub += kWarp) {
       const int32_t uu = ub + lane;
       const int aa = (uu < cend) ? __ldg(dplus + uu) : 0;
-      unsigned elig = __ballot_sync(kFull, aa >= 2 && aa <= sp.warp_max && (uu % sp.nshards) == sp.shard);
+      unsigned elig = __ballot_sync(kFull, aa >= 2 && aa <= smax && (uu % sp.nshards) == sp.shard);
       while (elig) {
         const int sl = __ffs(elig) - 1;
         elig &= elig - 1;
         const int32_t u = ub + sl;
         const int a = __shfl_sync(kFull, aa, sl);
         if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (2ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
-        const int32_t* Ag = indp + __ldg(offp + u);
-        ws.hkeys[lane] = -1;
-        ws.hkeys[lane + kWarp] = -1;
-        ws.cnt[lane] = 0;
-        int32_t x = 0;
-        if (lane < a) {
-          x = __ldg(Ag + lane);
-          ws.sA[lane] = x;
-        }
-        __syncwarp();
-        if (lane < a) hash_insert(ws.hkeys, ws.hidx, 6, x, lane);
-        __syncwarp();
-        uint32_t u_acc = 0;
-        process_group<PV>(u, Ag, ws.sA, 0, a, ws.hkeys, ws.hidx, 6, ws.cnt, 0, a, dplus, offp, indp, out,
-                          ws, sp, tri, u_acc);
-        if (PV != TC_PV_NONE) {
-          if (lane < a) {
-            const uint32_t c = ws.cnt[lane];
-            if (c) atomicAdd(&out[x], c * flush_mult<PV>());
-          }
-          __syncwarp();
-          u_acc = warp_sum(u_acc);
-          if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
-        }
-        __syncwarp();
+        warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri);
       }
     }
   }
@@ -443,48 +487,81 @@ __device__ __forceinline__ bool precedes(int32_t du, int32_t u, int32_t dv, int3
   return du < dv || (du == dv && u < v);
 }
 
+// Count the out-neighbours of u among its entries [k_begin, k_end) and check them.
+// Warp-wide; the result is warp-uniform.
+template <class View>
+__device__ __forceinline__ int orient_count_range(const View& g, const int32_t n, const int32_t u, const int32_t d,
+                                                  const int64_t s, const int32_t k_begin, const int32_t k_end,
+                                                  unsigned long long& chk, unsigned& bad) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  int cnt = 0;
+  int32_t last = k_begin > 0 ? g.ind[s + k_begin - 1] : INT32_MIN;
+  for (int32_t k0 = k_begin; k0 < k_end; k0 += kWarp) {
+    const int32_t k = k0 + lane;
+    const bool in = k < k_end;
+    const int32_t v = in ? g.ind[s + k] : INT32_MAX;
+    int32_t prev = __shfl_up_sync(kFull, v, 1);
+    if (lane == 0) prev = last;
+    last = __shfl_sync(kFull, v, kWarp - 1);
+    bool pred = false;
+    if (in) {
+      if (v < 0 || v >= n) {
+        bad |= kBadRange;
+      } else {
+        if (k > 0 && prev >= v) bad |= kBadOrder;
+        if (v == u) bad |= kBadSelfLoop;
+        const int32_t dv = g.len(v);
+        pred = precedes(d, u, dv, v);
+        const uint64_t h = (u < v) ? sym_hash((uint32_t)u, (uint32_t)v) : sym_hash((uint32_t)v, (uint32_t)u);
+        chk += (u < v) ? h : (0ull - h);
+      }
+    }
+    __syncwarp();
+    cnt += __popc(__ballot_sync(kFull, pred));
+  }
+  return cnt;
+}
+
 template <class View>
 __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_t n, int32_t* __restrict__ dplus,
+                                                      int32_t* __restrict__ hub_u, int32_t* __restrict__ hub_base,
+                                                      int32_t* __restrict__ hub_cnt, int32_t* __restrict__ chunk_hub,
+                                                      const int64_t hub_cap, const int64_t chunk_cap,
                                                       DevStatus* __restrict__ st) {
   TC_DBG_ENTER(1);
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
-  unsigned long long chk = 0, ei = 0;
-  unsigned bad = 0, mx = 0;
+  unsigned long long chk = 0;
+  unsigned bad = 0;
   for (int64_t uu = gw; uu < n; uu += nw) {
     const int32_t u = (int32_t)uu;
     const int64_t s = g.start(u);
     const int32_t d = g.len(u);
-    int cnt = 0;
-    int32_t last = INT32_MIN;
-    for (int32_t k0 = 0; k0 < d; k0 += kWarp) {
-      const int32_t k = k0 + lane;
-      const bool in = k < d;
-      const int32_t v = in ? g.ind[s + k] : INT32_MAX;
-      int32_t prev = __shfl_up_sync(kFull, v, 1);
-      if (lane == 0) prev = last;
-      last = __shfl_sync(kFull, v, kWarp - 1);
-      bool pred = false;
-      if (in) {
-        if (v < 0 || v >= n) {
-          bad |= kBadRange;
-        } else {
-          if (k > 0 && prev >= v) bad |= kBadOrder;
-          if (v == u) bad |= kBadSelfLoop;
-          const int32_t dv = g.len(v);
-          pred = precedes(d, u, dv, v);
-          const uint64_t h = (u < v) ? sym_hash((uint32_t)u, (uint32_t)v) : sym_hash((uint32_t)v, (uint32_t)u);
-          chk += (u < v) ? h : (0ull - h);
-        }
+    const int32_t dd = min(d, kHubChunk);
+    const int cnt = orient_count_range(g, n, u, d, s, 0, dd, chk, bad);
+    if (lane == 0) dplus[u] = cnt;
+    if (d > kHubChunk) {
+      // Hub: chunks 1.. are counted by k_orient_count_hub.
+      const int nch = (d + kHubChunk - 1) / kHubChunk;
+      int h = 0, base = 0;
+      if (lane == 0) {
+        h = (int)atomicAdd(&st->n_hubs, 1u);
+        base = (int)atomicAdd(&st->n_hub_chunks, (unsigned)nch);
       }
       __syncwarp();
-      cnt += __popc(__ballot_sync(kFull, pred));
-    }
-    if (lane == 0) {
-      dplus[u] = cnt;
-      if (d >= 2) ei += (unsigned long long)cnt;
-      mx = max(mx, (unsigned)cnt);
+      h = __shfl_sync(kFull, h, 0);
+      base = __shfl_sync(kFull, base, 0);
+      if (h < hub_cap && base + nch <= chunk_cap) {
+        if (lane == 0) {
+          hub_u[h] = u;
+          hub_base[h] = base;
+          hub_cnt[base] = cnt;
+        }
+        for (int c = lane; c < nch; c += kWarp) chunk_hub[base + c] = h;
+      } else {
+        bad |= kBadCapacity;
+      }
     }
   }
   __syncwarp();
@@ -494,26 +571,102 @@ __global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_
   if (lane == 0) {
     if (chk) atomicAdd(&st->sym_checksum, chk);
     if (bad) atomicOr(&st->bad_flags, bad);
-    if (ei) atomicAdd(&st->edges_intersected, ei);
-    if (mx) atomicMax(&st->max_dplus, mx);
   }
   TC_DBG_EXIT(1);
+}
+
+// Chunks 1.. of hub lists: one warp per chunk, claimed from a queue.
+template <class View>
+__global__ void __launch_bounds__(256) k_orient_count_hub(const View g, const int32_t n, int32_t* __restrict__ dplus,
+                                                          const int32_t* __restrict__ hub_u,
+                                                          const int32_t* __restrict__ hub_base,
+                                                          int32_t* __restrict__ hub_cnt,
+                                                          const int32_t* __restrict__ chunk_hub,
+                                                          const int64_t chunk_cap, DevStatus* __restrict__ st) {
+  TC_DBG_ENTER(7);
+  const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
+  unsigned long long chk = 0;
+  unsigned bad = 0;
+  while (true) {
+    unsigned q = 0;
+    if (lane == 0) q = atomicAdd(&st->q_hub_count, 1u);
+    __syncwarp();
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= nchunks) break;
+    const int h = chunk_hub[q];
+    if (h < 0 || h >= (int)st->n_hubs) continue;
+    const int c = (int)q - hub_base[h];
+    if (c <= 0) continue;  // chunk 0 is counted by k_orient_count
+    const int32_t u = hub_u[h];
+    const int64_t s = g.start(u);
+    const int32_t d = g.len(u);
+    const int32_t k_begin = c * kHubChunk, k_end = min(d, k_begin + kHubChunk);
+    const int cnt = orient_count_range(g, n, u, d, s, k_begin, k_end, chk, bad);
+    if (lane == 0) {
+      hub_cnt[q] = cnt;
+      if (cnt) atomicAdd(&dplus[u], cnt);
+    }
+  }
+  __syncwarp();
+  chk = warp_sum(chk);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  if (lane == 0) {
+    if (chk) atomicAdd(&st->sym_checksum, chk);
+    if (bad) atomicOr(&st->bad_flags, bad);
+  }
+  TC_DBG_EXIT(7);
+}
+
+// Write the out-neighbours of u among entries [k_begin, k_end) at indp[out_base ...] (in list
+// order, at most `room` of them); returns the sum of their out-degrees. Warp-wide.
+template <class View>
+__device__ __forceinline__ unsigned long long orient_fill_range(const View& g, const int32_t n, const int32_t u,
+                                                                const int32_t d, const int64_t s,
+                                                                const int32_t k_begin, const int32_t k_end,
+                                                                const int32_t* __restrict__ dplus,
+                                                                int32_t* __restrict__ indp, const int64_t out_base,
+                                                                const int32_t room) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned lt = lanemask_lt();
+  int pos = 0;
+  unsigned long long ws = 0;
+  for (int32_t k0 = k_begin; k0 < k_end; k0 += kWarp) {
+    const int32_t k = k0 + lane;
+    bool pred = false;
+    int32_t v = 0;
+    if (k < k_end) {
+      v = g.ind[s + k];
+      if (v >= 0 && v < n) pred = precedes(d, u, g.len(v), v);
+    }
+    __syncwarp();
+    const unsigned msk = __ballot_sync(kFull, pred);
+    const int at = pos + __popc(msk & lt);
+    if (pred && at < room) {
+      indp[out_base + at] = v;
+      ws += (unsigned long long)__ldg(dplus + v);
+    }
+    pos += __popc(msk);
+  }
+  __syncwarp();
+  return warp_sum(ws);
 }
 
 template <class View>
 __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t n, const int32_t* __restrict__ dplus,
                                                      const int64_t* __restrict__ offp, int32_t* __restrict__ indp,
                                                      const int64_t e_cap, int32_t* __restrict__ large,
-                                                     DevStatus* __restrict__ st, const int warp_max,
-                                                     const int shard, const int nshards) {
+                                                     int32_t* __restrict__ medium, DevStatus* __restrict__ st,
+                                                     const int warp_max, const int shard, const int nshards) {
   TC_DBG_ENTER(5);
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
-  const unsigned lt = lanemask_lt();
-  unsigned long long work = 0;
-  int nbuf = 0;
-  int32_t buf = 0;
+  unsigned long long work = 0, ei = 0;
+  unsigned mx = 0;
+  int nbl = 0, nbm = 0;
+  int32_t bufl = 0, bufm = 0;
   unsigned bad = 0;
   for (int64_t uu = gw; uu < n; uu += nw) {
     const int32_t u = (int32_t)uu;
@@ -525,54 +678,113 @@ __global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t
       bad |= kBadCapacity;
       continue;
     }
-    int pos = 0;
-    unsigned long long ws = 0;
-    for (int32_t k0 = 0; k0 < d; k0 += kWarp) {
-      const int32_t k = k0 + lane;
-      bool pred = false;
-      int32_t v = 0;
-      if (k < d) {
-        v = g.ind[s + k];
-        if (v >= 0 && v < n) pred = precedes(d, u, g.len(v), v);
-      }
-      __syncwarp();
-      const unsigned msk = __ballot_sync(kFull, pred);
-      const int at = pos + __popc(msk & lt);
-      if (pred && at < a) {
-        indp[base + at] = v;
-        ws += (unsigned long long)__ldg(dplus + v);
-      }
-      pos += __popc(msk);
+    // hubs: chunk 0 here (it starts at the list's own offset), the rest in k_orient_fill_hub
+    const unsigned long long ws = orient_fill_range(g, n, u, d, s, 0, min(d, kHubChunk), dplus, indp, base, a);
+    if (lane == 0) {
+      work += ws + (unsigned long long)a * (unsigned long long)a;
+      if (d >= 2) ei += (unsigned long long)a;
+      mx = max(mx, (unsigned)a);
     }
-    __syncwarp();
-    ws = warp_sum(ws);
-    if (lane == 0) work += ws + (unsigned long long)a * (unsigned long long)a;
-    if (a > warp_max && (u % nshards) == shard) {
-      if (lane == nbuf) buf = u;
-      if (++nbuf == kWarp) {
-        unsigned at = 0;
-        if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)kWarp);
-        __syncwarp();
-        at = __shfl_sync(kFull, at, 0);
-        large[at + lane] = buf;
-        nbuf = 0;
+    if ((u % nshards) == shard) {
+      if (a > warp_max) {
+        if (lane == nbl) bufl = u;
+        if (++nbl == kWarp) {
+          unsigned at = 0;
+          if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)kWarp);
+          __syncwarp();
+          at = __shfl_sync(kFull, at, 0);
+          large[at + lane] = bufl;
+          nbl = 0;
+        }
+      } else if (a > kSmallMax) {
+        if (lane == nbm) bufm = u;
+        if (++nbm == kWarp) {
+          unsigned at = 0;
+          if (lane == 0) at = atomicAdd(&st->n_medium, (unsigned)kWarp);
+          __syncwarp();
+          at = __shfl_sync(kFull, at, 0);
+          medium[at + lane] = bufm;
+          nbm = 0;
+        }
       }
     }
   }
-  if (nbuf) {
+  if (nbl) {
     unsigned at = 0;
-    if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)nbuf);
+    if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)nbl);
     __syncwarp();
     at = __shfl_sync(kFull, at, 0);
-    if (lane < nbuf) large[at + lane] = buf;
+    if (lane < nbl) large[at + lane] = bufl;
   }
+  if (nbm) {
+    unsigned at = 0;
+    if (lane == 0) at = atomicAdd(&st->n_medium, (unsigned)nbm);
+    __syncwarp();
+    at = __shfl_sync(kFull, at, 0);
+    if (lane < nbm) medium[at + lane] = bufm;
+  }
+  __syncwarp();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  if (lane == 0) {
+    if (work) atomicAdd(&st->oriented_work, work);
+    if (ei) atomicAdd(&st->edges_intersected, ei);
+    if (mx) atomicMax(&st->max_dplus, mx);
+    if (bad) atomicOr(&st->bad_flags, bad);
+  }
+  TC_DBG_EXIT(5);
+}
+
+template <class View>
+__global__ void __launch_bounds__(256) k_orient_fill_hub(const View g, const int32_t n, const int32_t* __restrict__ dplus,
+                                                         const int64_t* __restrict__ offp, int32_t* __restrict__ indp,
+                                                         const int64_t e_cap, const int32_t* __restrict__ hub_u,
+                                                         const int32_t* __restrict__ hub_base,
+                                                         const int32_t* __restrict__ hub_cnt,
+                                                         const int32_t* __restrict__ chunk_hub,
+                                                         const int64_t chunk_cap, DevStatus* __restrict__ st) {
+  TC_DBG_ENTER(8);
+  const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
+  unsigned long long work = 0;
+  unsigned bad = 0;
+  while (true) {
+    unsigned q = 0;
+    if (lane == 0) q = atomicAdd(&st->q_hub_fill, 1u);
+    __syncwarp();
+    q = __shfl_sync(kFull, q, 0);
+    if (q >= nchunks) break;
+    const int h = chunk_hub[q];
+    if (h < 0 || h >= (int)st->n_hubs) continue;
+    const int hb = hub_base[h];
+    const int c = (int)q - hb;
+    if (c <= 0) continue;  // chunk 0 is written by k_orient_fill
+    const int32_t u = hub_u[h];
+    const int64_t s = g.start(u);
+    const int32_t d = g.len(u);
+    const int32_t a = dplus[u];
+    // entries of this chunk go after those of the chunks before it
+    int prefix = 0;
+    for (int cc = lane; cc < c; cc += kWarp) prefix += hub_cnt[hb + cc];
+    __syncwarp();
+    prefix = warp_sum(prefix);
+    if (offp[u] + a > e_cap || prefix > a) {
+      bad |= kBadCapacity;
+      continue;
+    }
+    const int32_t k_begin = c * kHubChunk, k_end = min(d, k_begin + kHubChunk);
+    const unsigned long long ws =
+        orient_fill_range(g, n, u, d, s, k_begin, k_end, dplus, indp, offp[u] + prefix, a - prefix);
+    if (lane == 0) work += ws;
+  }
+  __syncwarp();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
   if (lane == 0) {
     if (work) atomicAdd(&st->oriented_work, work);
     if (bad) atomicOr(&st->bad_flags, bad);
   }
-  TC_DBG_EXIT(5);
+  TC_DBG_EXIT(8);
 }
 
 // ---- exclusive scan of int32 counts into int64 offsets ------------------------------------
@@ -680,6 +892,8 @@ int orient_grid(int64_t n) {
   return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 
+int hub_grid() { return device_info().sms * 8; }
+
 template <int PV>
 tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const SchedParams& sp,
                        cudaStream_t stream) {
@@ -700,7 +914,27 @@ tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const Sche
 #ifdef TC_DEBUG_PROGRESS
   if (tc_dbg_progress_host_dev) cudaMemsetAsync(tc_dbg_progress_host_dev, 0, tc_dbg_progress_bytes, stream);
 #endif
-  k_count<PV><<<grid, kThreads, smem, stream>>>(n, ws.dplus, ws.offp, ws.indp, ws.large, out, ws.st, sp);
+  k_count<PV><<<grid, kThreads, smem, stream>>>(n, ws.dplus, ws.offp, ws.indp, ws.large, ws.medium, out, ws.st, sp);
+  TC_CUDA_TRY(cudaGetLastError());
+  return TC_OK;
+}
+
+template <class View>
+tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& sp, bool fill, cudaStream_t stream) {
+  const int grid = orient_grid(n);
+  k_orient_count<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.hub_u, ws.hub_base, ws.hub_cnt, ws.chunk_hub,
+                                                 ws.hub_cap, ws.chunk_cap, ws.st);
+  TC_CUDA_TRY(cudaGetLastError());
+  k_orient_count_hub<View><<<hub_grid(), 256, 0, stream>>>(view, n, ws.dplus, ws.hub_u, ws.hub_base, ws.hub_cnt,
+                                                           ws.chunk_hub, ws.chunk_cap, ws.st);
+  TC_CUDA_TRY(cudaGetLastError());
+  if (!fill) return TC_OK;
+  TC_TRY(scan_counts(ws.dplus, n, ws.offp, ws.tile_sums, stream));
+  k_orient_fill<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.medium,
+                                                ws.st, sp.warp_max, sp.shard, sp.nshards);
+  TC_CUDA_TRY(cudaGetLastError());
+  k_orient_fill_hub<View><<<hub_grid(), 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.hub_u,
+                                                          ws.hub_base, ws.hub_cnt, ws.chunk_hub, ws.chunk_cap, ws.st);
   TC_CUDA_TRY(cudaGetLastError());
   return TC_OK;
 }
@@ -729,14 +963,14 @@ SchedParams to_params(const tc_sched* s) {
     s = &d;
   }
   SchedParams p;
-  p.warp_max = std::min(32, std::max(2, s->warp_max_deg));
+  p.warp_max = std::min(kWarpTierMax, std::max(2, s->warp_max_deg));
   p.search_ratio_x16 = std::max(0, s->search_ratio_x16);
   p.use_table = s->use_table ? 1 : 0;
   p.chunk = std::max(32, (s->chunk + 31) / 32 * 32);
   p.blocks_per_sm = std::max(0, s->blocks_per_sm);
   p.nshards = std::max(1, s->nshards);
-  p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
   p.shard = std::min(std::max(0, s->shard), p.nshards - 1);
+  p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
   memcpy(p.table, s->table, sizeof(p.table));
   return p;
 }
@@ -749,13 +983,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
     TC_CUDA_TRY(cudaMemsetAsync(per_vertex, 0, sizeof(int32_t) * (size_t)n, stream));
   if (n > 0) {
     prof_mark(0, stream);
-    const int grid = orient_grid(n);
-    k_orient_count<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.st);
-    TC_CUDA_TRY(cudaGetLastError());
-    TC_TRY(scan_counts(ws.dplus, n, ws.offp, ws.tile_sums, stream));
-    k_orient_fill<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.st,
-                                                  sp.warp_max, sp.shard, sp.nshards);
-    TC_CUDA_TRY(cudaGetLastError());
+    TC_TRY(orient(view, n, ws, sp, true, stream));
     prof_mark(1, stream);
     uint32_t* out = reinterpret_cast<uint32_t*>(per_vertex);
     switch (pv_mode) {
@@ -765,7 +993,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);
-    prof_launches(scan_tiles(n) > 0 ? 6 : 3);
+    prof_launches(scan_tiles(n) > 0 ? 8 : 5);
   }
   (void)m;
   if (triangles_dev)
@@ -806,10 +1034,6 @@ tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* inf
   return TC_OK;
 }
 
-}  // namespace tc
-
-namespace tc {
-
 namespace {
 // Warp per source vertex: per degree-cell sums over its oriented edges, in shared memory, then
 // one atomic per touched cell per CTA.
@@ -835,6 +1059,7 @@ __global__ void __launch_bounds__(256) k_cell_stats(const int32_t n, const int32
       atomicAdd(&acc[4 * c + 3], (double)min(a, b) / (double)max(max(a, b), 1));
     }
   }
+  __syncwarp();
   __syncthreads();
   for (int i = threadIdx.x; i < 256 * 4; i += blockDim.x)
     if (acc[i] != 0.0) atomicAdd(&out[i], acc[i]);
@@ -856,10 +1081,7 @@ tc_status cell_stats(int32_t n, Workspace& ws, double* out_host, cudaStream_t st
 template <class View>
 tc_status validate_view(const View& view, int32_t n, Workspace& ws, cudaStream_t stream) {
   TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
-  if (n > 0) {
-    k_orient_count<View><<<orient_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.st);
-    TC_CUDA_TRY(cudaGetLastError());
-  }
+  if (n > 0) TC_TRY(orient(view, n, ws, to_params(nullptr), false, stream));
   return TC_OK;
 }
 

@@ -40,10 +40,10 @@ int ilog2(int64_t x) {
 
 std::vector<tc_sched> candidates() {
   std::vector<tc_sched> out;
-  const int warp_max[] = {8, 16, 32};
-  const int ratio[] = {8, 16, 32, 64, 1 << 30};
+  const int warp_max[] = {64, 128, 256};
+  const int ratio[] = {8, 16, 32, 1 << 30};
   const int chunk[] = {32, 128};
-  const int bps[] = {0, 2};
+  const int bps[] = {0, 6};
   for (int w : warp_max)
     for (int r : ratio)
       for (int c : chunk)

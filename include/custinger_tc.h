@@ -58,7 +58,7 @@ enum { TC_MEM_DEVICE = 0, TC_MEM_HOST = 1 };
 /* Scheduler: which intersection strategy each oriented edge uses and the launch shapes.
  * tc_sched_default() fills the fixed degree-threshold heuristic. */
 typedef struct tc_sched {
-  int32_t warp_max_deg;   /* out-degree up to which a vertex is counted by one warp (<= 32) */
+  int32_t warp_max_deg;   /* out-degree up to which a vertex is counted by one warp (<= 256) */
   int32_t search_ratio_x16; /* edge (u,v) uses binary search of N+(u) into N+(v) when
                                16*d+(v) > search_ratio_x16 * d+(u) * (log2 d+(v) + 1) */
   int32_t blocks_per_sm;  /* persistent grid = SMs x blocks_per_sm (0 = occupancy limit) */

@@ -32,5 +32,5 @@ def test_generator_library_exports():
 
 def test_default_sched_and_strings():
     s = N.default_sched()
-    assert 2 <= s.warp_max_deg <= 32
+    assert 2 <= s.warp_max_deg <= 256
     assert N.lib().tc_status_string(N.TC_ERR_NOT_SYMMETRIC) == b"graph not symmetric"
