@@ -84,7 +84,7 @@ tc_status grow(T*& p, int64_t& cap, int64_t want) {
 }
 }  // namespace
 
-tc_status Workspace::ensure(int64_t n, int64_t m) {
+tc_status Workspace::ensure(int64_t n, int64_t m, int64_t extent) {
   int dev = 0;
   TC_CUDA_TRY(cudaGetDevice(&dev));
   if (device >= 0 && device != dev) return fail(TC_ERR_INVALID_ARG, "workspace used on device %d, created on %d", dev, device);
@@ -101,13 +101,14 @@ tc_status Workspace::ensure(int64_t n, int64_t m) {
     TC_TRY(grow(medium, c4, n + 1));
     n_cap = n + 1;
   }
-  TC_TRY(grow(indp, e_cap, m));
-  TC_TRY(grow(tile_sums, tiles_cap, scan_tiles(n) + 1));
+  TC_TRY(grow(indp, e_cap, std::max(m, extent)));
   if (hubs_for(m) > hub_cap) {
-    int64_t c1 = 0;
+    int64_t c1 = 0, c2 = 0;
     if (hub_base) { cudaFree(hub_base); hub_base = nullptr; }
-    TC_TRY(grow(hub_u, hub_cap, hubs_for(m)));
+    if (hub_done) { cudaFree(hub_done); hub_done = nullptr; }
     TC_TRY(grow(hub_base, c1, hubs_for(m)));
+    TC_TRY(grow(hub_done, c2, hubs_for(m)));
+    TC_TRY(grow(hub_u, hub_cap, hubs_for(m)));
   }
   if (chunks_for(m) > chunk_cap) {
     int64_t c1 = 0;
@@ -125,10 +126,10 @@ void Workspace::release() {
   cudaFree(indp);
   cudaFree(large);
   cudaFree(medium);
-  cudaFree(tile_sums);
   cudaFree(hub_u);
   cudaFree(hub_base);
   cudaFree(hub_cnt);
+  cudaFree(hub_done);
   cudaFree(chunk_hub);
   cudaFree(st);
   *this = Workspace();

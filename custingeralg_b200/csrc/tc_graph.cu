@@ -258,7 +258,7 @@ tc_status tc_graph_export(tc_graph* g, int64_t* off_host, int32_t* ind_host) {
 tc_status tc_graph_validate(tc_graph* g, void* stream) {
   if (!g) return fail(TC_ERR_INVALID_ARG, "graph is NULL");
   cudaStream_t s = (cudaStream_t)stream;
-  TC_TRY(g->ws.ensure(g->n, g->m));
+  TC_TRY(g->ws.ensure(g->n, g->m, g->pool_cap));
   SlackView view{g->start, g->used, g->pool};
   TC_TRY(validate_view(view, g->n, g->ws, s));
   tc_count_info info;
@@ -276,7 +276,7 @@ tc_status tc_count_static(tc_graph* g, int pv_mode, int32_t* per_vertex, int64_t
   extern volatile int tc_dbg_host_stage;
   tc_dbg_host_stage = 201;
 #endif
-  TC_TRY(g->ws.ensure(g->n, g->m));
+  TC_TRY(g->ws.ensure(g->n, g->m, g->pool_cap));
   SlackView view{g->start, g->used, g->pool};
   TC_TRY(static_count(view, g->n, g->m, g->ws, pv_mode, per_vertex, triangles_dev, to_params(sched), s));
 #ifdef TC_DEBUG_PROGRESS

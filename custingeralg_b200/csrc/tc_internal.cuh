@@ -70,7 +70,7 @@ enum : unsigned { kBadRange = 1u, kBadOrder = 2u, kBadSelfLoop = 4u, kBadCapacit
 struct DevStatus {
   unsigned long long triangles;          // T
   unsigned long long edges_intersected;  // oriented edges with deg(u) >= 2
-  unsigned long long oriented_work;      // sum over u->v of d+(u) + d+(v)
+  unsigned long long oriented_work;      // sum over u->v with d+(u) >= 2 of d+(u) + d+(v)
   unsigned long long sym_checksum;       // signed edge checksum, 0 when symmetric
   unsigned long long q_small;            // work-queue head over vertex ids
   unsigned int bad_flags;
@@ -81,8 +81,8 @@ struct DevStatus {
   unsigned int q_medium;
   unsigned int n_hubs;                   // vertices whose list is split into chunks
   unsigned int n_hub_chunks;
-  unsigned int q_hub_count;              // work-queue heads of the two hub kernels
-  unsigned int q_hub_fill;
+  unsigned int q_orient_hub;             // orientation work-queue heads: hub chunks,
+  unsigned int q_orient_vtx;             // vertex ids
 };
 
 // ---- scheduler parameters as the kernels see them --------------------------------------
@@ -107,21 +107,21 @@ struct Workspace {
   int device = -1;
   int64_t n_cap = 0;       // vertices
   int64_t e_cap = 0;       // oriented edge slots
-  int64_t tiles_cap = 0;
   int32_t* dplus = nullptr;      // [n]
   int64_t* offp = nullptr;       // [n+1]
-  int32_t* indp = nullptr;       // [e_cap]
+  int32_t* indp = nullptr;       // [e_cap] N+(u) at indp[start(u) ...] (the input's own index space)
   int32_t* large = nullptr;      // [n]
   int32_t* medium = nullptr;     // [n]
-  int64_t* tile_sums = nullptr;  // [tiles+1]
   int32_t* hub_u = nullptr;      // [hub_cap] vertices split into chunks
   int32_t* hub_base = nullptr;   // [hub_cap] their first chunk index
   int32_t* hub_cnt = nullptr;    // [chunk_cap] out-neighbours found per chunk
+  int32_t* hub_done = nullptr;   // [hub_cap] chunks of each hub oriented so far
   int32_t* chunk_hub = nullptr;  // [chunk_cap] hub of each chunk
   int64_t hub_cap = 0;
   int64_t chunk_cap = 0;
   DevStatus* st = nullptr;       // [1]
-  tc_status ensure(int64_t n, int64_t m_directed);
+  // n vertices, m directed edges, lists inside [0, extent) of the input's index space.
+  tc_status ensure(int64_t n, int64_t m_directed, int64_t extent = -1);
   void release();
   // Hub arrays needed for a graph of m directed edges.
   static int64_t hubs_for(int64_t m) { return m / kHubChunk + 1; }

@@ -23,25 +23,23 @@ namespace {
 
 constexpr int64_t kMaxNv = TC_NOALLOC_MAX_NV;
 constexpr int64_t kMaxEdges = TC_NOALLOC_MAX_EDGES;
-constexpr int64_t kScanTile = 2048;  // scan tile of tc_static.cu (scan_tiles rounds by it)
-constexpr int64_t kMaxTiles = (kMaxNv + kScanTile - 1) / kScanTile + 1;
 
 constexpr int64_t kMaxHubs = kMaxEdges / kHubChunk + 1;
 constexpr int64_t kMaxChunks = 2 * (kMaxEdges / kHubChunk) + 2;
 
-// Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | tile_sums int64[tiles+1]
-// | dplus int32[maxnv+1] | large int32[maxnv+1] | medium int32[maxnv+1] | hub_u, hub_base
-// int32[hubs] | hub_cnt, chunk_hub int32[chunks] | indp int32[max_edges]
+// Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | dplus int32[maxnv+1]
+// | large int32[maxnv+1] | medium int32[maxnv+1] | hub_u, hub_base, hub_done int32[hubs]
+// | hub_cnt, chunk_hub int32[chunks] | indp int32[max_edges]
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffStatus = 0;
 constexpr size_t kOffOffp = align256(kOffStatus + sizeof(DevStatus));
-constexpr size_t kOffTiles = align256(kOffOffp + sizeof(int64_t) * (kMaxNv + 1));
-constexpr size_t kOffDplus = align256(kOffTiles + sizeof(int64_t) * (kMaxTiles + 1));
+constexpr size_t kOffDplus = align256(kOffOffp + sizeof(int64_t) * (kMaxNv + 1));
 constexpr size_t kOffLarge = align256(kOffDplus + sizeof(int32_t) * (kMaxNv + 1));
 constexpr size_t kOffMedium = align256(kOffLarge + sizeof(int32_t) * (kMaxNv + 1));
 constexpr size_t kOffHubU = align256(kOffMedium + sizeof(int32_t) * (kMaxNv + 1));
 constexpr size_t kOffHubBase = align256(kOffHubU + sizeof(int32_t) * kMaxHubs);
-constexpr size_t kOffHubCnt = align256(kOffHubBase + sizeof(int32_t) * kMaxHubs);
+constexpr size_t kOffHubDone = align256(kOffHubBase + sizeof(int32_t) * kMaxHubs);
+constexpr size_t kOffHubCnt = align256(kOffHubDone + sizeof(int32_t) * kMaxHubs);
 constexpr size_t kOffChunkHub = align256(kOffHubCnt + sizeof(int32_t) * kMaxChunks);
 constexpr size_t kOffIndp = align256(kOffChunkHub + sizeof(int32_t) * kMaxChunks);
 constexpr size_t kScratchBytes = align256(kOffIndp + sizeof(int32_t) * kMaxEdges);
@@ -106,21 +104,19 @@ extern "C" tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, co
   ws.device = -1;
   ws.n_cap = kMaxNv + 1;
   ws.e_cap = kMaxEdges;
-  ws.tiles_cap = kMaxTiles + 1;
   ws.st = reinterpret_cast<DevStatus*>(base + kOffStatus);
   ws.offp = reinterpret_cast<int64_t*>(base + kOffOffp);
-  ws.tile_sums = reinterpret_cast<int64_t*>(base + kOffTiles);
   ws.dplus = reinterpret_cast<int32_t*>(base + kOffDplus);
   ws.large = reinterpret_cast<int32_t*>(base + kOffLarge);
   ws.medium = reinterpret_cast<int32_t*>(base + kOffMedium);
   ws.hub_u = reinterpret_cast<int32_t*>(base + kOffHubU);
   ws.hub_base = reinterpret_cast<int32_t*>(base + kOffHubBase);
+  ws.hub_done = reinterpret_cast<int32_t*>(base + kOffHubDone);
   ws.hub_cnt = reinterpret_cast<int32_t*>(base + kOffHubCnt);
   ws.chunk_hub = reinterpret_cast<int32_t*>(base + kOffChunkHub);
   ws.hub_cap = kMaxHubs;
   ws.chunk_cap = kMaxChunks;
   ws.indp = reinterpret_cast<int32_t*>(base + kOffIndp);
-  if (scan_tiles(nv) + 1 > ws.tiles_cap) return fail(TC_ERR_CAPACITY, "scan tiles exceed the fixed limit");
   Csr32View view{d_off, d_ind};
   // static_count clears the status word (the only scratch that must start at zero) itself.
   TC_TRY(static_count(view, nv, (int64_t)m, ws, pv_mode, per_vertex, triangles_dev, to_params(sched), s));

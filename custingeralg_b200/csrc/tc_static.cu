@@ -5,26 +5,27 @@
 // lists of every directed edge with a merge path split across 1-32 lanes and one block
 // reduction per source vertex. Here:
 //
-//  1. Orientation. k_orient_count / k_orient_count_hub / scan / k_orient_fill /
-//     k_orient_fill_hub build the degree orientation G+ (u -> v iff (deg u, u) < (deg v, v)) as
-//     a compact CSR whose lists stay ascending by id. Every triangle {x < y < z in that order}
-//     is found exactly once: at x, on edge x->y, as the common element z of N+(x) and N+(y).
-//     One warp takes a vertex; a vertex with more than kHubChunk neighbours is split into
-//     chunks of kHubChunk that separate warps take (the hub kernels), so a degree-64k hub is
-//     not one warp's serial tail. The same passes check the input (ids in range, strictly
-//     ascending lists, no self-loops, a signed edge checksum for symmetry).
+//  1. Orientation (one pass). k_find_hubs registers the vertices with more than kHubChunk
+//     neighbours; k_orient then builds the degree orientation G+ (u -> v iff
+//     (deg u, u) < (deg v, v)) in the input's own index space: N+(u) is written, ascending by
+//     id, at indp[start(u) ...], so no offsets scan is needed. Every triangle {x < y < z in
+//     that order} is found exactly once: at x, on edge x->y, as the common element z of N+(x)
+//     and N+(y). Warps take hub chunks from one queue (the warp that finishes a hub's last
+//     chunk moves the pieces together), then tiles of 32 vertex ids from another, so a
+//     degree-64k hub is neither one warp's serial tail nor a load imbalance. The same pass
+//     checks the input (ids in range, strictly ascending lists, no self-loops, a signed edge
+//     checksum for symmetry) and fills the tier queues of the count.
 //  2. Counting. k_count is a persistent grid over three tiers of source vertex u by its
 //     out-degree a = d+(u):
-//       L  a > warp_max:    one CTA per vertex; N+(u) staged in shared memory as an
-//                           open-addressing hash set (2048 entries per pass);
-//       M  32 < a <= warp_max (<= 256): one warp per vertex with a warp-private hash set;
+//       L  a > warp_max:    one CTA per vertex; N+(u) staged in shared memory as a bucketized
+//                           hash set (1024 entries per pass);
+//       M  32 < a <= warp_max (<= 256): one warp per vertex from a queue, warp-private set;
 //       S  2 <= a <= 32:    one warp per vertex, claimed in chunks of vertex ids.
-//     For each group of 32 out-neighbours v of u the warp walks the concatenation of their
-//     lists N+(v) with coalesced loads; each lane advances its own segment pointer, held in
-//     registers (no warp collective inside the data-dependent loop), and probes every element
-//     into the hash set ("probe" strategy). For an edge whose N+(v) is long next to N+(u) the
-//     warp binary-searches the entries of N+(u) into N+(v) instead ("search" strategy). The
-//     scheduler (threshold or learned per-degree-cell table) picks the strategy per edge.
+//     The warp takes the out-neighbours v of u one at a time and streams N+(v) with coalesced
+//     loads (four per lane in flight), probing every element into the hash set ("probe"
+//     strategy); for an edge whose N+(v) is long next to N+(u) it binary-searches the entries
+//     of N+(u) into N+(v) instead ("search" strategy). The scheduler (threshold or learned
+//     per-degree-cell table) picks the strategy per edge.
 //  3. Attribution. Per-vertex counts never take a global atomic per triangle: the three
 //     vertices of a triangle found at u are u, v = A[i] and w = A[j], all in the staged list
 //     A, so they accumulate in registers / shared-memory counters and flush with at most one
@@ -108,6 +109,7 @@ struct CountSmem {
     WarpTable W[kWarps];
   } t;
   unsigned long long tri[kWarps];
+  unsigned long long work[kWarps];
   unsigned item;
   int gctr;
 };
@@ -240,13 +242,14 @@ __device__ __forceinline__ void process_group(
     const int chunk_len, const int32_t* hkeys, const IdxT* hidx, const int bits, uint32_t* cnt,
     const int g0, const int gcount, const int32_t* __restrict__ dplus,
     const int64_t* __restrict__ offp, const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
-    const SchedParams& sp, uint32_t& tri, uint32_t& u_acc) {
+    const SchedParams& sp, uint32_t& tri, uint32_t& u_acc, unsigned long long& work) {
   const int lane = threadIdx.x & (kWarp - 1);
   const bool valid = lane < gcount;
   const int i = g0 + lane;
   const int li = i - chunk_base;
   const int32_t v = valid ? ((li >= 0 && li < chunk_len) ? sA[li] : __ldg(Ag + i)) : 0;
   const int b = valid ? __ldg(dplus + v) : 0;
+  if (chunk_base == 0) work += (unsigned)b;  // the d+(v) part of the oriented work, once per edge
   const int64_t base = valid ? __ldg(offp + v) : 0;
   const bool active =
       valid && b > 0 &&
@@ -323,7 +326,7 @@ template <int PV>
 __device__ __forceinline__ void warp_vertex(const int32_t u, const int a, WarpTable& t,
                                             const int32_t* __restrict__ dplus, const int64_t* __restrict__ offp,
                                             const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
-                                            const SchedParams& sp, uint32_t& tri) {
+                                            const SchedParams& sp, uint32_t& tri, unsigned long long& work) {
   const int lane = threadIdx.x & (kWarp - 1);
   const int32_t* Ag = indp + __ldg(offp + u);
   int bits = 4;  // buckets: 4 * 2^bits slots >= 4a (load <= 0.25) while they fit in kMedSlots
@@ -340,7 +343,7 @@ __device__ __forceinline__ void warp_vertex(const int32_t u, const int a, WarpTa
   uint32_t u_acc = 0;
   for (int g0 = 0; g0 < a; g0 += kWarp)
     process_group<PV>(u, Ag, t.sA, 0, a, t.hkeys, t.hidx, bits, t.cnt, g0, min(kWarp, a - g0), dplus, offp, indp, out,
-                      sp, tri, u_acc);
+                      sp, tri, u_acc, work);
   if (PV != TC_PV_NONE) {
     for (int j = lane; j < a; j += kWarp) {
       const uint32_t c = t.cnt[j];
@@ -367,6 +370,7 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
   const int lane = threadIdx.x & (kWarp - 1);
   const int wid = threadIdx.x / kWarp;
   uint32_t tri = 0;
+  unsigned long long work = 0;
   const unsigned n_large = st->n_large;
   const unsigned n_medium = st->n_medium;
 
@@ -408,7 +412,7 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
         process_group<PV>(u, Ag, L.sA, cb, clen, L.hkeys, L.hidx, bits, L.cnt, g * kWarp, min(kWarp, a - g * kWarp),
-                          dplus, offp, indp, out, sp, tri, u_acc);
+                          dplus, offp, indp, out, sp, tri, u_acc, work);
       }
       __syncwarp();
       __syncthreads();
@@ -440,7 +444,7 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
     const int32_t u = medium[idx];
     const int a = __ldg(dplus + u);
     if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (3ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
-    warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri);
+    warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri, work);
   }
 
   // Tier S: vertices with 2 <= d+ <= 32 (and <= warp_max), one warp each, claimed in chunks.
@@ -462,7 +466,7 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
         const int32_t u = ub + sl;
         const int a = __shfl_sync(kFull, aa, sl);
         if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (2ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
-        warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri);
+        warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri, work);
       }
     }
   }
@@ -470,13 +474,21 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
   if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4 + 3, 1ull);
   // One global atomic per CTA for the triangle total.
   __syncwarp();
-  unsigned long long t = warp_sum((unsigned long long)tri);
-  if (lane == 0) sm.tri[wid] = t;
+  const unsigned long long t = warp_sum((unsigned long long)tri);
+  work = warp_sum(work);
+  if (lane == 0) {
+    sm.tri[wid] = t;
+    sm.work[wid] = work;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long s = 0;
-    for (int w = 0; w < kWarps; ++w) s += sm.tri[w];
+    unsigned long long s = 0, wk = 0;
+    for (int w = 0; w < kWarps; ++w) {
+      s += sm.tri[w];
+      wk += sm.work[w];
+    }
     if (s) atomicAdd(&st->triangles, s);
+    if (wk) atomicAdd(&st->oriented_work, wk);
   }
   TC_DBG_EXIT(6);
 }
@@ -487,13 +499,17 @@ __device__ __forceinline__ bool precedes(int32_t du, int32_t u, int32_t dv, int3
   return du < dv || (du == dv && u < v);
 }
 
-// Count the out-neighbours of u among its entries [k_begin, k_end) and check them.
-// Warp-wide; the result is warp-uniform.
-template <class View>
-__device__ __forceinline__ int orient_count_range(const View& g, const int32_t n, const int32_t u, const int32_t d,
-                                                  const int64_t s, const int32_t k_begin, const int32_t k_end,
-                                                  unsigned long long& chk, unsigned& bad) {
+// One warp orients entries [k_begin, k_end) of u's list (s = its start, d = its degree): it
+// checks each entry (id in range, strictly ascending, no self-loop, signed symmetry checksum)
+// and, when kWrite, writes the out-neighbours (in list order) to indp[out_base ...]. Returns
+// their number (warp-uniform).
+template <class View, bool kWrite>
+__device__ __forceinline__ int orient_range(const View& g, const int32_t n, const int32_t u, const int32_t d,
+                                            const int64_t s, const int32_t k_begin, const int32_t k_end,
+                                            int32_t* __restrict__ indp, const int64_t out_base,
+                                            unsigned long long& chk, unsigned& bad) {
   const int lane = threadIdx.x & (kWarp - 1);
+  const unsigned lt = lanemask_lt();
   int cnt = 0;
   int32_t last = k_begin > 0 ? g.ind[s + k_begin - 1] : INT32_MIN;
   for (int32_t k0 = k_begin; k0 < k_end; k0 += kWarp) {
@@ -510,281 +526,211 @@ __device__ __forceinline__ int orient_count_range(const View& g, const int32_t n
       } else {
         if (k > 0 && prev >= v) bad |= kBadOrder;
         if (v == u) bad |= kBadSelfLoop;
-        const int32_t dv = g.len(v);
-        pred = precedes(d, u, dv, v);
+        pred = precedes(d, u, g.len(v), v);
         const uint64_t h = (u < v) ? sym_hash((uint32_t)u, (uint32_t)v) : sym_hash((uint32_t)v, (uint32_t)u);
         chk += (u < v) ? h : (0ull - h);
       }
     }
     __syncwarp();
-    cnt += __popc(__ballot_sync(kFull, pred));
+    const unsigned msk = __ballot_sync(kFull, pred);
+    if (kWrite && pred) indp[out_base + cnt + __popc(msk & lt)] = v;
+    cnt += __popc(msk);
   }
   return cnt;
 }
 
-template <class View>
-__global__ void __launch_bounds__(256) k_orient_count(const View g, const int32_t n, int32_t* __restrict__ dplus,
-                                                      int32_t* __restrict__ hub_u, int32_t* __restrict__ hub_base,
-                                                      int32_t* __restrict__ hub_cnt, int32_t* __restrict__ chunk_hub,
-                                                      const int64_t hub_cap, const int64_t chunk_cap,
-                                                      DevStatus* __restrict__ st) {
-  TC_DBG_ENTER(1);
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
-  unsigned long long chk = 0;
-  unsigned bad = 0;
-  for (int64_t uu = gw; uu < n; uu += nw) {
-    const int32_t u = (int32_t)uu;
-    const int64_t s = g.start(u);
-    const int32_t d = g.len(u);
-    const int32_t dd = min(d, kHubChunk);
-    const int cnt = orient_count_range(g, n, u, d, s, 0, dd, chk, bad);
-    if (lane == 0) dplus[u] = cnt;
-    if (d > kHubChunk) {
-      // Hub: chunks 1.. are counted by k_orient_count_hub.
-      const int nch = (d + kHubChunk - 1) / kHubChunk;
-      int h = 0, base = 0;
-      if (lane == 0) {
-        h = (int)atomicAdd(&st->n_hubs, 1u);
-        base = (int)atomicAdd(&st->n_hub_chunks, (unsigned)nch);
-      }
-      __syncwarp();
-      h = __shfl_sync(kFull, h, 0);
-      base = __shfl_sync(kFull, base, 0);
-      if (h < hub_cap && base + nch <= chunk_cap) {
-        if (lane == 0) {
-          hub_u[h] = u;
-          hub_base[h] = base;
-          hub_cnt[base] = cnt;
-        }
-        for (int c = lane; c < nch; c += kWarp) chunk_hub[base + c] = h;
-      } else {
-        bad |= kBadCapacity;
-      }
-    }
+// Per-warp buffer of vertex ids bound for one of the tier queues, flushed 32 at a time.
+struct TierBuf {
+  int32_t val = 0;
+  int n = 0;
+  __device__ __forceinline__ void push(int32_t u, int32_t* __restrict__ q, unsigned* head) {
+    const int lane = threadIdx.x & (kWarp - 1);
+    if (lane == n) val = u;
+    if (++n == kWarp) flush(q, head);
   }
-  __syncwarp();
-  chk = warp_sum(chk);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
-  if (lane == 0) {
-    if (chk) atomicAdd(&st->sym_checksum, chk);
-    if (bad) atomicOr(&st->bad_flags, bad);
-  }
-  TC_DBG_EXIT(1);
-}
-
-// Chunks 1.. of hub lists: one warp per chunk, claimed from a queue.
-template <class View>
-__global__ void __launch_bounds__(256) k_orient_count_hub(const View g, const int32_t n, int32_t* __restrict__ dplus,
-                                                          const int32_t* __restrict__ hub_u,
-                                                          const int32_t* __restrict__ hub_base,
-                                                          int32_t* __restrict__ hub_cnt,
-                                                          const int32_t* __restrict__ chunk_hub,
-                                                          const int64_t chunk_cap, DevStatus* __restrict__ st) {
-  TC_DBG_ENTER(7);
-  const int lane = threadIdx.x & (kWarp - 1);
-  const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
-  unsigned long long chk = 0;
-  unsigned bad = 0;
-  while (true) {
-    unsigned q = 0;
-    if (lane == 0) q = atomicAdd(&st->q_hub_count, 1u);
+  __device__ __forceinline__ void flush(int32_t* __restrict__ q, unsigned* head) {
+    const int lane = threadIdx.x & (kWarp - 1);
+    if (n == 0) return;
+    unsigned at = 0;
+    if (lane == 0) at = atomicAdd(head, (unsigned)n);
     __syncwarp();
-    q = __shfl_sync(kFull, q, 0);
-    if (q >= nchunks) break;
-    const int h = chunk_hub[q];
-    if (h < 0 || h >= (int)st->n_hubs) continue;
-    const int c = (int)q - hub_base[h];
-    if (c <= 0) continue;  // chunk 0 is counted by k_orient_count
-    const int32_t u = hub_u[h];
-    const int64_t s = g.start(u);
-    const int32_t d = g.len(u);
-    const int32_t k_begin = c * kHubChunk, k_end = min(d, k_begin + kHubChunk);
-    const int cnt = orient_count_range(g, n, u, d, s, k_begin, k_end, chk, bad);
-    if (lane == 0) {
-      hub_cnt[q] = cnt;
-      if (cnt) atomicAdd(&dplus[u], cnt);
-    }
+    at = __shfl_sync(kFull, at, 0);
+    if (lane < n) q[at + lane] = val;
+    n = 0;
   }
-  __syncwarp();
-  chk = warp_sum(chk);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
-  if (lane == 0) {
-    if (chk) atomicAdd(&st->sym_checksum, chk);
-    if (bad) atomicOr(&st->bad_flags, bad);
-  }
-  TC_DBG_EXIT(7);
-}
+};
 
-// Write the out-neighbours of u among entries [k_begin, k_end) at indp[out_base ...] (in list
-// order, at most `room` of them); returns the sum of their out-degrees. Warp-wide.
-template <class View>
-__device__ __forceinline__ unsigned long long orient_fill_range(const View& g, const int32_t n, const int32_t u,
-                                                                const int32_t d, const int64_t s,
-                                                                const int32_t k_begin, const int32_t k_end,
-                                                                const int32_t* __restrict__ dplus,
-                                                                int32_t* __restrict__ indp, const int64_t out_base,
-                                                                const int32_t room) {
-  const int lane = threadIdx.x & (kWarp - 1);
-  const unsigned lt = lanemask_lt();
-  int pos = 0;
-  unsigned long long ws = 0;
-  for (int32_t k0 = k_begin; k0 < k_end; k0 += kWarp) {
-    const int32_t k = k0 + lane;
-    bool pred = false;
-    int32_t v = 0;
-    if (k < k_end) {
-      v = g.ind[s + k];
-      if (v >= 0 && v < n) pred = precedes(d, u, g.len(v), v);
-    }
-    __syncwarp();
-    const unsigned msk = __ballot_sync(kFull, pred);
-    const int at = pos + __popc(msk & lt);
-    if (pred && at < room) {
-      indp[out_base + at] = v;
-      ws += (unsigned long long)__ldg(dplus + v);
-    }
-    pos += __popc(msk);
-  }
-  __syncwarp();
-  return warp_sum(ws);
-}
-
-template <class View>
-__global__ void __launch_bounds__(256) k_orient_fill(const View g, const int32_t n, const int32_t* __restrict__ dplus,
-                                                     const int64_t* __restrict__ offp, int32_t* __restrict__ indp,
-                                                     const int64_t e_cap, int32_t* __restrict__ large,
-                                                     int32_t* __restrict__ medium, DevStatus* __restrict__ st,
-                                                     const int warp_max, const int shard, const int nshards) {
-  TC_DBG_ENTER(5);
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+// Orientation bookkeeping of a finished vertex u with out-degree a (warp-uniform call): its
+// offset and out-degree, the work figures and its tier queue.
+struct OrientAcc {
   unsigned long long work = 0, ei = 0;
   unsigned mx = 0;
-  int nbl = 0, nbm = 0;
-  int32_t bufl = 0, bufm = 0;
-  unsigned bad = 0;
-  for (int64_t uu = gw; uu < n; uu += nw) {
-    const int32_t u = (int32_t)uu;
-    const int64_t s = g.start(u);
-    const int32_t d = g.len(u);
-    const int64_t base = offp[u];
-    const int32_t a = dplus[u];
-    if (base + a > e_cap) {
-      bad |= kBadCapacity;
-      continue;
-    }
-    // hubs: chunk 0 here (it starts at the list's own offset), the rest in k_orient_fill_hub
-    const unsigned long long ws = orient_fill_range(g, n, u, d, s, 0, min(d, kHubChunk), dplus, indp, base, a);
-    if (lane == 0) {
-      work += ws + (unsigned long long)a * (unsigned long long)a;
-      if (d >= 2) ei += (unsigned long long)a;
-      mx = max(mx, (unsigned)a);
-    }
-    if ((u % nshards) == shard) {
-      if (a > warp_max) {
-        if (lane == nbl) bufl = u;
-        if (++nbl == kWarp) {
-          unsigned at = 0;
-          if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)kWarp);
-          __syncwarp();
-          at = __shfl_sync(kFull, at, 0);
-          large[at + lane] = bufl;
-          nbl = 0;
-        }
-      } else if (a > kSmallMax) {
-        if (lane == nbm) bufm = u;
-        if (++nbm == kWarp) {
-          unsigned at = 0;
-          if (lane == 0) at = atomicAdd(&st->n_medium, (unsigned)kWarp);
-          __syncwarp();
-          at = __shfl_sync(kFull, at, 0);
-          medium[at + lane] = bufm;
-          nbm = 0;
-        }
-      }
-    }
-  }
-  if (nbl) {
-    unsigned at = 0;
-    if (lane == 0) at = atomicAdd(&st->n_large, (unsigned)nbl);
-    __syncwarp();
-    at = __shfl_sync(kFull, at, 0);
-    if (lane < nbl) large[at + lane] = bufl;
-  }
-  if (nbm) {
-    unsigned at = 0;
-    if (lane == 0) at = atomicAdd(&st->n_medium, (unsigned)nbm);
-    __syncwarp();
-    at = __shfl_sync(kFull, at, 0);
-    if (lane < nbm) medium[at + lane] = bufm;
-  }
-  __syncwarp();
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  TierBuf large, medium;
+};
+
+__device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, const int64_t s, const int32_t a,
+                                              int32_t* __restrict__ dplus, int64_t* __restrict__ offp,
+                                              int32_t* __restrict__ large, int32_t* __restrict__ medium,
+                                              DevStatus* __restrict__ st, const int warp_max, const int shard,
+                                              const int nshards, OrientAcc& acc) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const bool mine = (u % nshards) == shard;
   if (lane == 0) {
-    if (work) atomicAdd(&st->oriented_work, work);
-    if (ei) atomicAdd(&st->edges_intersected, ei);
-    if (mx) atomicMax(&st->max_dplus, mx);
-    if (bad) atomicOr(&st->bad_flags, bad);
+    dplus[u] = a;
+    offp[u] = s;
+    if (d >= 2) acc.ei += (unsigned long long)a;
+    if (a >= 2 && mine) acc.work += (unsigned long long)a * (unsigned long long)a;
+    acc.mx = max(acc.mx, (unsigned)a);
   }
-  TC_DBG_EXIT(5);
+  if (mine) {
+    if (a > warp_max) acc.large.push(u, large, &st->n_large);
+    else if (a > kSmallMax) acc.medium.push(u, medium, &st->n_medium);
+  }
 }
 
+// Register the vertices whose list is longer than kHubChunk: they are oriented in chunks that
+// separate warps take. One thread per vertex; hubs are rare. A hub starts with out-degree 0,
+// so a hub that is never completed (capacity error) leaves nothing for the count to read.
 template <class View>
-__global__ void __launch_bounds__(256) k_orient_fill_hub(const View g, const int32_t n, const int32_t* __restrict__ dplus,
-                                                         const int64_t* __restrict__ offp, int32_t* __restrict__ indp,
-                                                         const int64_t e_cap, const int32_t* __restrict__ hub_u,
-                                                         const int32_t* __restrict__ hub_base,
-                                                         const int32_t* __restrict__ hub_cnt,
-                                                         const int32_t* __restrict__ chunk_hub,
-                                                         const int64_t chunk_cap, DevStatus* __restrict__ st) {
-  TC_DBG_ENTER(8);
+__global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n, int32_t* __restrict__ dplus,
+                                                   int64_t* __restrict__ offp, int32_t* __restrict__ hub_u,
+                                                   int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_done,
+                                                   int32_t* __restrict__ chunk_hub, const int64_t hub_cap,
+                                                   const int64_t chunk_cap, DevStatus* __restrict__ st) {
+  for (int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; uu < n; uu += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t u = (int32_t)uu;
+    const int32_t d = g.len(u);
+    if (d <= kHubChunk) continue;
+    dplus[u] = 0;
+    offp[u] = 0;
+    const int nch = (d + kHubChunk - 1) / kHubChunk;
+    const unsigned h = atomicAdd(&st->n_hubs, 1u);
+    const unsigned base = atomicAdd(&st->n_hub_chunks, (unsigned)nch);
+    const bool ok = h < hub_cap && (int64_t)base + nch <= chunk_cap;
+    if (ok) {
+      hub_u[h] = u;
+      hub_base[h] = (int32_t)base;
+      hub_done[h] = 0;
+    } else {
+      atomicOr(&st->bad_flags, kBadCapacity);
+    }
+    for (int c = 0; c < nch && (int64_t)base + c < chunk_cap; ++c) chunk_hub[base + c] = ok ? (int32_t)h : -1;
+  }
+}
+
+// Single-pass orientation into the input's own index space: N+(u) is written at
+// indp[start(u) ...], so no offsets scan is needed (offp[u] = start(u)). A persistent grid of
+// warps first takes hub chunks from one queue, then tiles of vertex ids from another. A hub
+// chunk is written at its own position in the hub's list; the warp that finishes a hub's last
+// chunk (a counter per hub) moves the pieces together and completes the vertex.
+template <class View, bool kWrite>
+__global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, int32_t* __restrict__ dplus,
+                                                int64_t* __restrict__ offp, int32_t* __restrict__ indp,
+                                                const int64_t e_cap, int32_t* __restrict__ large,
+                                                int32_t* __restrict__ medium, const int32_t* __restrict__ hub_u,
+                                                const int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_cnt,
+                                                int32_t* __restrict__ hub_done, const int32_t* __restrict__ chunk_hub,
+                                                const int64_t hub_cap, const int64_t chunk_cap, DevStatus* __restrict__ st,
+                                                const int warp_max, const int shard, const int nshards) {
   const int lane = threadIdx.x & (kWarp - 1);
   const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
-  unsigned long long work = 0;
+  const unsigned nhubs = (unsigned)min((long long)st->n_hubs, (long long)hub_cap);
+  unsigned long long chk = 0;
   unsigned bad = 0;
+  OrientAcc acc;
+
+  // Hub chunks.
   while (true) {
     unsigned q = 0;
-    if (lane == 0) q = atomicAdd(&st->q_hub_fill, 1u);
+    if (lane == 0) q = atomicAdd(&st->q_orient_hub, 1u);
     __syncwarp();
     q = __shfl_sync(kFull, q, 0);
     if (q >= nchunks) break;
     const int h = chunk_hub[q];
-    if (h < 0 || h >= (int)st->n_hubs) continue;
+    if (h < 0 || h >= (int)nhubs) continue;
     const int hb = hub_base[h];
-    const int c = (int)q - hb;
-    if (c <= 0) continue;  // chunk 0 is written by k_orient_fill
     const int32_t u = hub_u[h];
     const int64_t s = g.start(u);
     const int32_t d = g.len(u);
-    const int32_t a = dplus[u];
-    // entries of this chunk go after those of the chunks before it
-    int prefix = 0;
-    for (int cc = lane; cc < c; cc += kWarp) prefix += hub_cnt[hb + cc];
-    __syncwarp();
-    prefix = warp_sum(prefix);
-    if (offp[u] + a > e_cap || prefix > a) {
+    const int nch = (d + kHubChunk - 1) / kHubChunk;
+    const int c = (int)q - hb;
+    if (c < 0 || c >= nch) continue;
+    if (s < 0 || s + d > e_cap) {
       bad |= kBadCapacity;
       continue;
     }
     const int32_t k_begin = c * kHubChunk, k_end = min(d, k_begin + kHubChunk);
-    const unsigned long long ws =
-        orient_fill_range(g, n, u, d, s, k_begin, k_end, dplus, indp, offp[u] + prefix, a - prefix);
-    if (lane == 0) work += ws;
+    const int cnt = orient_range<View, kWrite>(g, n, u, d, s, k_begin, k_end, indp, s + k_begin, chk, bad);
+    // Publish this chunk (entries written by every lane, then its count), then count it done.
+    if (lane == 0) hub_cnt[q] = cnt;
+    __threadfence();
+    __syncwarp();
+    int done = 0;
+    if (lane == 0) done = atomicAdd(&hub_done[h], 1);
+    __syncwarp();
+    done = __shfl_sync(kFull, done, 0);
+    if (done != nch - 1) continue;
+    // Last chunk of this hub: gather the pieces (each chunk's out-neighbours start at the
+    // chunk's own position; moving them down in chunk order never overwrites an unread entry).
+    __threadfence();
+    int a = 0;
+    for (int cc = 0; cc < nch; ++cc) {
+      const int cn = __ldcg(hub_cnt + hb + cc);
+      if (kWrite && cc > 0 && cn > 0) {
+        const int64_t src = s + (int64_t)cc * kHubChunk, dst = s + a;
+        for (int k0 = 0; k0 < cn; k0 += kWarp) {
+          const int k = k0 + lane;
+          const int32_t x = k < cn ? __ldcg(indp + src + k) : 0;
+          __syncwarp();
+          if (k < cn) indp[dst + k] = x;
+          __syncwarp();
+        }
+      }
+      a += cn;
+    }
+    finish_vertex(u, d, s, a, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
   }
+
+  // Vertex tiles (hubs skipped: done above).
+  constexpr int kTile = 32;
+  while (true) {
+    unsigned t0 = 0;
+    if (lane == 0) t0 = atomicAdd(&st->q_orient_vtx, (unsigned)kTile);
+    __syncwarp();
+    t0 = __shfl_sync(kFull, t0, 0);
+    if (t0 >= (unsigned)n) break;
+    const int32_t uu = (int32_t)t0 + lane;
+    const int32_t dl = uu < n ? g.len(uu) : 0;
+    const int64_t sl = uu < n ? g.start(uu) : 0;
+    const int cnt_t = min(kTile, n - (int32_t)t0);
+    for (int i = 0; i < cnt_t; ++i) {
+      const int32_t u = (int32_t)t0 + i;
+      const int32_t d = __shfl_sync(kFull, dl, i);
+      const int64_t s = __shfl_sync(kFull, sl, i);
+      if (d > kHubChunk) continue;
+      if (s < 0 || s + d > e_cap) {
+        bad |= kBadCapacity;
+        finish_vertex(u, 0, 0, 0, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
+        continue;
+      }
+      const int a = d > 0 ? orient_range<View, kWrite>(g, n, u, d, s, 0, d, indp, s, chk, bad) : 0;
+      finish_vertex(u, d, s, a, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
+    }
+  }
+
+  acc.large.flush(large, &st->n_large);
+  acc.medium.flush(medium, &st->n_medium);
   __syncwarp();
+  chk = warp_sum(chk);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
   if (lane == 0) {
-    if (work) atomicAdd(&st->oriented_work, work);
+    if (chk) atomicAdd(&st->sym_checksum, chk);
     if (bad) atomicOr(&st->bad_flags, bad);
+    if (acc.work) atomicAdd(&st->oriented_work, acc.work);
+    if (acc.ei) atomicAdd(&st->edges_intersected, acc.ei);
+    if (acc.mx) atomicMax(&st->max_dplus, acc.mx);
   }
-  TC_DBG_EXIT(8);
 }
 
 // ---- exclusive scan of int32 counts into int64 offsets ------------------------------------
@@ -892,7 +838,10 @@ int orient_grid(int64_t n) {
   return (int)std::max<int64_t>(1, std::min(want, cap));
 }
 
-int hub_grid() { return device_info().sms * 8; }
+int hubs_grid(int64_t n) {
+  const int64_t want = (n + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)device_info().sms * 8));
+}
 
 template <int PV>
 tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const SchedParams& sp,
@@ -919,22 +868,40 @@ tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const Sche
   return TC_OK;
 }
 
+// Grid of a persistent kernel: every CTA resident at once (occupancy looked up once per device).
+template <auto kernel>
+tc_status resident_grid(int threads, int* grid) {
+  constexpr int kMaxDev = 64;
+  static int per_sm[kMaxDev] = {};
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  if (per_sm[dev] == 0) {
+    int b = 0;
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, threads, 0));
+    per_sm[dev] = std::max(1, b);
+  }
+  *grid = device_info().sms * per_sm[dev];
+  return TC_OK;
+}
+
 template <class View>
-tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& sp, bool fill, cudaStream_t stream) {
-  const int grid = orient_grid(n);
-  k_orient_count<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.hub_u, ws.hub_base, ws.hub_cnt, ws.chunk_hub,
-                                                 ws.hub_cap, ws.chunk_cap, ws.st);
+tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& sp, bool write, cudaStream_t stream) {
+  k_find_hubs<View><<<hubs_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.hub_u, ws.hub_base, ws.hub_done,
+                                                      ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st);
   TC_CUDA_TRY(cudaGetLastError());
-  k_orient_count_hub<View><<<hub_grid(), 256, 0, stream>>>(view, n, ws.dplus, ws.hub_u, ws.hub_base, ws.hub_cnt,
-                                                           ws.chunk_hub, ws.chunk_cap, ws.st);
-  TC_CUDA_TRY(cudaGetLastError());
-  if (!fill) return TC_OK;
-  TC_TRY(scan_counts(ws.dplus, n, ws.offp, ws.tile_sums, stream));
-  k_orient_fill<View><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.medium,
-                                                ws.st, sp.warp_max, sp.shard, sp.nshards);
-  TC_CUDA_TRY(cudaGetLastError());
-  k_orient_fill_hub<View><<<hub_grid(), 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.hub_u,
-                                                          ws.hub_base, ws.hub_cnt, ws.chunk_hub, ws.chunk_cap, ws.st);
+  int grid = 0;
+  if (write) TC_TRY((resident_grid<k_orient<View, true>>(256, &grid)));
+  else TC_TRY((resident_grid<k_orient<View, false>>(256, &grid)));
+  if (write)
+    k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.medium,
+                                                   ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
+                                                   ws.hub_cap, ws.chunk_cap, ws.st, sp.warp_max, sp.shard, sp.nshards);
+  else
+    k_orient<View, false><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large,
+                                                    ws.medium, ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done,
+                                                    ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st, sp.warp_max,
+                                                    sp.shard, sp.nshards);
   TC_CUDA_TRY(cudaGetLastError());
   return TC_OK;
 }
@@ -993,7 +960,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);
-    prof_launches(scan_tiles(n) > 0 ? 8 : 5);
+    prof_launches(3);
   }
   (void)m;
   if (triangles_dev)
