@@ -4,7 +4,9 @@ Imported by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, as 
   - liboracle.so: the plain-C restatement in tc_oracle.c (always present after build);
   - _ref/libref_cct.so: the reference's own hostCountTriangles (tests/cct.cpp:71-89) compiled
     from the reference sources by oracle/Makefile (present when the reference was available at
-    build time; it travels with the repository snapshot, the sources do not).
+    build time; it travels with the repository snapshot, the sources do not);
+  - _ref/libref_cct_gpu.so: the reference's own raw-CSR GPU counter (tests/cct_csr.cu:228-285)
+    compiled for sm_100a the same way, for side-by-side timing and per-vertex parity.
 """
 from __future__ import annotations
 
@@ -16,6 +18,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None
 _ref = None
+_ref_gpu = None
 
 _P = ctypes.c_void_p
 
@@ -73,6 +76,27 @@ def ref():
         L.ref_host_count_triangles_omp_sample.restype = ctypes.c_int64
         _ref = L
     return _ref
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libref_cct_gpu.so"))
+
+
+def ref_gpu():
+    """The reference's callDeviceAllTrianglesCSR behind ref_gpu_count_csr(nv, d_off, d_ind, d_out,
+    threads_per_intersection, shifter, blocks, block_size) -> cudaError_t (launch only, default
+    stream). d_ind must have readable guard entries before and after the list array."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        path = os.path.join(_HERE, "_ref", "libref_cct_gpu.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: the reference was not present at build time")
+        L = ctypes.CDLL(path)
+        i32 = ctypes.c_int32
+        L.ref_gpu_count_csr.argtypes = [i32, _P, _P, _P, i32, i32, i32, i32]
+        L.ref_gpu_count_csr.restype = ctypes.c_int
+        _ref_gpu = L
+    return _ref_gpu
 
 
 class _Batch(ctypes.Structure):
