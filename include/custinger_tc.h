@@ -245,11 +245,14 @@ tc_status tc_mlp_adam_step(float* d_params, const float* d_grad, float* d_m, flo
 tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strategy, const float* d_label, int32_t n,
                        int32_t epochs, float lr, float* loss_host, void* stream);
 
-/* Fill a scheduler from a trained MLP (device parameters): for every degree cell the
- * strategy with the lowest predicted cost among those of `kind` (0 = static count: hash probe
- * or search; 1 = streaming delta: search or merge) goes into s->table and s->use_table = 1.
- * cell_features (host, 256 x TC_MLP_IN floats) are the features of each cell, e.g. from
- * tc_cell_stats; NULL uses the cells' nominal degrees. */
+/* Fill a scheduler from a trained MLP (device parameters) whose outputs are predicted log2
+ * costs per edge of each strategy: for every degree cell, the choice between the two strategies
+ * of `kind` (0 = static count: hash probe or search; 1 = streaming delta: search or merge) goes
+ * into s->table and s->use_table = 1. The fixed threshold rule (s->search_ratio_x16 on the
+ * cell's mean degrees) is the fallback: a cell takes the other strategy only when the network
+ * predicts it at least 5% cheaper. cell_features (host, 256 x TC_MLP_IN floats: mean
+ * log2(1 + d+(u)), mean log2(1 + d+(v)), mean min/max degree ratio, cell id / 255) describe each
+ * cell, e.g. from tc_cell_stats; NULL uses the cells' nominal degrees. */
 tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* s, void* stream);
 
 /* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching

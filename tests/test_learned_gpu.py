@@ -1,0 +1,91 @@
+"""Learned scheduler: the committed network's table never changes a count, and what it gains.
+
+The network (custingeralg_b200/data/sched_mlp.bin) is trained by
+`python -m custingeralg_b200.sched_learn all` on timings of the count kernel itself. These tests
+check that its table keeps every count bit-exact (handle and CSR per-vertex modes) on graphs it
+was not trained on, and report its time against the fixed threshold rule.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from custingeralg_b200 import api, generators as G, native as N
+from custingeralg_b200 import sched_learn as L
+from oracle import pyoracle as O
+
+pytestmark = pytest.mark.gpu
+
+needs_weights = pytest.mark.skipif(not os.path.exists(L.WEIGHTS), reason="no trained weights committed")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def test_cell_stats_sum_to_oriented_edges():
+    torch = _torch()
+    g = G.rmat(12, 16, seed=9)
+    graph = api.Graph.from_csr(g)
+    out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    graph.count(N.TC_PV_HANDLE, out)
+    stats = L.cell_stats(graph)
+    assert int(round(stats[:, 0].sum())) == g.m // 2
+    feat = L.cell_features(stats)
+    assert feat.shape == (256, 4) and np.isfinite(feat).all()
+
+
+def test_forced_strategies_and_cell_filters_keep_the_count():
+    torch = _torch()
+    g = G.rmat(13, 16, seed=4)
+    graph = api.Graph.from_csr(g)
+    out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    T_ref, _ = graph.count(N.TC_PV_HANDLE, out)
+    ref = out.clone()
+    for strategy in (0, 1):
+        T, _ = graph.count(N.TC_PV_HANDLE, out, sched=L.forced(strategy))
+        assert T == T_ref and torch.equal(out, ref)
+    # the per-cell filters partition the work: their triangle totals add up
+    stats = L.cell_stats(graph)
+    total = 0
+    for c in np.nonzero(stats[:, 0])[0]:
+        T, _ = graph.count(N.TC_PV_NONE, None, sched=L.forced(0, int(c)))
+        total += T
+    assert total == T_ref
+    T_none, _ = graph.count(N.TC_PV_NONE, None, sched=L.forced(0, -2))
+    assert T_none == 0
+
+
+def test_untrained_network_keeps_counts():
+    """Whatever the network predicts, the count is the oracle's."""
+    torch = _torch()
+    params = np.zeros(N.MLP_PARAMS, dtype=np.float32)
+    N.check(N.lib().tc_mlp_init(params.ctypes.data, 123))
+    g = G.barabasi_albert(1 << 12, 6, seed=5)
+    graph = api.Graph.from_csr(g)
+    out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    graph.count(N.TC_PV_HANDLE, out)
+    s = L.learned_sched(params, graph)
+    assert s.use_table == 1
+    T, _ = graph.count(N.TC_PV_HANDLE, out, sched=s)
+    tot, pv = O.fast_count(g.n, g.off, g.ind)
+    assert T == tot // 6
+    assert np.array_equal(out[:g.n].cpu().numpy(), pv)
+
+
+@needs_weights
+@pytest.mark.parametrize("spec", [("rmat", dict(scale=17, a=0.57, seed=1717)),
+                                  ("ba", dict(n_log=17, m0=16, seed=1718)),
+                                  ("er", dict(n_log=17, deg=40, seed=1719))],
+                         ids=["rmat17", "ba17", "er17"])
+def test_learned_table_is_exact_and_reports_gain(spec):
+    params = L.load()
+    r = L.evaluate_graph(params, spec, reps=5)
+    print(json.dumps(r))
+    assert r["counts_equal"]
+    g = L.make_graph(spec)
+    assert r["triangles"] == O.fast_count(g.n, g.off, g.ind, per_vertex=False)[0] // 6
+    # the fallback keeps the learned table from losing much where it departs from the rule
+    assert r["learned_ms"] <= 1.15 * r["fixed_ms"] + 0.05
