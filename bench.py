@@ -22,6 +22,7 @@ vertices, extrapolated to the whole graph, on rank 0 only.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -226,6 +227,7 @@ def run_ours(a, rank, world, local_rank):
     # One synchronous count for the structural check, the work figures and the answer.
     T_full, info = graph.count(N.TC_PV_HANDLE, out, tri, sched=N.default_sched())
     ref_T = None
+    checks = {"triangles": "no known answer for this graph"}
     gold_path = os.path.join(ROOT, "tests", "golden", "bench_configs.json")
     if os.path.exists(gold_path):
         gold = json.load(open(gold_path)).get(f"rmat{a.scale}_ef{a.edge_factor}_s{a.seed}")
@@ -233,6 +235,11 @@ def run_ours(a, rank, world, local_rank):
             ref_T = gold["triangles"]
             if ref_T != T_full:
                 raise SystemExit(f"count mismatch: {T_full} vs known answer {ref_T}")
+            pv = out[:g.n].cpu().numpy()
+            pv_digest = hashlib.sha256(np.ascontiguousarray(pv).astype("<i4").tobytes()).hexdigest()[:32]
+            if pv_digest != gold["per_vertex_handle_digest"]:
+                raise SystemExit("per-vertex counts differ from the known answer's digest")
+            checks = {"triangles": "equals the known answer", "per_vertex_2t": "digest equals the known answer"}
     assert info.edges_intersected == e_int, (info.edges_intersected, e_int)
 
     def step():
@@ -310,7 +317,7 @@ def run_ours(a, rank, world, local_rank):
               "warmup": a.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
               "scaling": "strong", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
               "config": workload_config(a, g.n, g.m, e_int),
-              "triangles": T_full, "gpu_launches": launches, "roofline": roofline,
+              "triangles": T_full, "checks": checks, "gpu_launches": launches, "roofline": roofline,
               "phase_ms": {"orient": round(statistics.mean(orient_ms), 4),
                            "count": round(statistics.mean(count_ms), 4)},
               "clocks": clocks.summary(t_wall0, t_wall1)}
