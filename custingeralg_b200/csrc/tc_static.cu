@@ -160,21 +160,12 @@ __device__ __forceinline__ void hash_insert(int32_t* keys, IdxT* idx, int bbits,
   }
 }
 
-// Slot holding key, or -1. One 128-bit load per bucket visited; the first bucket is resolved
-// without branches, the chain continues only when that bucket is full and lacks the key.
-__device__ __forceinline__ int hash_find(const int32_t* keys, int bbits, int32_t key) {
+// Continue a lookup whose first bucket b was full and lacked key: slot of key, or -1.
+__device__ __forceinline__ int hash_find_after(const int32_t* keys, int bbits, int32_t key, uint32_t b) {
   const uint32_t bmask = (1u << bbits) - 1;
-  uint32_t b = hash_bucket(key, bbits);
-  int4 q = *reinterpret_cast<const int4*>(keys + 4 * b);
-  int pos = q.w == key ? 3 : -1;
-  pos = q.z == key ? 2 : pos;
-  pos = q.y == key ? 1 : pos;
-  pos = q.x == key ? 0 : pos;
-  if (pos >= 0) return 4 * b + pos;
-  if (q.w == -1) return -1;  // slots fill in order: a free last slot means the bucket is not full
   for (uint32_t it = 0; it < bmask; ++it) {
     b = (b + 1) & bmask;
-    q = *reinterpret_cast<const int4*>(keys + 4 * b);
+    const int4 q = *reinterpret_cast<const int4*>(keys + 4 * b);
     if (q.x == key) return 4 * b;
     if (q.y == key) return 4 * b + 1;
     if (q.z == key) return 4 * b + 2;
@@ -281,6 +272,7 @@ __device__ __forceinline__ void process_group(
       }
     } else {
       // ---- probe strategy: stream N+(v) and probe each element into the hash set ----
+      uint32_t hits = 0;
       for (int k0 = lane; k0 < sb; k0 += kUnroll * kWarp) {
         int32_t w[kUnroll];
 #pragma unroll
@@ -290,24 +282,36 @@ __device__ __forceinline__ void process_group(
         }
 #pragma unroll
         for (int j = 0; j < kUnroll; ++j) {
-          if (w[j] < 0) continue;
-          const int s = hash_find(hkeys, bits, w[j]);
-          if (s >= 0) {
-            ++tri;
-            if (PV == TC_PV_HANDLE) {
-              ++vacc;
-              atomicAdd(&cnt[hidx[s]], 1u);
-            } else if (PV == TC_PV_CSR) {
-              uint32_t wu, wv, ww;
-              tri_weights<PV>(u, sv, w[j], wu, wv, ww);
-              u_acc += wu;
-              vacc += wv;
-              if (ww) atomicAdd(&cnt[hidx[s]], ww);
+          const int32_t key = w[j];
+          if (key < 0) continue;
+          // First bucket in one 128-bit load; the common case (a miss in a bucket with a free
+          // slot) ends here without computing a slot.
+          const uint32_t bk = hash_bucket(key, bits);
+          const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
+          const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
+          if (hit | (q.w != -1)) {
+            const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
+                              : hash_find_after(hkeys, bits, key, bk);
+            if (s >= 0) {
+              ++hits;
+              if (PV == TC_PV_HANDLE) {
+                atomicAdd(&cnt[hidx[s]], 1u);
+              } else if (PV == TC_PV_CSR) {
+                uint32_t wu, wv, ww;
+                tri_weights<PV>(u, sv, key, wu, wv, ww);
+                u_acc += wu;
+                vacc += wv;
+                if (ww) atomicAdd(&cnt[hidx[s]], ww);
+              }
             }
           }
         }
       }
-      if (PV == TC_PV_HANDLE) u_acc += vacc;
+      tri += hits;
+      if (PV == TC_PV_HANDLE) {
+        u_acc += hits;
+        vacc = hits;
+      }
     }
     // v-role count: into the chunk counter when v is staged, else global.
     if (PV != TC_PV_NONE) {
