@@ -90,16 +90,20 @@ tc_status Workspace::ensure(int64_t n, int64_t m, int64_t extent) {
   if (device >= 0 && device != dev) return fail(TC_ERR_INVALID_ARG, "workspace used on device %d, created on %d", dev, device);
   device = dev;
   if (n + 1 > n_cap) {
-    int64_t c1 = 0, c2 = 0, c3 = 0, c4 = 0;
+    int64_t c1 = 0, c2 = 0, c3 = 0;
     if (dplus) { cudaFree(dplus); dplus = nullptr; }
     if (offp) { cudaFree(offp); offp = nullptr; }
-    if (large) { cudaFree(large); large = nullptr; }
-    if (medium) { cudaFree(medium); medium = nullptr; }
+    if (degv) { cudaFree(degv); degv = nullptr; }
     TC_TRY(grow(dplus, c1, n + 1));
     TC_TRY(grow(offp, c2, n + 1));
-    TC_TRY(grow(large, c3, n + 1));
-    TC_TRY(grow(medium, c4, n + 1));
+    TC_TRY(grow(degv, c3, n + 1));
     n_cap = n + 1;
+  }
+  if (items_for(n, m) > item_cap) {
+    int64_t c1 = 0;
+    if (medium) { cudaFree(medium); medium = nullptr; }
+    TC_TRY(grow(medium, c1, items_for(n, m)));
+    TC_TRY(grow(large, item_cap, items_for(n, m)));
   }
   TC_TRY(grow(indp, e_cap, std::max(m, extent)));
   if (hubs_for(m) > hub_cap) {
@@ -124,6 +128,7 @@ void Workspace::release() {
   cudaFree(dplus);
   cudaFree(offp);
   cudaFree(indp);
+  cudaFree(degv);
   cudaFree(large);
   cudaFree(medium);
   cudaFree(hub_u);

@@ -14,6 +14,7 @@ constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kHubChunk = 2048;     // orientation: list entries per warp work item of a hub
 constexpr int kWarpTierMax = 256;   // largest out-degree a single warp counts on its own
+constexpr int kItemRangeMin = 256;  // fewest neighbours of a count work item (queue sizing)
 
 // ---- error reporting -------------------------------------------------------------------
 
@@ -110,8 +111,10 @@ struct Workspace {
   int32_t* dplus = nullptr;      // [n]
   int64_t* offp = nullptr;       // [n+1]
   int32_t* indp = nullptr;       // [e_cap] N+(u) at indp[start(u) ...] (the input's own index space)
-  int32_t* large = nullptr;      // [n]
-  int32_t* medium = nullptr;     // [n]
+  int32_t* degv = nullptr;       // [n] deg(u)
+  unsigned long long* large = nullptr;   // [item_cap] count work items (centre << 32 | first neighbour)
+  unsigned long long* medium = nullptr;  // [item_cap]
+  int64_t item_cap = 0;
   int32_t* hub_u = nullptr;      // [hub_cap] vertices split into chunks
   int32_t* hub_base = nullptr;   // [hub_cap] their first chunk index
   int32_t* hub_cnt = nullptr;    // [chunk_cap] out-neighbours found per chunk
@@ -126,6 +129,8 @@ struct Workspace {
   // Hub arrays needed for a graph of m directed edges.
   static int64_t hubs_for(int64_t m) { return m / kHubChunk + 1; }
   static int64_t chunks_for(int64_t m) { return 2 * (m / kHubChunk) + 2; }
+  // Count work items of one queue: at most one per vertex plus one per kItemRangeMin neighbours.
+  static constexpr int64_t items_for(int64_t n, int64_t m) { return n + m / kItemRangeMin + 1; }
 };
 
 // Device properties cached per device.

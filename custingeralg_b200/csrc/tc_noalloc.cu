@@ -27,16 +27,18 @@ constexpr int64_t kMaxEdges = TC_NOALLOC_MAX_EDGES;
 constexpr int64_t kMaxHubs = kMaxEdges / kHubChunk + 1;
 constexpr int64_t kMaxChunks = 2 * (kMaxEdges / kHubChunk) + 2;
 
-// Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | dplus int32[maxnv+1]
-// | large int32[maxnv+1] | medium int32[maxnv+1] | hub_u, hub_base, hub_done int32[hubs]
+// Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | dplus, degv
+// int32[maxnv+1] | large, medium uint64[items] | hub_u, hub_base, hub_done int32[hubs]
 // | hub_cnt, chunk_hub int32[chunks] | indp int32[max_edges]
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffStatus = 0;
 constexpr size_t kOffOffp = align256(kOffStatus + sizeof(DevStatus));
 constexpr size_t kOffDplus = align256(kOffOffp + sizeof(int64_t) * (kMaxNv + 1));
-constexpr size_t kOffLarge = align256(kOffDplus + sizeof(int32_t) * (kMaxNv + 1));
-constexpr size_t kOffMedium = align256(kOffLarge + sizeof(int32_t) * (kMaxNv + 1));
-constexpr size_t kOffHubU = align256(kOffMedium + sizeof(int32_t) * (kMaxNv + 1));
+constexpr int64_t kMaxItems = Workspace::items_for(kMaxNv, kMaxEdges);
+constexpr size_t kOffDegv = align256(kOffDplus + sizeof(int32_t) * (kMaxNv + 1));
+constexpr size_t kOffLarge = align256(kOffDegv + sizeof(int32_t) * (kMaxNv + 1));
+constexpr size_t kOffMedium = align256(kOffLarge + sizeof(unsigned long long) * kMaxItems);
+constexpr size_t kOffHubU = align256(kOffMedium + sizeof(unsigned long long) * kMaxItems);
 constexpr size_t kOffHubBase = align256(kOffHubU + sizeof(int32_t) * kMaxHubs);
 constexpr size_t kOffHubDone = align256(kOffHubBase + sizeof(int32_t) * kMaxHubs);
 constexpr size_t kOffHubCnt = align256(kOffHubDone + sizeof(int32_t) * kMaxHubs);
@@ -107,8 +109,10 @@ extern "C" tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, co
   ws.st = reinterpret_cast<DevStatus*>(base + kOffStatus);
   ws.offp = reinterpret_cast<int64_t*>(base + kOffOffp);
   ws.dplus = reinterpret_cast<int32_t*>(base + kOffDplus);
-  ws.large = reinterpret_cast<int32_t*>(base + kOffLarge);
-  ws.medium = reinterpret_cast<int32_t*>(base + kOffMedium);
+  ws.degv = reinterpret_cast<int32_t*>(base + kOffDegv);
+  ws.large = reinterpret_cast<unsigned long long*>(base + kOffLarge);
+  ws.medium = reinterpret_cast<unsigned long long*>(base + kOffMedium);
+  ws.item_cap = kMaxItems;
   ws.hub_u = reinterpret_cast<int32_t*>(base + kOffHubU);
   ws.hub_base = reinterpret_cast<int32_t*>(base + kOffHubBase);
   ws.hub_done = reinterpret_cast<int32_t*>(base + kOffHubDone);

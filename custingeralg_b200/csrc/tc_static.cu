@@ -50,7 +50,9 @@ constexpr int kWarps = kThreads / kWarp;
 constexpr int kChunk = 1024;      // A entries staged per pass for an L-tier vertex
 constexpr int kHashMax = 2048;    // hash slots for such a chunk (load <= 0.5)
 constexpr int kUnroll = 4;        // list elements a lane loads before probing (independent loads)
-constexpr int kSmallMax = 32;     // S tier: out-degree up to one warp group
+constexpr int kWarpRange = 256;   // neighbours of a warp-tier centre per work item
+constexpr int kCtaRange = 512;    // neighbours of a CTA-tier centre per work item
+static_assert(kWarpRange >= kItemRangeMin && kCtaRange >= kItemRangeMin, "queue sizing");
 constexpr int kMedSlots = 2 * kWarpTierMax;  // warp-private hash slots (load <= 0.25 up to a = 128, else <= 0.5)
 // Hash sets are bucketized: 4 slots per 16-byte bucket, probed with one 128-bit shared load,
 // so a lookup ends after one bucket unless that bucket is full (rare at these loads).
@@ -87,7 +89,7 @@ __device__ unsigned long long* tc_dbg_kern = nullptr;
   } while (0)
 #endif
 
-// Warp-private staging of one vertex (S and M tiers).
+// Warp-private staging of one centre's N+(c) (warp tier).
 struct WarpTable {
   alignas(16) int32_t hkeys[kMedSlots];
   int32_t sA[kWarpTierMax];
@@ -95,7 +97,7 @@ struct WarpTable {
   uint8_t hidx[kMedSlots];
 };
 
-// CTA-shared staging of one chunk of an L-tier vertex.
+// CTA-shared staging of one chunk of a CTA-tier centre's N+(c).
 struct BlockTable {
   alignas(16) int32_t hkeys[kHashMax];
   int32_t sA[kChunk];
@@ -109,8 +111,7 @@ struct CountSmem {
     WarpTable W[kWarps];
   } t;
   unsigned long long tri[kWarps];
-  unsigned long long work[kWarps];
-  unsigned item;
+  unsigned long long item;
   int gctr;
 };
 
@@ -175,25 +176,9 @@ __device__ __forceinline__ int hash_find_after(const int32_t* keys, int bbits, i
   return -1;
 }
 
-__device__ __forceinline__ bool search_sorted(const int32_t* __restrict__ list, int len, int32_t key) {
-  int lo = 0, hi = len;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(list + mid) < key) lo = mid + 1;
-    else hi = mid;
-  }
-  return lo < len && __ldg(list + lo) == key;
-}
-
 __device__ __forceinline__ int log2_cell(int x) {
   const int c = 31 - __clz(max(x, 1));
   return min(c, 15);
-}
-
-__device__ __forceinline__ bool use_search(const SchedParams& sp, int a, int b) {
-  if (sp.use_table) return sp.table[log2_cell(a)][log2_cell(b)] == 1;
-  const int lg = 32 - __clz(b);
-  return 16LL * b > (long long)sp.search_ratio_x16 * a * lg;
 }
 
 // Weights a found triangle (u, v, w) adds to each vertex's per-vertex output.
@@ -217,122 +202,114 @@ __host__ __device__ constexpr uint32_t flush_mult() {
   return PV == TC_PV_HANDLE ? 2u : 1u;
 }
 
-// One warp intersects N+(u) with N+(v) for the out-neighbours v = A[g0 .. g0+gcount) of u.
-// The current chunk of A (entries [chunk_base, chunk_base+chunk_len)) is in shared memory as
-// sA and as a hash set of 2^bits buckets (hidx[slot] = entry); cnt[] holds the chunk's
-// per-entry counters.
-//
-// The out-neighbours are taken one at a time (warp-uniform). For each, either the warp streams
-// N+(v) with coalesced loads, kUnroll elements per lane in flight, and probes the hash set
-// (probe strategy), or it binary-searches the chunk's entries in N+(v) (search strategy).
-// Almost all probe work lies in lists of 32 or more entries, so walking one list at a time
-// wastes few lanes and keeps v, its list pointer and its v-role count warp-uniform.
+// Is the edge {c, o} intersected at c? At the endpoint with the larger out-degree (its list is
+// the hash set, the other one is streamed), ties to the smaller id. Both endpoints read the same
+// dplus values, so exactly one of them takes the edge.
+__device__ __forceinline__ bool centre_of(int32_t c, int a, int32_t o, int b) {
+  return b < a || (b == a && c < o);
+}
+
+// Stream the list lst[0 .. len) through the hash set; returns the hits. Per hit, the third
+// vertex's counter cnt[hidx[slot]] gets its weight; vacc and c_acc collect the weights of the
+// streamed list's owner o and of the centre c (TC_PV_CSR only: in handle mode all are the hits).
 template <int PV, typename IdxT>
-__device__ __forceinline__ void process_group(
-    const int32_t u, const int32_t* __restrict__ Ag, const int32_t* sA, const int chunk_base,
-    const int chunk_len, const int32_t* hkeys, const IdxT* hidx, const int bits, uint32_t* cnt,
-    const int g0, const int gcount, const int32_t* __restrict__ dplus,
-    const int64_t* __restrict__ offp, const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
-    const SchedParams& sp, uint32_t& tri, uint32_t& u_acc, unsigned long long& work) {
+__device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
+                                               const int32_t o, const int32_t* hkeys, const IdxT* hidx,
+                                               const int bits, uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
   const int lane = threadIdx.x & (kWarp - 1);
-  const bool valid = lane < gcount;
-  const int i = g0 + lane;
-  const int li = i - chunk_base;
-  const int32_t v = valid ? ((li >= 0 && li < chunk_len) ? sA[li] : __ldg(Ag + i)) : 0;
-  const int b = valid ? __ldg(dplus + v) : 0;
-  if (chunk_base == 0) work += (unsigned)b;  // the d+(v) part of the oriented work, once per edge
-  const int64_t base = valid ? __ldg(offp + v) : 0;
-  const bool active =
-      valid && b > 0 &&
-      (sp.cell_filter == -1 || (sp.cell_filter >= 0 && log2_cell(chunk_len) * 16 + log2_cell(b) == sp.cell_filter));
-  unsigned todo = __ballot_sync(kFull, active);
+  uint32_t hits = 0;
+  for (int k0 = lane; k0 < len; k0 += kUnroll * kWarp) {
+    int32_t w[kUnroll];
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j) {
+      const int k = k0 + j * kWarp;
+      w[j] = k < len ? __ldg(lst + k) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j) {
+      const int32_t key = w[j];
+      if (key < 0) continue;
+      // First bucket in one 128-bit load; the common case (a miss in a bucket with a free
+      // slot) ends here without computing a slot.
+      const uint32_t bk = hash_bucket(key, bits);
+      const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
+      const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
+      if (hit | (q.w != -1)) {
+        const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
+                          : hash_find_after(hkeys, bits, key, bk);
+        if (s >= 0) {
+          ++hits;
+          if (PV == TC_PV_HANDLE) {
+            atomicAdd(&cnt[hidx[s]], 1u);
+          } else if (PV == TC_PV_CSR) {
+            uint32_t wc, wo, ww;
+            tri_weights<PV>(c, o, key, wc, wo, ww);
+            c_acc += wc;
+            vacc += wo;
+            if (ww) atomicAdd(&cnt[hidx[s]], ww);
+          }
+        }
+      }
+    }
+  }
+  return hits;
+}
+
+// One warp takes the neighbours o = nbr[0 .. gcount) of centre c (out-degree a) and
+// intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), is
+// streamed through the hash set of the staged chunk of N+(c) (2^bits buckets, hidx[slot] =
+// entry, cnt[entry] its counter) with coalesced loads, kUnroll per lane in flight. The lists are
+// taken one at a time, so o, its list and its count stay warp-uniform; nearly all of the work
+// lies in lists of 32 entries or more.
+template <int PV, typename IdxT>
+__device__ __forceinline__ void process_group(const int32_t n, const int32_t c, const int a,
+                                              const int32_t* __restrict__ nbr, const int gcount,
+                                              const int32_t* hkeys, const IdxT* hidx,
+                                              const int bits, uint32_t* cnt, const int32_t* __restrict__ dplus,
+                                              const int64_t* __restrict__ offp, const int32_t* __restrict__ indp,
+                                              uint32_t* __restrict__ out, const SchedParams& sp, uint32_t& tri,
+                                              uint32_t& c_acc) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  int32_t o = lane < gcount ? __ldg(nbr + lane) : -1;
+  const bool valid = o >= 0 && o < n;  // ids out of range were flagged by the orientation
+  if (!valid) o = 0;
+  const int b = valid ? __ldg(dplus + o) : 0;
+  const bool mine = valid && b > 0 && centre_of(c, a, o, b) &&
+                    (sp.cell_filter == -1 ||
+                     (sp.cell_filter >= 0 && log2_cell(a) * 16 + log2_cell(b) == sp.cell_filter));
+  const int64_t base = mine ? __ldg(offp + o) : 0;
+  unsigned todo = __ballot_sync(kFull, mine);
   while (todo) {
     const int sl = __ffs(todo) - 1;
     todo &= todo - 1;
-    const int32_t sv = __shfl_sync(kFull, v, sl);
+    const int32_t so = __shfl_sync(kFull, o, sl);
     const int sb = __shfl_sync(kFull, b, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
-    const int sli = __shfl_sync(kFull, li, sl);
-    const int32_t* __restrict__ lst = indp + sbase;
-    uint32_t vacc = 0;  // v-role weight found by this lane
-    if (use_search(sp, chunk_len, sb)) {
-      // ---- search strategy: binary-search the chunk's entries into N+(v) ----
-      for (int j = lane; j < chunk_len; j += kWarp) {
-        const int32_t w = sA[j];
-        if (search_sorted(lst, sb, w)) {
-          ++tri;
-          if (PV != TC_PV_NONE) {
-            uint32_t wu, wv, ww;
-            tri_weights<PV>(u, sv, w, wu, wv, ww);
-            u_acc += wu;
-            vacc += wv;
-            if (ww) atomicAdd(&cnt[j], ww);
-          }
-        }
-      }
-    } else {
-      // ---- probe strategy: stream N+(v) and probe each element into the hash set ----
-      uint32_t hits = 0;
-      for (int k0 = lane; k0 < sb; k0 += kUnroll * kWarp) {
-        int32_t w[kUnroll];
-#pragma unroll
-        for (int j = 0; j < kUnroll; ++j) {
-          const int k = k0 + j * kWarp;
-          w[j] = k < sb ? __ldg(lst + k) : -1;
-        }
-#pragma unroll
-        for (int j = 0; j < kUnroll; ++j) {
-          const int32_t key = w[j];
-          if (key < 0) continue;
-          // First bucket in one 128-bit load; the common case (a miss in a bucket with a free
-          // slot) ends here without computing a slot.
-          const uint32_t bk = hash_bucket(key, bits);
-          const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
-          const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
-          if (hit | (q.w != -1)) {
-            const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
-                              : hash_find_after(hkeys, bits, key, bk);
-            if (s >= 0) {
-              ++hits;
-              if (PV == TC_PV_HANDLE) {
-                atomicAdd(&cnt[hidx[s]], 1u);
-              } else if (PV == TC_PV_CSR) {
-                uint32_t wu, wv, ww;
-                tri_weights<PV>(u, sv, key, wu, wv, ww);
-                u_acc += wu;
-                vacc += wv;
-                if (ww) atomicAdd(&cnt[hidx[s]], ww);
-              }
-            }
-          }
-        }
-      }
-      tri += hits;
-      if (PV == TC_PV_HANDLE) {
-        u_acc += hits;
-        vacc = hits;
-      }
+    uint32_t vacc = 0;
+    const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, hidx, bits, cnt, c_acc, vacc);
+    tri += hits;
+    if (PV == TC_PV_HANDLE) {
+      c_acc += hits;
+      vacc = hits;
     }
-    // v-role count: into the chunk counter when v is staged, else global.
     if (PV != TC_PV_NONE) {
       vacc = warp_sum(vacc);
-      if (lane == 0 && vacc) {
-        if (sli >= 0 && sli < chunk_len) atomicAdd(&cnt[sli], vacc);
-        else atomicAdd(&out[sv], vacc * flush_mult<PV>());
-      }
+      if (lane == 0 && vacc) atomicAdd(&out[so], vacc * flush_mult<PV>());
     }
   }
   __syncwarp();
 }
 
-// One warp counts the triangles whose lowest vertex is u (S and M tiers, a <= kWarpTierMax).
+// One warp counts the edges of centre c (out-degree a <= kWarpTierMax) among its neighbours
+// N(c)[k0 .. k1).
 template <int PV>
-__device__ __forceinline__ void warp_vertex(const int32_t u, const int a, WarpTable& t,
-                                            const int32_t* __restrict__ dplus, const int64_t* __restrict__ offp,
-                                            const int32_t* __restrict__ indp, uint32_t* __restrict__ out,
-                                            const SchedParams& sp, uint32_t& tri, unsigned long long& work) {
+__device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, const int a, const int64_t start,
+                                            const int k0, const int k1, WarpTable& t,
+                                            const int32_t* __restrict__ ind, const int32_t* __restrict__ dplus,
+                                            const int64_t* __restrict__ offp, const int32_t* __restrict__ indp,
+                                            uint32_t* __restrict__ out, const SchedParams& sp, uint32_t& tri) {
   const int lane = threadIdx.x & (kWarp - 1);
-  const int32_t* Ag = indp + __ldg(offp + u);
+  const int32_t* Ag = indp + start;
   int bits = 4;  // buckets: 4 * 2^bits slots >= 4a (load <= 0.25) while they fit in kMedSlots
   while ((1 << bits) < a && (8 << bits) <= kMedSlots) ++bits;
   const int S = 4 << bits;
@@ -344,28 +321,35 @@ __device__ __forceinline__ void warp_vertex(const int32_t u, const int a, WarpTa
   __syncwarp();
   for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, t.hidx, bits, t.sA[j], j);
   __syncwarp();
-  uint32_t u_acc = 0;
-  for (int g0 = 0; g0 < a; g0 += kWarp)
-    process_group<PV>(u, Ag, t.sA, 0, a, t.hkeys, t.hidx, bits, t.cnt, g0, min(kWarp, a - g0), dplus, offp, indp, out,
-                      sp, tri, u_acc, work);
+  uint32_t c_acc = 0;
+  for (int g = k0; g < k1; g += kWarp)
+    process_group<PV>(n, c, a, ind + start + g, min(kWarp, k1 - g), t.hkeys, t.hidx, bits, t.cnt, dplus, offp,
+                      indp, out, sp, tri, c_acc);
   if (PV != TC_PV_NONE) {
     for (int j = lane; j < a; j += kWarp) {
-      const uint32_t c = t.cnt[j];
-      if (c) atomicAdd(&out[t.sA[j]], c * flush_mult<PV>());
+      const uint32_t x = t.cnt[j];
+      if (x) atomicAdd(&out[t.sA[j]], x * flush_mult<PV>());
     }
     __syncwarp();
-    u_acc = warp_sum(u_acc);
-    if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
+    c_acc = warp_sum(c_acc);
+    if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
   }
   __syncwarp();
 }
 
+// Work items of the queues: centre c and the first neighbour index k0 of its range of N(c).
+__device__ __forceinline__ unsigned long long make_item(int32_t c, int32_t k0) {
+  return ((unsigned long long)(uint32_t)c << 32) | (uint32_t)k0;
+}
+
 template <int PV>
-__global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const int32_t* __restrict__ dplus,
+__global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const int32_t* __restrict__ ind,
+                                                    const int32_t* __restrict__ degv,
+                                                    const int32_t* __restrict__ dplus,
                                                     const int64_t* __restrict__ offp,
                                                     const int32_t* __restrict__ indp,
-                                                    const int32_t* __restrict__ large,
-                                                    const int32_t* __restrict__ medium,
+                                                    const unsigned long long* __restrict__ large,
+                                                    const unsigned long long* __restrict__ medium,
                                                     uint32_t* __restrict__ out, DevStatus* __restrict__ st,
                                                     const SchedParams sp) {
   TC_DBG_ENTER(6);
@@ -374,24 +358,29 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
   const int lane = threadIdx.x & (kWarp - 1);
   const int wid = threadIdx.x / kWarp;
   uint32_t tri = 0;
-  unsigned long long work = 0;
   const unsigned n_large = st->n_large;
   const unsigned n_medium = st->n_medium;
 
-  // Tier L: one CTA per vertex, in chunks of kChunk staged entries.
+  // CTA tier: one CTA per item (centre with a > warp_max, kCtaRange of its neighbours), over
+  // chunks of kChunk staged entries of N+(c).
   BlockTable& L = sm.t.L;
   while (true) {
-    if (threadIdx.x == 0) sm.item = atomicAdd(&st->q_large, 1u);
+    if (threadIdx.x == 0) {
+      const unsigned q = atomicAdd(&st->q_large, 1u);
+      sm.item = q < n_large ? large[q] : ~0ull;
+    }
     __syncwarp();
     __syncthreads();
-    const unsigned item = sm.item;
+    const unsigned long long item = sm.item;
     __syncthreads();
-    if (item >= n_large) break;
-    const int32_t u = large[item];
-    if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (1ull << 60) | ((unsigned long long)item << 32) | (unsigned)u);
-    const int32_t a = dplus[u];
-    const int32_t* Ag = indp + offp[u];
-    uint32_t u_acc = 0;
+    if (item == ~0ull) break;
+    const int32_t c = (int32_t)(item >> 32);
+    const int32_t k0 = (int32_t)(uint32_t)item;
+    const int32_t a = dplus[c];
+    const int64_t start = offp[c];
+    const int32_t k1 = min(degv[c], k0 + kCtaRange);
+    const int32_t* Ag = indp + start;
+    uint32_t c_acc = 0;
     for (int cb = 0; cb < a; cb += kChunk) {
       const int clen = min(kChunk, a - cb);
       int bits = 4;  // buckets: 4 * 2^bits slots >= 2 clen, load <= 0.5
@@ -408,51 +397,57 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
       for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, L.hidx, bits, L.sA[j], j);
       __syncwarp();
       __syncthreads();
-      const int ngroups = (a + kWarp - 1) / kWarp;
+      const int ngroups = (k1 - k0 + kWarp - 1) / kWarp;
       while (true) {
         int g = 0;
         if (lane == 0) g = atomicAdd(&sm.gctr, 1);
         __syncwarp();
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
-        process_group<PV>(u, Ag, L.sA, cb, clen, L.hkeys, L.hidx, bits, L.cnt, g * kWarp, min(kWarp, a - g * kWarp),
-                          dplus, offp, indp, out, sp, tri, u_acc, work);
+        const int gk = k0 + g * kWarp;
+        process_group<PV>(n, c, a, ind + start + gk, min(kWarp, k1 - gk), L.hkeys, L.hidx, bits, L.cnt, dplus,
+                          offp, indp, out, sp, tri, c_acc);
       }
       __syncwarp();
       __syncthreads();
       if (PV != TC_PV_NONE) {
         for (int j = threadIdx.x; j < clen; j += kThreads) {
-          const uint32_t c = L.cnt[j];
-          if (c) atomicAdd(&out[L.sA[j]], c * flush_mult<PV>());
+          const uint32_t x = L.cnt[j];
+          if (x) atomicAdd(&out[L.sA[j]], x * flush_mult<PV>());
         }
       }
       __syncwarp();
       __syncthreads();
     }
     if (PV != TC_PV_NONE) {
-      u_acc = warp_sum(u_acc);
-      if (lane == 0 && u_acc) atomicAdd(&out[u], u_acc * flush_mult<PV>());
+      c_acc = warp_sum(c_acc);
+      if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
     }
   }
 
   // From here every warp works alone, on its own slice of the (now free) staging area.
   WarpTable& W = sm.t.W[wid];
 
-  // Tier M: one warp per vertex with 32 < d+ <= warp_max, from the medium queue.
+  // Warp tier, centres with many neighbours: one warp per item (kWarpRange neighbours).
   while (true) {
-    unsigned idx = 0;
-    if (lane == 0) idx = atomicAdd(&st->q_medium, 1u);
+    unsigned long long item = ~0ull;
+    if (lane == 0) {
+      const unsigned q = atomicAdd(&st->q_medium, 1u);
+      if (q < n_medium) item = medium[q];
+    }
     __syncwarp();
-    idx = __shfl_sync(kFull, idx, 0);
-    if (idx >= n_medium) break;
-    const int32_t u = medium[idx];
-    const int a = __ldg(dplus + u);
-    if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (3ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
-    warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri, work);
+    item = __shfl_sync(kFull, item, 0);
+    if (item == ~0ull) break;
+    const int32_t c = (int32_t)(item >> 32);
+    const int32_t k0 = (int32_t)(uint32_t)item;
+    const int a = __ldg(dplus + c);
+    const int64_t start = __ldg(offp + c);
+    const int k1 = min(__ldg(degv + c), k0 + kWarpRange);
+    warp_centre<PV>(n, c, a, start, k0, k1, W, ind, dplus, offp, indp, out, sp, tri);
   }
 
-  // Tier S: vertices with 2 <= d+ <= 32 (and <= warp_max), one warp each, claimed in chunks.
-  const int smax = min(kSmallMax, sp.warp_max);
+  // Warp tier, the rest (1 <= a <= warp_max, degree <= kWarpRange): one warp per centre,
+  // claimed in chunks of vertex ids.
   while (true) {
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(&st->q_small, (unsigned long long)sp.chunk);
@@ -462,37 +457,31 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
     const int32_t cend = (int32_t)min((unsigned long long)n, c0 + (unsigned long long)sp.chunk);
     for (int32_t ub = (int32_t)c0; ub < cend; ub += kWarp) {
       const int32_t uu = ub + lane;
-      const int aa = (uu < cend) ? __ldg(dplus + uu) : 0;
-      unsigned elig = __ballot_sync(kFull, aa >= 2 && aa <= smax && (uu % sp.nshards) == sp.shard);
+      const bool in = uu < cend;
+      const int aa = in ? __ldg(dplus + uu) : 0;
+      const int dd = in ? __ldg(degv + uu) : 0;
+      unsigned elig =
+          __ballot_sync(kFull, aa >= 1 && aa <= sp.warp_max && dd <= kWarpRange && (uu % sp.nshards) == sp.shard);
       while (elig) {
         const int sl = __ffs(elig) - 1;
         elig &= elig - 1;
-        const int32_t u = ub + sl;
+        const int32_t c = ub + sl;
         const int a = __shfl_sync(kFull, aa, sl);
-        if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4, (2ull << 60) | ((unsigned long long)a << 32) | (unsigned)u);
-        warp_vertex<PV>(u, a, W, dplus, offp, indp, out, sp, tri, work);
+        const int d = __shfl_sync(kFull, dd, sl);
+        warp_centre<PV>(n, c, a, __ldg(offp + c), 0, d, W, ind, dplus, offp, indp, out, sp, tri);
       }
     }
   }
 
-  if (lane == 0) TC_DBG_MARK((blockIdx.x * kWarps + wid) * 4 + 3, 1ull);
   // One global atomic per CTA for the triangle total.
   __syncwarp();
   const unsigned long long t = warp_sum((unsigned long long)tri);
-  work = warp_sum(work);
-  if (lane == 0) {
-    sm.tri[wid] = t;
-    sm.work[wid] = work;
-  }
+  if (lane == 0) sm.tri[wid] = t;
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long s = 0, wk = 0;
-    for (int w = 0; w < kWarps; ++w) {
-      s += sm.tri[w];
-      wk += sm.work[w];
-    }
+    unsigned long long s = 0;
+    for (int w = 0; w < kWarps; ++w) s += sm.tri[w];
     if (s) atomicAdd(&st->triangles, s);
-    if (wk) atomicAdd(&st->oriented_work, wk);
   }
   TC_DBG_EXIT(6);
 }
@@ -543,52 +532,52 @@ __device__ __forceinline__ int orient_range(const View& g, const int32_t n, cons
   return cnt;
 }
 
-// Per-warp buffer of vertex ids bound for one of the tier queues, flushed 32 at a time.
-struct TierBuf {
-  int32_t val = 0;
-  int n = 0;
-  __device__ __forceinline__ void push(int32_t u, int32_t* __restrict__ q, unsigned* head) {
-    const int lane = threadIdx.x & (kWarp - 1);
-    if (lane == n) val = u;
-    if (++n == kWarp) flush(q, head);
+// Append the work items (u, k0) for k0 = 0, range, 2 range, ... < d to a queue (warp-wide,
+// warp-uniform arguments). Only centres with many neighbours or a large out-degree are queued;
+// they are few, so one atomic per vertex is cheap.
+__device__ __forceinline__ void push_items(const int32_t u, const int32_t d, const int range,
+                                           unsigned long long* __restrict__ q, unsigned* head, const int64_t cap,
+                                           unsigned& bad) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int nit = (d + range - 1) / range;
+  unsigned at = 0;
+  if (lane == 0) at = atomicAdd(head, (unsigned)nit);
+  __syncwarp();
+  at = __shfl_sync(kFull, at, 0);
+  if ((int64_t)at + nit > cap) {
+    bad |= kBadCapacity;
+    return;
   }
-  __device__ __forceinline__ void flush(int32_t* __restrict__ q, unsigned* head) {
-    const int lane = threadIdx.x & (kWarp - 1);
-    if (n == 0) return;
-    unsigned at = 0;
-    if (lane == 0) at = atomicAdd(head, (unsigned)n);
-    __syncwarp();
-    at = __shfl_sync(kFull, at, 0);
-    if (lane < n) q[at + lane] = val;
-    n = 0;
-  }
-};
+  for (int j = lane; j < nit; j += kWarp) q[at + j] = make_item(u, j * range);
+}
 
-// Orientation bookkeeping of a finished vertex u with out-degree a (warp-uniform call): its
-// offset and out-degree, the work figures and its tier queue.
+// Orientation bookkeeping of a finished vertex u with degree d and out-degree a (warp-uniform
+// call): its offset, degree and out-degree, the work figures and its count work items.
 struct OrientAcc {
   unsigned long long work = 0, ei = 0;
   unsigned mx = 0;
-  TierBuf large, medium;
 };
 
 __device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, const int64_t s, const int32_t a,
                                               int32_t* __restrict__ dplus, int64_t* __restrict__ offp,
-                                              int32_t* __restrict__ large, int32_t* __restrict__ medium,
+                                              int32_t* __restrict__ degv, unsigned long long* __restrict__ large,
+                                              unsigned long long* __restrict__ medium, const int64_t item_cap,
                                               DevStatus* __restrict__ st, const int warp_max, const int shard,
-                                              const int nshards, OrientAcc& acc) {
+                                              const int nshards, OrientAcc& acc, unsigned& bad) {
   const int lane = threadIdx.x & (kWarp - 1);
   const bool mine = (u % nshards) == shard;
   if (lane == 0) {
     dplus[u] = a;
     offp[u] = s;
+    degv[u] = d;
     if (d >= 2) acc.ei += (unsigned long long)a;
-    if (a >= 2 && mine) acc.work += (unsigned long long)a * (unsigned long long)a;
+    // sum over u -> v of d+(u) + d+(v) = sum over v of d+(v) deg(v)
+    if (mine) acc.work += (unsigned long long)a * (unsigned long long)d;
     acc.mx = max(acc.mx, (unsigned)a);
   }
-  if (mine) {
-    if (a > warp_max) acc.large.push(u, large, &st->n_large);
-    else if (a > kSmallMax) acc.medium.push(u, medium, &st->n_medium);
+  if (mine && a > 0) {
+    if (a > warp_max) push_items(u, d, kCtaRange, large, &st->n_large, item_cap, bad);
+    else if (d > kWarpRange) push_items(u, d, kWarpRange, medium, &st->n_medium, item_cap, bad);
   }
 }
 
@@ -597,7 +586,8 @@ __device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, 
 // so a hub that is never completed (capacity error) leaves nothing for the count to read.
 template <class View>
 __global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n, int32_t* __restrict__ dplus,
-                                                   int64_t* __restrict__ offp, int32_t* __restrict__ hub_u,
+                                                   int64_t* __restrict__ offp, int32_t* __restrict__ degv,
+                                                   int32_t* __restrict__ hub_u,
                                                    int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_done,
                                                    int32_t* __restrict__ chunk_hub, const int64_t hub_cap,
                                                    const int64_t chunk_cap, DevStatus* __restrict__ st) {
@@ -607,6 +597,7 @@ __global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n
     if (d <= kHubChunk) continue;
     dplus[u] = 0;
     offp[u] = 0;
+    degv[u] = 0;
     const int nch = (d + kHubChunk - 1) / kHubChunk;
     const unsigned h = atomicAdd(&st->n_hubs, 1u);
     const unsigned base = atomicAdd(&st->n_hub_chunks, (unsigned)nch);
@@ -629,9 +620,11 @@ __global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n
 // chunk (a counter per hub) moves the pieces together and completes the vertex.
 template <class View, bool kWrite>
 __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, int32_t* __restrict__ dplus,
-                                                int64_t* __restrict__ offp, int32_t* __restrict__ indp,
-                                                const int64_t e_cap, int32_t* __restrict__ large,
-                                                int32_t* __restrict__ medium, const int32_t* __restrict__ hub_u,
+                                                int64_t* __restrict__ offp, int32_t* __restrict__ degv,
+                                                int32_t* __restrict__ indp, const int64_t e_cap,
+                                                unsigned long long* __restrict__ large,
+                                                unsigned long long* __restrict__ medium, const int64_t item_cap,
+                                                const int32_t* __restrict__ hub_u,
                                                 const int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_cnt,
                                                 int32_t* __restrict__ hub_done, const int32_t* __restrict__ chunk_hub,
                                                 const int64_t hub_cap, const int64_t chunk_cap, DevStatus* __restrict__ st,
@@ -692,7 +685,7 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
       }
       a += cn;
     }
-    finish_vertex(u, d, s, a, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
+    finish_vertex(u, d, s, a, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc, bad);
   }
 
   // Vertex tiles (hubs skipped: done above).
@@ -714,16 +707,15 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
       if (d > kHubChunk) continue;
       if (s < 0 || s + d > e_cap) {
         bad |= kBadCapacity;
-        finish_vertex(u, 0, 0, 0, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
+        finish_vertex(u, 0, 0, 0, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc,
+                      bad);
         continue;
       }
       const int a = d > 0 ? orient_range<View, kWrite>(g, n, u, d, s, 0, d, indp, s, chk, bad) : 0;
-      finish_vertex(u, d, s, a, dplus, offp, large, medium, st, warp_max, shard, nshards, acc);
+      finish_vertex(u, d, s, a, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc, bad);
     }
   }
 
-  acc.large.flush(large, &st->n_large);
-  acc.medium.flush(medium, &st->n_medium);
   __syncwarp();
   chk = warp_sum(chk);
 #pragma unroll
@@ -848,7 +840,7 @@ int hubs_grid(int64_t n) {
 }
 
 template <int PV>
-tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const SchedParams& sp,
+tc_status launch_count(int32_t n, const int32_t* ind, const Workspace& ws, uint32_t* out, const SchedParams& sp,
                        cudaStream_t stream) {
   constexpr int kMaxDev = 64;
   static int blocks_per_sm[kMaxDev] = {};  // 0 = not configured on that device yet
@@ -867,7 +859,8 @@ tc_status launch_count(int32_t n, const Workspace& ws, uint32_t* out, const Sche
 #ifdef TC_DEBUG_PROGRESS
   if (tc_dbg_progress_host_dev) cudaMemsetAsync(tc_dbg_progress_host_dev, 0, tc_dbg_progress_bytes, stream);
 #endif
-  k_count<PV><<<grid, kThreads, smem, stream>>>(n, ws.dplus, ws.offp, ws.indp, ws.large, ws.medium, out, ws.st, sp);
+  k_count<PV><<<grid, kThreads, smem, stream>>>(n, ind, ws.degv, ws.dplus, ws.offp, ws.indp, ws.large, ws.medium, out,
+                                                ws.st, sp);
   TC_CUDA_TRY(cudaGetLastError());
   return TC_OK;
 }
@@ -891,21 +884,22 @@ tc_status resident_grid(int threads, int* grid) {
 
 template <class View>
 tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& sp, bool write, cudaStream_t stream) {
-  k_find_hubs<View><<<hubs_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.hub_u, ws.hub_base, ws.hub_done,
-                                                      ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st);
+  k_find_hubs<View><<<hubs_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.hub_u, ws.hub_base,
+                                                      ws.hub_done, ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st);
   TC_CUDA_TRY(cudaGetLastError());
   int grid = 0;
   if (write) TC_TRY((resident_grid<k_orient<View, true>>(256, &grid)));
   else TC_TRY((resident_grid<k_orient<View, false>>(256, &grid)));
   if (write)
-    k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large, ws.medium,
-                                                   ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
-                                                   ws.hub_cap, ws.chunk_cap, ws.st, sp.warp_max, sp.shard, sp.nshards);
+    k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap, ws.large,
+                                                   ws.medium, ws.item_cap, ws.hub_u, ws.hub_base, ws.hub_cnt,
+                                                   ws.hub_done, ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st,
+                                                   sp.warp_max, sp.shard, sp.nshards);
   else
-    k_orient<View, false><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.indp, ws.e_cap, ws.large,
-                                                    ws.medium, ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done,
-                                                    ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st, sp.warp_max,
-                                                    sp.shard, sp.nshards);
+    k_orient<View, false><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap,
+                                                    ws.large, ws.medium, ws.item_cap, ws.hub_u, ws.hub_base,
+                                                    ws.hub_cnt, ws.hub_done, ws.chunk_hub, ws.hub_cap, ws.chunk_cap,
+                                                    ws.st, sp.warp_max, sp.shard, sp.nshards);
   TC_CUDA_TRY(cudaGetLastError());
   return TC_OK;
 }
@@ -958,9 +952,9 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
     prof_mark(1, stream);
     uint32_t* out = reinterpret_cast<uint32_t*>(per_vertex);
     switch (pv_mode) {
-      case TC_PV_NONE: TC_TRY(launch_count<TC_PV_NONE>(n, ws, out, sp, stream)); break;
-      case TC_PV_HANDLE: TC_TRY(launch_count<TC_PV_HANDLE>(n, ws, out, sp, stream)); break;
-      case TC_PV_CSR: TC_TRY(launch_count<TC_PV_CSR>(n, ws, out, sp, stream)); break;
+      case TC_PV_NONE: TC_TRY(launch_count<TC_PV_NONE>(n, view.ind, ws, out, sp, stream)); break;
+      case TC_PV_HANDLE: TC_TRY(launch_count<TC_PV_HANDLE>(n, view.ind, ws, out, sp, stream)); break;
+      case TC_PV_CSR: TC_TRY(launch_count<TC_PV_CSR>(n, view.ind, ws, out, sp, stream)); break;
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);

@@ -247,7 +247,6 @@ void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind,
   int64_t tri = 0;
 #pragma omp parallel for num_threads(nt) schedule(dynamic, 64) reduction(+ : tri)
   for (int32_t u = 0; u < nv; ++u) {
-    if (nshards > 1 && u % nshards != shard) continue;
     const int32_t* a = pind + poff[u];
     int64_t al = poff[u + 1] - poff[u];
     uint32_t tu = 0;
@@ -255,6 +254,12 @@ void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind,
       int32_t v = a[i];
       const int32_t* bb = pind + poff[v];
       int64_t bl = poff[v + 1] - poff[v];
+      if (nshards > 1) {
+        /* A shard owns the edges whose centre (the endpoint with the larger out-degree, ties to
+         * the smaller id: the GPU count's hash side) is one of its vertices. */
+        const int32_t centre = (bl < al || (bl == al && u < v)) ? u : v;
+        if (centre % nshards != shard) continue;
+      }
       int64_t x = 0, y = 0;
       uint32_t c = 0;
       while (x < al && y < bl) {

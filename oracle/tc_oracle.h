@@ -72,9 +72,10 @@ void oracle_sort_batch(int32_t nv, const int64_t* off, const int32_t* ind, int64
 void oracle_fast_count(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads,
                        int64_t* total, int32_t* per_vertex);
 
-/* The same restricted to the triangles whose lowest vertex u (in the degree order) has
- * u % nshards == shard: the work split of the multi-GPU count. Summing the shards' totals and
- * per-vertex arrays gives the full count. */
+/* The same restricted to the triangles x < y < z (degree order) whose edge {x, y} has its
+ * centre c with c % nshards == shard, the centre being the endpoint with the larger
+ * out-degree (ties: the smaller id): the work split of the multi-GPU count. Summing the shards'
+ * totals and per-vertex arrays gives the full count. */
 void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
                              int32_t nshards, int64_t* total, int32_t* per_vertex);
 

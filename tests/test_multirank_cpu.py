@@ -1,6 +1,6 @@
-"""Multi-rank work split on CPU: two gloo ranks count their vertex shards (the split the GPU
-kernel uses, u % nshards over the lowest vertex of each triangle) and all-reduce; the sum must
-equal the single-rank count bit for bit."""
+"""Multi-rank work split on CPU: two gloo ranks count their shards (the split the GPU kernel
+uses: c % nshards over the centre c of the edge each triangle is found on) and all-reduce; the
+sum must equal the single-rank count bit for bit."""
 import os
 import socket
 
