@@ -89,14 +89,15 @@ struct DevStatus {
 // ---- scheduler parameters as the kernels see them --------------------------------------
 
 struct SchedParams {
-  int32_t warp_max;        // <= 32
+  int32_t warp_max;        // <= kWarpTierMax
   int32_t search_ratio_x16;
   int32_t use_table;
   int32_t chunk;
   int32_t blocks_per_sm;   // 0 = occupancy limit
-  int32_t shard;           // count source vertices u with u % nshards == shard
+  int32_t shard;           // count the edges whose centre c has c % nshards == shard
   int32_t nshards;
   int32_t cell_filter;     // -1 all edges, -2 none, >= 0 only that degree cell
+  int32_t lane_max;        // static: lists of at most this many entries are walked by one lane
   uint8_t table[16][16];
 };
 

@@ -292,22 +292,25 @@ tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_fe
   cudaFree(dx);
   cudaFree(dy);
   if (rc != TC_OK) return rc;
-  // Strategy ids: 0 = hash probe, 1 = binary search, 2 = merge; static chooses {0, 1},
-  // streaming {1, 2}. Table entry 1 selects the second of the pair. The outputs are predicted
-  // log2 costs per edge. A cell departs from the fixed threshold rule (the caller's
-  // search_ratio_x16 applied to the cell's mean degrees) only when the network predicts the
-  // other strategy at least kMargin cheaper; otherwise the rule's choice stays (the fallback).
+  // Output ids: static count 0 = the warp streams the list through the hash set, 1 = one lane
+  // walks it; streaming 1 = binary search, 2 = merge. Table entry 1 selects the second of the
+  // pair. The outputs are predicted log2 costs per edge. A cell departs from the fixed rule
+  // (static: lane_max_deg; streaming: search_ratio_x16; applied to the cell's mean degrees) only
+  // when the network predicts the other strategy at least kMargin cheaper; otherwise the rule's
+  // choice stays (the fallback).
   constexpr double kMargin = 0.05;
   const float log_keep = (float)std::log2(1.0 - kMargin);
   const int s0 = kind == 0 ? 0 : 1, s1 = kind == 0 ? 1 : 2;
   const long long ratio = std::max(0, sch->search_ratio_x16);
+  const long long lane_max = std::max(0, sch->lane_max_deg);
   for (int c = 0; c < 256; ++c) {
     const double a = std::max(1.0, std::exp2((double)feat[c * kIn + 0]) - 1.0);
     const double b = std::max(1.0, std::exp2((double)feat[c * kIn + 1]) - 1.0);
     const long long ai = (long long)std::llround(a), bi = (long long)std::llround(b);
     int lg = 0;
     for (long long t = bi; t > 0; t >>= 1) ++lg;
-    const int rule = 16LL * bi > ratio * ai * lg ? 1 : 0;
+    // static: 1 = one lane walks the list (b <= lane_max); streaming: 1 = merge (no search)
+    const int rule = kind == 0 ? (bi <= lane_max ? 1 : 0) : (16LL * bi > ratio * ai * lg ? 0 : 1);
     const float c0 = y[c * kOut + s0], c1 = y[c * kOut + s1];
     const float c_rule = rule ? c1 : c0, c_other = rule ? c0 : c1;
     const int pick = (c_other < c_rule + log_keep) ? 1 - rule : rule;

@@ -209,9 +209,37 @@ __device__ __forceinline__ bool centre_of(int32_t c, int a, int32_t o, int b) {
   return b < a || (b == a && c < o);
 }
 
-// Stream the list lst[0 .. len) through the hash set; returns the hits. Per hit, the third
-// vertex's counter cnt[hidx[slot]] gets its weight; vacc and c_acc collect the weights of the
-// streamed list's owner o and of the centre c (TC_PV_CSR only: in handle mode all are the hits).
+// Probe one entry key of the list owned by o into the hash set; returns 1 on a hit. Per hit, the
+// third vertex's counter cnt[hidx[slot]] gets its weight; vacc and c_acc collect the weights of
+// o and of the centre c (TC_PV_CSR only: in handle mode all weights are 1 and the caller counts
+// the hits instead).
+template <int PV, typename IdxT>
+__device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c, const int32_t o,
+                                              const int32_t* hkeys, const IdxT* hidx, const int bits,
+                                              uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+  // First bucket in one 128-bit load; the common case (a miss in a bucket with a free slot)
+  // ends here without computing a slot.
+  const uint32_t bk = hash_bucket(key, bits);
+  const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
+  const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
+  if (!(hit | (q.w != -1))) return 0;
+  const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
+                    : hash_find_after(hkeys, bits, key, bk);
+  if (s < 0) return 0;
+  if (PV == TC_PV_HANDLE) {
+    atomicAdd(&cnt[hidx[s]], 1u);
+  } else if (PV == TC_PV_CSR) {
+    uint32_t wc, wo, ww;
+    tri_weights<PV>(c, o, key, wc, wo, ww);
+    c_acc += wc;
+    vacc += wo;
+    if (ww) atomicAdd(&cnt[hidx[s]], ww);
+  }
+  return 1;
+}
+
+// The warp streams the list lst[0 .. len) through the hash set with coalesced loads, kUnroll
+// per lane in flight; returns this lane's hits.
 template <int PV, typename IdxT>
 __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
                                                const int32_t o, const int32_t* hkeys, const IdxT* hidx,
@@ -255,12 +283,32 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, 
   return hits;
 }
 
+// One lane walks a whole (short) list lst[0 .. len), kUnroll entries in flight; returns the
+// hits. The lanes of a warp walk different lists at once, so short lists do not leave most of
+// the warp idle.
+template <int PV, typename IdxT>
+__device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
+                                              const int32_t o, const int32_t* hkeys, const IdxT* hidx,
+                                              const int bits, uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+  uint32_t hits = 0;
+  for (int k0 = 0; k0 < len; k0 += kUnroll) {
+    int32_t w[kUnroll];
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j) w[j] = k0 + j < len ? __ldg(lst + k0 + j) : -1;
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j)
+      if (w[j] >= 0) hits += probe_one<PV>(w[j], c, o, hkeys, hidx, bits, cnt, c_acc, vacc);
+  }
+  return hits;
+}
+
 // One warp takes the neighbours o = nbr[0 .. gcount) of centre c (out-degree a) and
-// intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), is
-// streamed through the hash set of the staged chunk of N+(c) (2^bits buckets, hidx[slot] =
-// entry, cnt[entry] its counter) with coalesced loads, kUnroll per lane in flight. The lists are
-// taken one at a time, so o, its list and its count stay warp-uniform; nearly all of the work
-// lies in lists of 32 entries or more.
+// intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), goes
+// through the hash set of the staged chunk of N+(c) (2^bits buckets, hidx[slot] = entry,
+// cnt[entry] its counter). Per edge the scheduler picks how (table cell, else b <= lane_max):
+//   lane: each such lane walks its own list, all at once (short lists);
+//   warp: the lists are taken one at a time and the warp streams each with coalesced loads, so
+//         o, its list and its count stay warp-uniform.
 template <int PV, typename IdxT>
 __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, const int a,
                                               const int32_t* __restrict__ nbr, const int gcount,
@@ -278,7 +326,22 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
                     (sp.cell_filter == -1 ||
                      (sp.cell_filter >= 0 && log2_cell(a) * 16 + log2_cell(b) == sp.cell_filter));
   const int64_t base = mine ? __ldg(offp + o) : 0;
-  unsigned todo = __ballot_sync(kFull, mine);
+  const bool by_lane =
+      mine && (sp.use_table ? sp.table[log2_cell(a)][log2_cell(b)] == 1 : b <= sp.lane_max);
+  if (__any_sync(kFull, by_lane)) {
+    if (by_lane) {
+      uint32_t vacc = 0;
+      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, hidx, bits, cnt, c_acc, vacc);
+      tri += hits;
+      if (PV == TC_PV_HANDLE) {
+        c_acc += hits;
+        vacc = hits;
+      }
+      if (PV != TC_PV_NONE && vacc) atomicAdd(&out[o], vacc * flush_mult<PV>());
+    }
+    __syncwarp();
+  }
+  unsigned todo = __ballot_sync(kFull, mine && !by_lane);
   while (todo) {
     const int sl = __ffs(todo) - 1;
     todo &= todo - 1;
@@ -936,6 +999,7 @@ SchedParams to_params(const tc_sched* s) {
   p.nshards = std::max(1, s->nshards);
   p.shard = std::min(std::max(0, s->shard), p.nshards - 1);
   p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
+  p.lane_max = std::min(64, std::max(0, s->lane_max_deg));
   memcpy(p.table, s->table, sizeof(p.table));
   return p;
 }
@@ -1012,16 +1076,17 @@ __global__ void __launch_bounds__(256) k_cell_stats(const int32_t n, const int32
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t uu = gw; uu < n; uu += nw) {
-    const int32_t a = dplus[uu];
+    const int32_t du = dplus[uu];
     const int64_t s = offp[uu];
-    const double la = log2(1.0 + a);
-    for (int32_t k = lane; k < a; k += 32) {
-      const int32_t b = dplus[indp[s + k]];
+    for (int32_t k = lane; k < du; k += 32) {
+      // the cell the count files the edge under: (centre's out-degree, the other endpoint's)
+      const int32_t dv = dplus[indp[s + k]];
+      const int32_t a = max(du, dv), b = min(du, dv);
       const int c = log2_cell(a) * 16 + log2_cell(b);
       atomicAdd(&acc[4 * c + 0], 1.0);
-      atomicAdd(&acc[4 * c + 1], la);
+      atomicAdd(&acc[4 * c + 1], log2(1.0 + a));
       atomicAdd(&acc[4 * c + 2], log2(1.0 + b));
-      atomicAdd(&acc[4 * c + 3], (double)min(a, b) / (double)max(max(a, b), 1));
+      atomicAdd(&acc[4 * c + 3], (double)b / (double)max(a, 1));
     }
   }
   __syncwarp();

@@ -41,17 +41,17 @@ int ilog2(int64_t x) {
 std::vector<tc_sched> candidates() {
   std::vector<tc_sched> out;
   const int warp_max[] = {64, 128, 256};
-  const int ratio[] = {8, 16, 32, 1 << 30};
+  const int lane_max[] = {0, 4, 8, 16};
   const int chunk[] = {32, 128};
   const int bps[] = {0, 6};
   for (int w : warp_max)
-    for (int r : ratio)
+    for (int r : lane_max)
       for (int c : chunk)
         for (int b : bps) {
           tc_sched s;
           tc_sched_default(&s);
           s.warp_max_deg = w;
-          s.search_ratio_x16 = r;
+          s.lane_max_deg = r;
           s.chunk = c;
           s.blocks_per_sm = b;
           out.push_back(s);
@@ -132,11 +132,11 @@ tc_status tc_autotune_save(const char* path) {
   FILE* f = fopen(path, "w");
   if (!f) return fail(TC_ERR_INVALID_ARG, "cannot write %s", path);
   std::lock_guard<std::mutex> lk(cache().mu);
-  fprintf(f, "# tc autotune v1: log2n log2m log2maxdplus warp_max ratio_x16 chunk blocks_per_sm\n");
+  fprintf(f, "# tc autotune v2: log2n log2m log2maxdplus warp_max lane_max chunk blocks_per_sm\n");
   for (const auto& kv : cache().entries) {
     const tc_sched& s = kv.second;
     fprintf(f, "%d %d %d %d %d %d %d\n", std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
-            s.warp_max_deg, s.search_ratio_x16, s.chunk, s.blocks_per_sm);
+            s.warp_max_deg, s.lane_max_deg, s.chunk, s.blocks_per_sm);
   }
   fclose(f);
   return TC_OK;
@@ -156,7 +156,7 @@ tc_status tc_autotune_load(const char* path) {
       tc_sched s;
       tc_sched_default(&s);
       s.warp_max_deg = w;
-      s.search_ratio_x16 = r;
+      s.lane_max_deg = r;
       s.chunk = ch;
       s.blocks_per_sm = bp;
       cache().entries[Key{a, b, c}] = s;

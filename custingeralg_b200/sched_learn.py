@@ -1,13 +1,15 @@
 """Learned scheduler for the static count: per-degree-cell strategy from a trained MLP.
 
-The count kernel intersects each oriented edge u->v by one of two strategies: hash probe (stream
-N+(v) into the hash set of N+(u)) or binary search (search the entries of N+(u) in N+(v)). The
-fixed heuristic picks by a degree-ratio threshold. Here a 3-layer FP32 MLP of width 64 predicts
-the cost per edge of each strategy from the features of the edge's degree cell
-(log2 d+(u), log2 d+(v) buckets): mean log2(1 + d+(u)), mean log2(1 + d+(v)), mean min/max
-degree ratio and cell id / 255. The cell's choice goes into the scheduler table; the fixed rule
-stays the fallback for cells where the network does not predict a clear gain
-(tc_sched_learned). The network only changes which strategy runs, never what is counted.
+The count kernel intersects each edge at its centre (the endpoint with the larger out-degree
+a): the other endpoint's list N+(o), b <= a entries, goes through the centre's shared-memory
+hash set by one of two strategies: the warp streams it with coalesced loads (one list at a
+time), or one lane walks it (the lanes of a warp walk different short lists at once). The fixed
+heuristic picks by a length threshold (lane_max_deg). Here a 3-layer FP32 MLP of width 64
+predicts the cost per edge of each strategy from the features of the edge's degree cell
+(log2 a, log2 b buckets): mean log2(1 + a), mean log2(1 + b), mean b/a and cell id / 255. The
+cell's choice goes into the scheduler table; the fixed rule stays the fallback for cells where
+the network does not predict a clear gain (tc_sched_learned). The network only changes which
+strategy runs, never what is counted.
 
 Pipeline, all on the GPU through the library's own kernels:
 
@@ -274,23 +276,22 @@ def evaluate_graph(params, spec, reps: int = 5):
     t_fixed, T_fixed = times(None, out_fixed)
     t_learned, T_learned = times(ls, out_learned)
     same = bool(torch.equal(out_fixed, out_learned)) and T_fixed == T_learned
-    t_probe, T_probe = times(forced(0), out_learned)
-    t_search, T_search = times(forced(1), out_learned)
-    same = same and T_probe == T_fixed and T_search == T_fixed
+    t_warp, T_warp = times(forced(0), out_learned)
+    t_lane, T_lane = times(forced(1), out_learned)
+    same = same and T_warp == T_fixed and T_lane == T_fixed
     changed = int(sum(ls.table[i][j] != forced_rule_choice(i, j) for i in range(16) for j in range(16)))
     graph.close()
     return dict(graph=spec_name(spec), n=g.n, m=g.m, triangles=T_fixed, fixed_ms=round(t_fixed, 4),
                 learned_ms=round(t_learned, 4), gain=round(t_fixed / t_learned, 4),
-                always_probe_ms=round(t_probe, 4), always_search_ms=round(t_search, 4), counts_equal=same,
+                always_warp_ms=round(t_warp, 4), always_lane_ms=round(t_lane, 4), counts_equal=same,
                 cells_departing_from_rule=changed)
 
 
-def forced_rule_choice(i: int, j: int, ratio: int = None) -> int:
+def forced_rule_choice(i: int, j: int, lane_max: int = None) -> int:
     """The fixed rule's choice for a cell at its nominal degrees (for reporting only)."""
-    if ratio is None:
-        ratio = N.default_sched().search_ratio_x16
-    a, b = round(1.5 * (1 << i)), round(1.5 * (1 << j))
-    return 1 if 16 * b > ratio * a * b.bit_length() else 0
+    if lane_max is None:
+        lane_max = N.default_sched().lane_max_deg
+    return 1 if round(1.5 * (1 << j)) <= lane_max else 0
 
 
 # ---- driver ---------------------------------------------------------------------------------

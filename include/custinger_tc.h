@@ -58,18 +58,25 @@ enum { TC_MEM_DEVICE = 0, TC_MEM_HOST = 1 };
 /* Scheduler: which intersection strategy each oriented edge uses and the launch shapes.
  * tc_sched_default() fills the fixed degree-threshold heuristic. */
 typedef struct tc_sched {
-  int32_t warp_max_deg;   /* out-degree up to which a vertex is counted by one warp (<= 256) */
-  int32_t search_ratio_x16; /* edge (u,v) uses binary search of N+(u) into N+(v) when
-                               16*d+(v) > search_ratio_x16 * d+(u) * (log2 d+(v) + 1) */
+  int32_t warp_max_deg;   /* static count: a centre (the edge endpoint whose N+ is hashed) with
+                             out-degree up to this is counted by one warp (<= 256), above by a CTA */
+  int32_t search_ratio_x16; /* streaming delta count: edge {x,y} binary-searches the shorter list
+                               into the longer one when 16 d_long > ratio * d_short (log2 d_long + 1),
+                               else merges */
   int32_t blocks_per_sm;  /* persistent grid = SMs x blocks_per_sm (0 = occupancy limit) */
   int32_t chunk;          /* vertices a warp claims per work-queue grab */
-  int32_t use_table;      /* 1 = per-(log d+u, log d+v) strategy table below overrides the ratio */
-  uint8_t table[16][16];  /* strategy per degree-cell: 0 = hash probe, 1 = binary search */
-  int32_t shard;          /* count only triangles whose lowest vertex u has u % nshards == shard */
+  int32_t use_table;      /* 1 = the per-degree-cell strategy table below overrides the rules */
+  uint8_t table[16][16];  /* strategy per cell [log2 d_a][log2 d_b]. Static count (a = the centre's
+                             out-degree, b = the other endpoint's): 0 = the warp streams N+(b)
+                             through the hash set, 1 = one lane walks it. Streaming: 0 = search,
+                             1 = merge */
+  int32_t shard;          /* count only the edges whose centre c has c % nshards == shard */
   int32_t nshards;        /* (multi-GPU work split; 1 = everything) */
   int32_t cell_filter;    /* timing mode for scheduler training: -1 = intersect every edge (normal),
                              -2 = none, c >= 0 = only edges of degree cell c (16*log2 d_a + log2 d_b);
                              counts are partial unless -1 */
+  int32_t lane_max_deg;   /* static count rule without a table: lists of at most this many entries
+                             are walked by one lane each (several lists per warp step) */
 } tc_sched;
 
 typedef struct tc_graph tc_graph;
@@ -199,9 +206,10 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
                          const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
                          const tc_sched* sched, void* stream);
 
-/* Per degree-cell statistics of the oriented edges u->v (cell = 16*min(15, log2 d+u) +
- * min(15, log2 d+v)): out[4*c + 0..3] = edge count, sum of log2(1 + d+u), sum of log2(1 + d+v),
- * sum of min/max of the two. Host array of 1024 doubles. Syncs. */
+/* Per degree-cell statistics of the oriented edges of the last static count, filed as the count
+ * files them: a = the larger out-degree of the two endpoints (the centre's), b = the smaller,
+ * cell = 16*min(15, log2 a) + min(15, log2 b). out[4*c + 0..3] = edge count, sum of
+ * log2(1 + a), sum of log2(1 + b), sum of b/a. Host array of 1024 doubles. Syncs. */
 tc_status tc_cell_stats(tc_graph* g, double* out_host, void* stream);
 
 /* ---- autotuner --------------------------------------------------------------------------- */
@@ -247,12 +255,13 @@ tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strat
 
 /* Fill a scheduler from a trained MLP (device parameters) whose outputs are predicted log2
  * costs per edge of each strategy: for every degree cell, the choice between the two strategies
- * of `kind` (0 = static count: hash probe or search; 1 = streaming delta: search or merge) goes
- * into s->table and s->use_table = 1. The fixed threshold rule (s->search_ratio_x16 on the
- * cell's mean degrees) is the fallback: a cell takes the other strategy only when the network
- * predicts it at least 5% cheaper. cell_features (host, 256 x TC_MLP_IN floats: mean
- * log2(1 + d+(u)), mean log2(1 + d+(v)), mean min/max degree ratio, cell id / 255) describe each
- * cell, e.g. from tc_cell_stats; NULL uses the cells' nominal degrees. */
+ * of `kind` (0 = static count: the warp streams the shorter list or one lane walks it; 1 =
+ * streaming delta: search or merge) goes into s->table and s->use_table = 1. The fixed rule
+ * (static: s->lane_max_deg; streaming: s->search_ratio_x16; on the cell's mean degrees) is the
+ * fallback: a cell takes the other strategy only when the network predicts it at least 5%
+ * cheaper. cell_features (host, 256 x TC_MLP_IN floats: mean log2(1 + a), mean log2(1 + b),
+ * mean b/a, cell id / 255, as tc_cell_stats files the cells) describe each cell; NULL uses the
+ * cells' nominal degrees. */
 tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* s, void* stream);
 
 /* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching

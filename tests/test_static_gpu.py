@@ -24,8 +24,8 @@ def sched(**kw):
 
 SCHEDS = {
     "default": None,
-    "always_search": dict(search_ratio_x16=0),
-    "never_search": dict(search_ratio_x16=1 << 30),
+    "lane_walk_up_to_64": dict(lane_max_deg=64),
+    "never_lane_walk": dict(lane_max_deg=0),
     "warp2": dict(warp_max_deg=2),
     "warp8_chunk32": dict(warp_max_deg=8, chunk=32),
     "one_block_per_sm": dict(blocks_per_sm=1),
