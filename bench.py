@@ -11,8 +11,9 @@ The unit of work is an edge intersected: an undirected edge {u,v} with deg(u), d
 
 Timing: W warm-up steps, then K steps, each bracketed by CUDA events on the launching stream;
 L2 (126 MB) is flushed by writing a 512 MB buffer between steps, outside the events. With N
-GPUs (torchrun), each rank counts the triangles whose lowest vertex falls in its shard of the
-vertex ids, then the per-vertex counts and the total are all-reduced over NCCL inside the timed
+GPUs (torchrun), each rank counts the edges whose centre (the endpoint with the larger
+out-degree) falls in its shard of the vertex ids, then the per-vertex counts and the total are
+all-reduced over NCCL inside the timed
 step; the time is the max over ranks (strong scaling: the graph is fixed).
 
 `--impl reference` times the reference's own CPU counter (hostSingleIntersection from
@@ -56,6 +57,8 @@ def parse():
     ap.add_argument("--stream-scale", type=int, default=22)
     ap.add_argument("--stream-batches", type=int, default=200)
     ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
+    ap.add_argument("--stream-path", choices=["pipeline", "apply"], default="pipeline",
+                    help="captured pipeline (tc_pipeline) or tc_apply_batch per batch")
     return ap.parse_args()
 
 
@@ -416,15 +419,25 @@ def run_streaming(a, dev):
     batches = streaming_batches(a.stream_scale, a.stream_batches, base)
     dbat = [(torch.from_numpy(s).to(dev), torch.from_numpy(d).to(dev), torch.from_numpy(x).to(dev))
             for s, d, x in batches]
+    pipe = None
+    if getattr(a, "stream_path", "pipeline") == "pipeline":
+        pipe = api.Pipeline(graph, max(s.numel() for s, _, _ in dbat))
+        pipe.prepare(per_vertex=pv, delta_dev=delta)  # pool headroom and captures, before timing
+        pipe.autotune(24)   # the first 24 timed batches also try the candidate delta grids
     torch.cuda.synchronize()
     stream = torch.cuda.current_stream()
     total_ms, updates, checked = 0.0, 0, 0
     for i, (s, d, x) in enumerate(dbat):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        graph.apply_batch(s, d, x, per_vertex=pv, delta_dev=delta, sync=False)
+        if pipe is not None:
+            pipe.apply(s, d, x, per_vertex=pv, delta_dev=delta)
+        else:
+            graph.apply_batch(s, d, x, per_vertex=pv, delta_dev=delta, sync=False)
         e1.record(stream)
         e1.synchronize()
+        if pipe is not None:
+            pipe.sync()
         total_ms += e0.elapsed_time(e1)
         updates += s.numel()
         if a.stream_verify and (i % a.stream_verify == 0 or i == len(dbat) - 1):
@@ -435,8 +448,13 @@ def run_streaming(a, dev):
                                                   _static_pv_cache(graph, base, T0, dev)).to(torch.int32)):
                 raise SystemExit(f"per-vertex streaming mismatch after batch {i}")
             checked += 1
+    path = "tc_pipeline (one captured CUDA graph per batch-size bin)" if pipe is not None else "tc_apply_batch"
+    bins = pipe.info() if pipe is not None else None
+    if pipe is not None:
+        pipe.close()
     return {"value": updates / (total_ms / 1e3), "unit": "update edges/s", "batches": len(dbat),
-            "updates": updates, "ms_total": total_ms, "recount_checks": checked,
+            "updates": updates, "ms_total": total_ms, "recount_checks": checked, "path": path,
+            "bins": [{"capacity": c, "delta_ctas_per_sm": b} for c, b in bins] if bins else None,
             "workload": f"R-MAT scale {a.stream_scale} ef 16 seed 4 base (slack 0.25), {len(dbat)} batches of "
                         "log-uniform size in [1, 2^20], 70% R-MAT insertions / 30% deletions of base edges; "
                         "timed per batch over sort + classify + structure update + delta count, batches resident "

@@ -121,6 +121,54 @@ def _apply_batch(self, src, dst, is_delete=None, per_vertex=None, delta_dev=None
 Graph.apply_batch = _apply_batch
 
 
+class Pipeline:
+    """tc_pipeline: streaming batches of device updates through one captured CUDA graph per
+    batch-size bin (same semantics as Graph.apply_batch)."""
+
+    def __init__(self, graph: Graph, max_batch: int, sched=None):
+        self._p = ctypes.c_void_p()
+        N.check(N.lib().tc_pipeline_create(graph._h, max_batch, ctypes.byref(sched) if sched is not None else None,
+                                           ctypes.byref(self._p)))
+        self.graph = graph
+
+    def apply(self, src, dst, is_delete=None, per_vertex=None, delta_dev=None, stream=None):
+        """Enqueue one batch (int32 CUDA tensors src/dst, optional uint8 is_delete)."""
+        b = src.numel()
+        N.check(N.lib().tc_pipeline_apply(self._p, _ptr(src) if b else None, _ptr(dst) if b else None,
+                                          _ptr(is_delete) if (is_delete is not None and b) else None, b,
+                                          _ptr(per_vertex), _ptr(delta_dev), _stream_ptr(stream)))
+
+    def prepare(self, per_vertex=None, delta_dev=None, stream=None):
+        """Reserve pool headroom and capture every bin's graph for these outputs now."""
+        N.check(N.lib().tc_pipeline_prepare(self._p, _ptr(per_vertex), _ptr(delta_dev), _stream_ptr(stream)))
+
+    def sync(self):
+        info = N.BatchInfo()
+        N.check(N.lib().tc_pipeline_sync(self._p, ctypes.byref(info)))
+        return info
+
+    def autotune(self, batches: int):
+        N.check(N.lib().tc_pipeline_autotune(self._p, batches))
+
+    def info(self):
+        nb = ctypes.c_int32(0)
+        caps = (ctypes.c_int64 * 8)()
+        blocks = (ctypes.c_int32 * 8)()
+        N.check(N.lib().tc_pipeline_info(self._p, ctypes.byref(nb), caps, blocks))
+        return [(int(caps[i]), int(blocks[i])) for i in range(nb.value)]
+
+    def close(self):
+        if self._p:
+            N.lib().tc_pipeline_destroy(self._p)
+            self._p = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def count_all_triangles(graph: Graph, out, sched=None, stream=None):
     """callDeviceAllTriangles: out[v] = 2 t(v) for v < nv (device int32 tensor, >= nv entries)."""
     return graph.count(N.TC_PV_HANDLE, out, sched=sched, stream=stream)

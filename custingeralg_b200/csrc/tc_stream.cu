@@ -211,6 +211,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
       __syncwarp();
       if ((int64_t)at + nc > pool_cap) {
         if (lane == 0) atomicOr(&st->err, kErrPool);
+        for (int64_t j = i0 + lane; j < i1; j += 32) slot[j] = -1;  // nothing to clear later
         continue;  // cannot happen when the host sized the pool from the demand pass
       }
       s_new = (int64_t)at;
@@ -272,7 +273,10 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
   }
 }
 
-__global__ void k_clear_slots(const int64_t* __restrict__ slot, const int64_t n, uint8_t* __restrict__ mark) {
+// Clear the marks of the inserted slots: n_host entries, or 2 * (*n_dev) when n_dev is given.
+__global__ void k_clear_slots(const int64_t* __restrict__ slot, const int64_t n_host,
+                              const unsigned long long* __restrict__ n_dev, uint8_t* __restrict__ mark) {
+  const int64_t n = n_dev ? 2 * (int64_t)(*n_dev) : n_host;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t s = slot[i];
     if (s >= 0) mark[s] = 0;
@@ -296,8 +300,10 @@ __global__ void k_mark_deletions(const int4* __restrict__ dlist, const BatchStat
 __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
                                  const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start,
                                  int32_t* __restrict__ used, int32_t* __restrict__ pool, uint8_t* __restrict__ mark,
-                                 unsigned* __restrict__ claim, const unsigned epoch, BatchStatus* __restrict__ st) {
+                                 unsigned* __restrict__ claim, const unsigned* __restrict__ epoch_dev,
+                                 BatchStatus* __restrict__ st) {
   const int lane = threadIdx.x & 31;
+  const unsigned epoch = *epoch_dev;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t cnt = nv_dev ? (int64_t)(*nv_dev) * stride : nv_list;
@@ -552,6 +558,34 @@ __global__ void k_endpoints(const int4* __restrict__ dlist, const BatchStatus* _
   }
 }
 
+// The compaction epoch lives on the device so that a captured launch sequence advances it.
+__global__ void k_bump_epoch(unsigned* __restrict__ epoch) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *epoch += 1u;
+}
+
+// Canonical keys of a padded batch: entries [b, cap) (b read on the device) become sentinels,
+// so a launch sequence sized for cap serves every batch of at most cap updates.
+__global__ void k_make_keys_cap(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                                const uint8_t* __restrict__ is_del, const int64_t* __restrict__ b_dev,
+                                const int64_t cap, const int32_t n, const int L, uint64_t* __restrict__ keys,
+                                BatchStatus* __restrict__ st) {
+  const uint64_t sent = (1ull << (2 * L + 1)) - 1;
+  const int64_t b = min(*b_dev, cap);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t k = sent;
+    if (i < b) {
+      const int32_t s = src[i], d = dst[i];
+      if (s < 0 || s >= n || d < 0 || d >= n) {
+        atomicOr(&st->err, kErrRange);
+      } else if (s != d) {
+        const uint64_t lo = (uint64_t)min(s, d), hi = (uint64_t)max(s, d);
+        k = (lo << (L + 1)) | (hi << 1) | (uint64_t)(is_del[i] ? 0 : 1);
+      }
+    }
+    keys[i] = k;
+  }
+}
+
 __global__ void k_add_delta(int64_t* __restrict__ delta, const unsigned long long* __restrict__ add,
                             const unsigned long long* __restrict__ sub) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *delta += (int64_t)(add ? *add : 0ull) - (int64_t)(sub ? *sub : 0ull);
@@ -583,7 +617,8 @@ struct StreamWs {
   int64_t* ins_slot = nullptr;  // [2b]
   int32_t* vlist = nullptr;     // [2b]
   unsigned* claim = nullptr;    // [n]
-  unsigned epoch = 0;
+  unsigned* d_epoch = nullptr;  // [1] compaction epoch
+  uint64_t version = 0;         // bumped when the batch-sized buffers are reallocated
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
   BatchStatus* st = nullptr;
@@ -598,7 +633,7 @@ struct StreamWs {
 void StreamWs::release() {
   cudaFree(src); cudaFree(dst); cudaFree(isdel); cudaFree(keys); cudaFree(keys2); cudaFree(head);
   cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(ins_slot);
-  cudaFree(vlist); cudaFree(claim); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
+  cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles);
   *this = StreamWs();
 }
@@ -619,14 +654,16 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     TC_CUDA_TRY(cudaMemset(g->mark, 0, (size_t)std::max<int64_t>(g->pool_cap, 1)));
   }
   if (w.n_cap < (int64_t)g->n + 1) {
-    cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles);
+    cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
     TC_CUDA_TRY(cudaMalloc(&w.claim, sizeof(unsigned) * ((size_t)g->n + 1)));
     TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * ((size_t)g->n + 1)));
+    TC_CUDA_TRY(cudaMalloc(&w.d_epoch, sizeof(unsigned)));
+    TC_CUDA_TRY(cudaMemset(w.d_epoch, 0, sizeof(unsigned)));
     TC_CUDA_TRY(cudaMalloc(&w.cnt, sizeof(int32_t) * ((size_t)g->n + 1)));
     TC_CUDA_TRY(cudaMalloc(&w.scan64, sizeof(int64_t) * ((size_t)g->n + 2)));
     TC_CUDA_TRY(cudaMalloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)));
     w.n_cap = g->n + 1;
-    w.epoch = 0;
+    ++w.version;
   }
   if (!w.st) {
     TC_CUDA_TRY(cudaMalloc(&w.st, sizeof(BatchStatus)));
@@ -658,6 +695,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   w.cub_bytes = std::max(t1, t2);
   TC_CUDA_TRY(cudaMalloc(&w.cub_tmp, w.cub_bytes));
   w.b_cap = nb;
+  ++w.version;
   return TC_OK;
 }
 
@@ -780,9 +818,9 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.weight = 2;
     k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
     k_endpoints<<<gd, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
-    ++w.epoch;
+    k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
-        w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.epoch, w.st);
+        w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch, w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
   // 4. insertions: merge into the lists, count on the post-insertion graph, clear marks
@@ -797,7 +835,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.weight = 2;
     k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
     k_clear_slots<<<grid_for(2 * (int64_t)h.n_ins, kThreads), kThreads, 0, s>>>(w.ins_slot, 2 * (int64_t)h.n_ins,
-                                                                                  g->mark);
+                                                                                  nullptr, g->mark);
     TC_CUDA_TRY(cudaGetLastError());
   }
   g->m += 2 * ((int64_t)h.n_ins - (int64_t)h.n_del);
@@ -920,9 +958,9 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   SlackView view{g->start, g->used, g->pool};
   k_mark_dir_deletions<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, g->mark, w.vlist,
                                                                    w.counter);
-  ++w.epoch;
+  k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
   k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
-                                                                   g->pool, g->mark, w.claim, w.epoch, w.st);
+                                                                   g->pool, g->mark, w.claim, w.d_epoch, w.st);
   TC_CUDA_TRY(cudaGetLastError());
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -954,6 +992,374 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
     if (sign > 0) k_add_delta<<<1, 32, 0, s>>>(delta_dev, w.counter, nullptr);
     else k_add_delta<<<1, 32, 0, s>>>(delta_dev, nullptr, w.counter);
     TC_CUDA_TRY(cudaGetLastError());
+  }
+  return TC_OK;
+}
+
+}  // extern "C"
+
+// ---- captured streaming pipeline ---------------------------------------------------------------
+//
+// tc_apply_batch reads the batch's sizes and the pool demand on the host halfway through (one
+// synchronisation) and sizes each launch from them. The pipeline below runs the same steps as
+// one CUDA graph per batch-size bin instead: every launch is sized for the bin's capacity and
+// reads the batch's real counts from device memory (grid-stride loops over device counts, the
+// batch padded with sentinel keys), so a batch is a few copies and one graph launch with no
+// host synchronisation inside. The pool headroom the relocations of one batch can take is
+// bounded ahead (every touched list moving: (m + 2b)(1 + slack) slots) and reserved before the
+// launch, so the device bump allocator cannot run out. The graphs capture the graph's pool and
+// workspace pointers and the caller's per-vertex and delta arrays; they are captured again when
+// any of these change. The autotuner times the candidate grids of the delta kernel per bin on
+// the caller's own batches (tc_pipeline_autotune) and keeps the fastest.
+
+namespace tc {
+namespace {
+constexpr int kPipeBins = 8;
+constexpr int kPipeCands = 4;
+constexpr int kPipeCandBlocks[kPipeCands] = {2, 4, 8, 16};  // delta-kernel CTAs per SM
+constexpr int64_t kPipeMinBin = 1 << 10;
+}  // namespace
+}  // namespace tc
+
+struct tc_pipeline {
+  tc_graph* g = nullptr;
+  int device = -1;
+  int64_t b_max = 0;
+  int nbins = 0;
+  int64_t bin_cap[tc::kPipeBins] = {};
+  int cand[tc::kPipeBins] = {};                      // chosen delta-grid candidate per bin
+  cudaGraphExec_t exec[tc::kPipeBins][tc::kPipeCands] = {};
+  // autotuning: per bin and candidate, accumulated ms per update and samples
+  double tune_ms_per_update[tc::kPipeBins][tc::kPipeCands] = {};
+  int tune_n[tc::kPipeBins][tc::kPipeCands] = {};
+  int tune_left = 0;                                 // batches still spent exploring
+  int tune_reps = 0;
+  // what the captured graphs hold
+  const void* key_pool = nullptr;
+  const void* key_mark = nullptr;
+  const void* key_pv = nullptr;
+  const void* key_delta = nullptr;
+  uint64_t key_ws = 0;
+  int64_t key_pool_cap = 0;
+  tc::SchedParams sp;
+  cudaStream_t cs = nullptr;     // capture stream
+  int64_t* d_b = nullptr;
+  int64_t* h_b = nullptr;        // pinned
+  tc::BatchStatus* h_st = nullptr;          // pinned: status of the last batch
+  unsigned long long* h_top = nullptr;      // pinned: pool bump pointer after it
+  uint32_t* pv_scratch = nullptr;
+  int64_t* delta_scratch = nullptr;
+  cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+  bool pending = false;
+  int pending_bin = -1, pending_cand = -1;
+  int64_t pending_b = 0;
+  bool timing = false;
+  tc_batch_info last{};
+};
+
+namespace tc {
+namespace {
+
+void drop_graphs(tc_pipeline* p) {
+  for (int i = 0; i < kPipeBins; ++i)
+    for (int j = 0; j < kPipeCands; ++j)
+      if (p->exec[i][j]) {
+        cudaGraphExecDestroy(p->exec[i][j]);
+        p->exec[i][j] = nullptr;
+      }
+}
+
+// Fold the finished batch's device status into the host view of the graph.
+tc_status pipe_settle(tc_pipeline* p) {
+  if (!p->pending) return TC_OK;
+  TC_CUDA_TRY(cudaEventSynchronize(p->done));
+  p->pending = false;
+  tc_graph* g = p->g;
+  const BatchStatus& f = *p->h_st;
+  g->pool_top = (int64_t)*p->h_top;
+  g->m += 2 * ((int64_t)f.n_ins - (int64_t)f.n_del);
+  g->view_version++;
+  p->last.updates = p->pending_b;
+  p->last.inserted = (int64_t)f.n_ins;
+  p->last.deleted = (int64_t)f.n_del;
+  p->last.ignored = p->pending_b - (int64_t)f.n_ins - (int64_t)f.n_del;
+  p->last.triangles_added = (int64_t)f.tri_added;
+  p->last.triangles_removed = (int64_t)f.tri_removed;
+  p->last.status = TC_OK;
+  if (p->timing) {
+    float ms = 0.f;
+    TC_CUDA_TRY(cudaEventElapsedTime(&ms, p->t0, p->t1));
+    const int bi = p->pending_bin, cj = p->pending_cand;
+    p->tune_ms_per_update[bi][cj] += (double)ms / (double)std::max<int64_t>(p->pending_b, 1);
+    p->tune_n[bi][cj] += 1;
+    p->timing = false;
+  }
+  if (f.err & kErrRange) {
+    p->last.status = TC_ERR_INVALID_ARG;
+    return fail(TC_ERR_INVALID_ARG, "batch had vertex ids outside [0, %d); they were ignored", g->n);
+  }
+  if (f.err & kErrPool) {
+    p->last.status = TC_ERR_CAPACITY;
+    return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+  }
+  return TC_OK;
+}
+
+int64_t pipe_worst_demand(const tc_graph* g, int64_t b) {
+  const int64_t q = std::max<int64_t>(g->slack_q10, 256);
+  return ((g->m + 2 * b) * (1024 + q) + 1023) / 1024 + 16 * b + 64;
+}
+
+// Drop the captured graphs when what they hold (pool, marks, workspace, outputs) has changed.
+void pipe_check_keys(tc_pipeline* p, const void* pv, const void* delta) {
+  tc_graph* g = p->g;
+  const StreamWs& w = *g->sw;
+  if (p->key_pool != g->pool || p->key_mark != g->mark || p->key_pv != pv || p->key_delta != delta ||
+      p->key_ws != w.version || p->key_pool_cap != g->pool_cap) {
+    drop_graphs(p);
+    p->key_pool = g->pool;
+    p->key_mark = g->mark;
+    p->key_pv = pv;
+    p->key_delta = delta;
+    p->key_ws = w.version;
+    p->key_pool_cap = g->pool_cap;
+  }
+}
+
+// Record the whole batch pipeline for a bin of capacity cap on the capture stream.
+tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t* delta) {
+  tc_graph* g = p->g;
+  StreamWs& w = *g->sw;
+  const int64_t cap = p->bin_cap[bin];
+  cudaStream_t s = p->cs;
+  const int L = bits_for(std::max(g->n, 2));
+  const uint64_t sent = (1ull << (2 * L + 1)) - 1;
+  const SlackView view{g->start, g->used, g->pool};
+  const int gb = grid_for(cap, kThreads);
+  const int g2 = grid_for(2 * cap, kThreads);
+  const int gw = grid_for(2 * cap * 32, kThreads);
+  const int gdelta = device_info().sms * kPipeCandBlocks[cand];
+  cudaGraph_t graph = nullptr;
+  TC_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  do {
+    cudaMemsetAsync(w.st, 0, sizeof(BatchStatus), s);
+    k_make_keys_cap<<<gb, kThreads, 0, s>>>(w.src, w.dst, w.isdel, p->d_b, cap, g->n, L, w.keys, w.st);
+    size_t tb = w.cub_bytes;
+    if ((e = cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb, w.keys, w.keys2, (int)cap, 0, 2 * L + 1, s)) != cudaSuccess)
+      break;
+    k_run_heads<<<gb, kThreads, 0, s>>>(w.keys2, cap, sent, w.head);
+    cudaMemsetAsync(w.dk, 0xff, sizeof(uint64_t) * 2 * cap, s);
+    k_classify<<<gb, kThreads, 0, s>>>(view, w.keys2, cap, L, w.head, w.dlist, w.ilist, w.dk, w.st);
+    size_t tb2 = w.cub_bytes;
+    if ((e = cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * cap), 0, 64, s)) != cudaSuccess)
+      break;
+    k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.st);
+    // deletions: mark, count on the pre-deletion graph, compact
+    k_mark_deletions<<<gb, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
+    DeltaArgs A = delta_args(g, p->sp);
+    A.dlist = w.dlist;
+    A.count_dev = &w.st->n_del;
+    A.sign = -1;
+    A.weight = 2;
+    k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
+    k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
+    k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
+    k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
+                                             w.claim, w.d_epoch, w.st);
+    // insertions: merge, count on the post-insertion graph, clear the marks
+    k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
+                                          g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10, w.st);
+    DeltaArgs B = delta_args(g, p->sp);
+    B.ilist = w.ilist;
+    B.count_dev = &w.st->n_ins;
+    B.sign = 1;
+    B.weight = 2;
+    k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
+    k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);
+    k_add_delta<<<1, 32, 0, s>>>(delta, &w.st->tri_added, &w.st->tri_removed);
+    cudaMemcpyAsync(p->h_st, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(p->h_top, g->d_pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s);
+    e = cudaGetLastError();
+  } while (0);
+  const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&p->exec[bin][cand], graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    p->exec[bin][cand] = nullptr;
+    return fail(TC_ERR_CUDA, "pipeline capture: %s", cudaGetErrorString(e));
+  }
+  return TC_OK;
+}
+
+}  // namespace
+}  // namespace tc
+
+extern "C" {
+
+tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sched, tc_pipeline** out) {
+  if (!g || !out || max_batch < 1) return fail(TC_ERR_INVALID_ARG, "invalid pipeline arguments");
+  if (max_batch > (int64_t)INT32_MAX / 4) return fail(TC_ERR_CAPACITY, "pipeline batch capacity exceeds 2^29");
+  *out = nullptr;
+  tc_pipeline* p = new tc_pipeline();
+  p->g = g;
+  p->sp = to_params(sched);
+  TC_CUDA_TRY(cudaGetDevice(&p->device));
+  for (int64_t c = kPipeMinBin; p->nbins < kPipeBins; c *= 4) {
+    p->bin_cap[p->nbins++] = std::min(c, std::max(max_batch, kPipeMinBin));
+    if (c >= max_batch) break;
+  }
+  p->b_max = p->bin_cap[p->nbins - 1];
+  for (int i = 0; i < kPipeBins; ++i) p->cand[i] = 2;  // 8 CTAs per SM until tuned
+  tc_status rc = TC_OK;
+  do {
+    if ((rc = ensure_stream_ws(g, p->b_max)) != TC_OK) break;
+    if (cudaStreamCreateWithFlags(&p->cs, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&p->d_b, sizeof(int64_t)) != cudaSuccess ||
+        cudaMallocHost(&p->h_b, sizeof(int64_t)) != cudaSuccess ||
+        cudaMallocHost(&p->h_st, sizeof(BatchStatus)) != cudaSuccess ||
+        cudaMallocHost(&p->h_top, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&p->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
+        cudaMalloc(&p->delta_scratch, sizeof(int64_t)) != cudaSuccess ||
+        cudaEventCreate(&p->done) != cudaSuccess || cudaEventCreate(&p->t0) != cudaSuccess ||
+        cudaEventCreate(&p->t1) != cudaSuccess) {
+      rc = fail(TC_ERR_OOM, "pipeline: allocation failed");
+      break;
+    }
+    if (cudaMemset(p->pv_scratch, 0, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
+        cudaMemset(p->delta_scratch, 0, sizeof(int64_t)) != cudaSuccess)
+      rc = fail(TC_ERR_CUDA, "pipeline: set-up failed");
+  } while (0);
+  if (rc != TC_OK) {
+    tc_pipeline_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_destroy(tc_pipeline* p) {
+  if (!p) return TC_OK;
+  if (p->pending) cudaEventSynchronize(p->done);
+  drop_graphs(p);
+  if (p->cs) cudaStreamDestroy(p->cs);
+  cudaFree(p->d_b);
+  cudaFreeHost(p->h_b);
+  cudaFreeHost(p->h_st);
+  cudaFreeHost(p->h_top);
+  cudaFree(p->pv_scratch);
+  cudaFree(p->delta_scratch);
+  if (p->done) cudaEventDestroy(p->done);
+  if (p->t0) cudaEventDestroy(p->t0);
+  if (p->t1) cudaEventDestroy(p->t1);
+  delete p;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t* d_dst, const uint8_t* d_is_delete,
+                            int64_t b, int32_t* per_vertex, int64_t* delta_dev, void* stream) {
+  if (!p || b < 0 || (b > 0 && (!d_src || !d_dst))) return fail(TC_ERR_INVALID_ARG, "invalid batch arguments");
+  if (b > p->b_max)
+    return fail(TC_ERR_CAPACITY, "batch of %lld updates exceeds the pipeline's %lld", (long long)b,
+                (long long)p->b_max);
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev != p->device) return fail(TC_ERR_INVALID_ARG, "pipeline used on device %d, created on %d", dev, p->device);
+  TC_TRY(pipe_settle(p));
+  tc_graph* g = p->g;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (b == 0) return TC_OK;
+  // Headroom for the worst case: every list the batch touches moves to the pool top.
+  const int64_t worst = pipe_worst_demand(g, b);
+  if (g->pool_cap - g->pool_top < worst) TC_TRY(ensure_pool(g, worst + worst / 2, s));
+  TC_TRY(ensure_stream_ws(g, p->b_max));
+  uint32_t* pv = per_vertex ? reinterpret_cast<uint32_t*>(per_vertex) : p->pv_scratch;
+  int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
+  StreamWs& w = *g->sw;
+  pipe_check_keys(p, pv, delta);
+  int bin = 0;
+  while (p->bin_cap[bin] < b) ++bin;
+  int cand = p->cand[bin];
+  if (p->tune_left > 0) {
+    // explore: the candidate with the fewest samples in this bin
+    cand = 0;
+    for (int j = 1; j < kPipeCands; ++j)
+      if (p->tune_n[bin][j] < p->tune_n[bin][cand]) cand = j;
+  }
+  if (!p->exec[bin][cand]) TC_TRY(pipe_capture(p, bin, cand, pv, delta));
+  // the batch into the capacity-sized buffers the graph reads
+  TC_CUDA_TRY(cudaMemcpyAsync(w.src, d_src, sizeof(int32_t) * b, cudaMemcpyDeviceToDevice, s));
+  TC_CUDA_TRY(cudaMemcpyAsync(w.dst, d_dst, sizeof(int32_t) * b, cudaMemcpyDeviceToDevice, s));
+  if (d_is_delete) TC_CUDA_TRY(cudaMemcpyAsync(w.isdel, d_is_delete, b, cudaMemcpyDeviceToDevice, s));
+  else TC_CUDA_TRY(cudaMemsetAsync(w.isdel, 0, b, s));
+  *p->h_b = b;
+  TC_CUDA_TRY(cudaMemcpyAsync(p->d_b, p->h_b, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  p->timing = p->tune_left > 0;
+  if (p->timing) TC_CUDA_TRY(cudaEventRecord(p->t0, s));
+  TC_CUDA_TRY(cudaGraphLaunch(p->exec[bin][cand], s));
+  if (p->timing) TC_CUDA_TRY(cudaEventRecord(p->t1, s));
+  TC_CUDA_TRY(cudaEventRecord(p->done, s));
+  p->pending = true;
+  p->pending_bin = bin;
+  p->pending_cand = cand;
+  p->pending_b = b;
+  if (p->tune_left > 0 && --p->tune_left == 0) {
+    // exploration over: settle the last sample, keep the fastest candidate per bin
+    TC_TRY(pipe_settle(p));
+    for (int i = 0; i < p->nbins; ++i) {
+      int best = p->cand[i];
+      double best_v = 0.0;
+      for (int j = 0; j < kPipeCands; ++j) {
+        if (p->tune_n[i][j] < 1) continue;
+        const double v = p->tune_ms_per_update[i][j] / p->tune_n[i][j];
+        if (best_v == 0.0 || v < best_v) {
+          best_v = v;
+          best = j;
+        }
+      }
+      p->cand[i] = best;
+    }
+  }
+  return TC_OK;
+}
+
+tc_status tc_pipeline_prepare(tc_pipeline* p, int32_t* per_vertex, int64_t* delta_dev, void* stream) {
+  if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
+  TC_TRY(pipe_settle(p));
+  tc_graph* g = p->g;
+  const int64_t worst = pipe_worst_demand(g, p->b_max);
+  if (g->pool_cap - g->pool_top < worst) TC_TRY(ensure_pool(g, 2 * worst, (cudaStream_t)stream));
+  TC_TRY(ensure_stream_ws(g, p->b_max));
+  uint32_t* pv = per_vertex ? reinterpret_cast<uint32_t*>(per_vertex) : p->pv_scratch;
+  int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
+  pipe_check_keys(p, pv, delta);
+  for (int i = 0; i < p->nbins; ++i)
+    if (!p->exec[i][p->cand[i]]) TC_TRY(pipe_capture(p, i, p->cand[i], pv, delta));
+  return TC_OK;
+}
+
+tc_status tc_pipeline_sync(tc_pipeline* p, tc_batch_info* last) {
+  if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
+  TC_TRY(pipe_settle(p));
+  if (last) *last = p->last;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_autotune(tc_pipeline* p, int32_t batches) {
+  if (!p || batches < 0) return fail(TC_ERR_INVALID_ARG, "invalid autotune arguments");
+  memset(p->tune_ms_per_update, 0, sizeof(p->tune_ms_per_update));
+  memset(p->tune_n, 0, sizeof(p->tune_n));
+  p->tune_left = batches;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_info(const tc_pipeline* p, int32_t* nbins, int64_t* bin_cap, int32_t* delta_blocks_per_sm) {
+  if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
+  if (nbins) *nbins = p->nbins;
+  for (int i = 0; i < p->nbins; ++i) {
+    if (bin_cap) bin_cap[i] = p->bin_cap[i];
+    if (delta_blocks_per_sm) delta_blocks_per_sm[i] = kPipeCandBlocks[p->cand[i]];
   }
   return TC_OK;
 }

@@ -107,6 +107,13 @@ SIGNATURES = {
     "tc_mlp_backward": (ctypes.c_int, [_P, _P, _P, _P, _i32, _P, _P, _P]),
     "tc_mlp_adam_step": (ctypes.c_int, [_P, _P, _P, _P, _i32, ctypes.c_float, _P]),
     "tc_mlp_train": (ctypes.c_int, [_P, _P, _P, _P, _i32, _i32, ctypes.c_float, _P, _P]),
+    "tc_pipeline_create": (ctypes.c_int, [_P, _i64, ctypes.POINTER(Sched), ctypes.POINTER(_P)]),
+    "tc_pipeline_apply": (ctypes.c_int, [_P, _P, _P, _P, _i64, _P, _P, _P]),
+    "tc_pipeline_prepare": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tc_pipeline_sync": (ctypes.c_int, [_P, ctypes.POINTER(BatchInfo)]),
+    "tc_pipeline_autotune": (ctypes.c_int, [_P, _i32]),
+    "tc_pipeline_info": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tc_pipeline_destroy": (ctypes.c_int, [_P]),
     "tc_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "tc_profile_last": (ctypes.c_int, [ctypes.POINTER(PhaseTimes)]),
 }

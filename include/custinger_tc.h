@@ -206,6 +206,38 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
                          const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
                          const tc_sched* sched, void* stream);
 
+/* ---- captured streaming pipeline (no counterpart in the reference: its driver launches the
+ * three streaming kernels one by one per batch, cct_upd.cu:412-440) ------------------------------
+ *
+ * The same semantics as tc_apply_batch for device batches, as one CUDA graph launch per batch
+ * with no host synchronisation inside it. Batches are binned by size (capacities 2^10, 2^12, ...
+ * up to max_batch); each bin's graph is captured on first use with launches sized for the bin
+ * and reads the batch's counts on the device. Pool headroom for the worst case of a batch (every
+ * list it touches relocating) is reserved before each launch.
+ *
+ * tc_pipeline_create: for batches of at most max_batch updates on graph g (the graph must not be
+ *                     updated through other calls while the pipeline has a batch in flight).
+ * tc_pipeline_apply:  enqueue one batch (device arrays; d_is_delete may be NULL = insertions) on
+ *                     `stream`. per_vertex (+= 2 per vertex per triangle created, -= 2 per one
+ *                     destroyed; NULL = internal scratch) and delta_dev (+= created - destroyed;
+ *                     NULL allowed) are updated when the graph runs. Returns after the launch; the
+ *                     previous batch is settled first (its status folded into the graph).
+ * tc_pipeline_prepare: reserve pool headroom for max_batch and capture every bin's graph for these
+ *                     outputs now (optional; otherwise both happen on first use).
+ * tc_pipeline_sync:   wait for the last batch and report it (errors of that batch surface here).
+ * tc_pipeline_autotune: time the next `batches` batches under the candidate grids of the delta
+ *                     kernel per bin (2, 4, 8, 16 CTAs per SM) and keep the fastest per bin.
+ * tc_pipeline_info:   bins, their capacities and the delta-kernel CTAs per SM each uses. */
+typedef struct tc_pipeline tc_pipeline;
+tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sched, tc_pipeline** out);
+tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t* d_dst, const uint8_t* d_is_delete,
+                            int64_t b, int32_t* per_vertex, int64_t* delta_dev, void* stream);
+tc_status tc_pipeline_prepare(tc_pipeline* p, int32_t* per_vertex, int64_t* delta_dev, void* stream);
+tc_status tc_pipeline_sync(tc_pipeline* p, tc_batch_info* last);
+tc_status tc_pipeline_autotune(tc_pipeline* p, int32_t batches);
+tc_status tc_pipeline_info(const tc_pipeline* p, int32_t* nbins, int64_t* bin_cap, int32_t* delta_blocks_per_sm);
+tc_status tc_pipeline_destroy(tc_pipeline* p);
+
 /* Per degree-cell statistics of the oriented edges of the last static count, filed as the count
  * files them: a = the larger out-degree of the two endpoints (the centre's), b = the smaller,
  * cell = 16*min(15, log2 a) + min(15, log2 b). out[4*c + 0..3] = edge count, sum of

@@ -1,0 +1,108 @@
+"""Captured streaming pipeline (tc_pipeline_*): the same results as tc_apply_batch, batch by batch.
+
+Every batch goes through the pipeline on one graph and through tc_apply_batch on a twin graph;
+after each batch the running totals, the per-vertex deltas and a full static recount must agree,
+bit for bit. Batch sizes span several bins (1 .. 20000 updates), so several captured graphs run.
+"""
+import numpy as np
+import pytest
+
+from custingeralg_b200 import api, generators as G, native as N
+from tests.test_stream_gpu import random_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _recount(graph, n):
+    torch = _torch()
+    out = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    T, _ = graph.count(N.TC_PV_HANDLE, out)
+    return T, out[:n].clone()
+
+
+def _dev(torch, s, d, x):
+    return (torch.from_numpy(np.ascontiguousarray(s)).cuda(), torch.from_numpy(np.ascontiguousarray(d)).cuda(),
+            torch.from_numpy(np.ascontiguousarray(x)).cuda())
+
+
+@pytest.mark.parametrize("slack", [0.0, 0.25])
+def test_pipeline_matches_apply_batch(slack):
+    torch = _torch()
+    rng = np.random.default_rng(7)
+    base = G.rmat(13, 16, seed=11)
+    g_pipe = api.Graph.from_csr(base, slack=slack)
+    g_ref = api.Graph.from_csr(base, slack=slack)
+    n = base.n
+    T0, pv0 = _recount(g_pipe, n)
+    pipe = api.Pipeline(g_pipe, 1 << 15)
+    pv_p = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    pv_r = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    dp = torch.zeros(1, dtype=torch.int64, device="cuda")
+    dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cur = base
+    for k in [1, 3, 37, 600, 5000, 20000, 2, 1500, 9000, 64]:
+        s, d, x = random_batch(rng, cur, k)
+        ts, td, tx = _dev(torch, s, d, x)
+        pipe.apply(ts, td, tx, per_vertex=pv_p, delta_dev=dp)
+        info = pipe.sync()
+        ref = g_ref.apply_batch(ts, td, tx, per_vertex=pv_r, delta_dev=dr)
+        assert (info.inserted, info.deleted, info.triangles_added, info.triangles_removed) == \
+            (ref.inserted, ref.deleted, ref.triangles_added, ref.triangles_removed)
+        assert int(dp.item()) == int(dr.item())
+        assert torch.equal(pv_p, pv_r)
+        T, pv = _recount(g_pipe, n)
+        assert T == T0 + int(dp.item())
+        assert torch.equal(pv, (pv0.to(torch.int64) + pv_p[:n].to(torch.int64)).to(torch.int32))
+        off, ind = g_pipe.export()
+        cur = G.Csr(n, off, ind)
+    pipe.close()
+
+
+def test_pipeline_autotune_keeps_counts_and_picks_a_grid():
+    torch = _torch()
+    rng = np.random.default_rng(3)
+    base = G.rmat(12, 16, seed=5)
+    graph = api.Graph.from_csr(base, slack=0.25)
+    n = base.n
+    T0, _ = _recount(graph, n)
+    pipe = api.Pipeline(graph, 1 << 12)
+    pipe.autotune(12)
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for i in range(16):
+        s, d, x = random_batch(rng, base, int(rng.integers(1, 4000)))
+        pipe.apply(*_dev(torch, s, d, x), delta_dev=delta)
+    pipe.sync()
+    T, _ = _recount(graph, n)
+    assert T == T0 + int(delta.item())
+    bins = pipe.info()
+    assert [c for c, _ in bins] == [1 << 10, 1 << 12]
+    assert all(b in (2, 4, 8, 16) for _, b in bins)
+    pipe.close()
+
+
+def test_pipeline_rejects_oversize_batch_and_recaptures_on_new_outputs():
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    base = G.rmat(11, 8, seed=2)
+    graph = api.Graph.from_csr(base)
+    n = base.n
+    T0, _ = _recount(graph, n)
+    pipe = api.Pipeline(graph, 1000)   # one bin of 1024
+    s, d, x = random_batch(rng, base, 1500)
+    with pytest.raises(N.TcError):
+        pipe.apply(*_dev(torch, s, d, x))
+    total = 0
+    for i in range(3):
+        delta = torch.zeros(1, dtype=torch.int64, device="cuda")   # a new output array each time
+        s, d, x = random_batch(rng, base, 500)
+        pipe.apply(*_dev(torch, s, d, x), delta_dev=delta)
+        pipe.sync()
+        total += int(delta.item())
+    T, _ = _recount(graph, n)
+    assert T == T0 + total
+    pipe.close()
