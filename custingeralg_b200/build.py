@@ -2,7 +2,8 @@
 
   custingeralg_b200/libcustinger_tc.so  CUDA kernels + C ABI + cuStinger-compatible C++ layer,
                                          nvcc -gencode arch=compute_100a,code=sm_100a
-  custingeralg_b200/libtcgen.so          seeded graph generators (host C++/OpenMP)
+  custingeralg_b200/libtcgen.so          seeded graph generators, graph file readers and the binary
+                                         CSR cache (host C++/OpenMP)
 
 Usage: python -m custingeralg_b200.build [--force] [--verbose]
 """
@@ -71,10 +72,10 @@ def build_tc(force=False, verbose=False, extra=()):
 
 
 def build_gen(force=False, verbose=False):
-    src = os.path.join(CSRC, "tcgen.cpp")
-    hdr = os.path.join(INCLUDE, "tc_gen.h")
-    if force or _newer(LIB_GEN, [src, hdr]):
-        _run(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall", src, "-o", LIB_GEN], verbose)
+    srcs = [os.path.join(CSRC, "tcgen.cpp"), os.path.join(CSRC, "tcgen_io.cpp")]
+    hdrs = [os.path.join(INCLUDE, "tc_gen.h"), os.path.join(INCLUDE, "cuStingerDefs.hpp")]
+    if force or _newer(LIB_GEN, srcs + hdrs):
+        _run(["g++", "-O3", "-std=c++17", "-fopenmp", "-fPIC", "-shared", "-Wall"] + srcs + ["-o", LIB_GEN], verbose)
     return LIB_GEN
 
 

@@ -39,6 +39,10 @@ def _load():
         lib.tcgen_from_pairs.argtypes = [i32, i64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, p]
         lib.tcgen_rmat_pairs.argtypes = [ctypes.c_int, i64, dbl, dbl, dbl, u64, ctypes.c_int, u64,
                                          ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.tcgen_read.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, p]
+        lib.tcgen_write_binary.argtypes = [ctypes.c_char_p, p]
+        lib.tcgen_read.restype = ctypes.c_int
+        lib.tcgen_write_binary.restype = ctypes.c_int
         lib.tcgen_free.argtypes = [p]
         for f in ("tcgen_rmat", "tcgen_er", "tcgen_ba", "tcgen_grid", "tcgen_from_pairs", "tcgen_rmat_pairs"):
             getattr(lib, f).restype = ctypes.c_int
@@ -138,3 +142,34 @@ def complete(n: int) -> Csr:
 def star(n: int) -> Csr:
     """One centre joined to n-1 leaves (no triangles)."""
     return from_pairs(n, np.zeros(n - 1, np.int32), np.arange(1, n, dtype=np.int32), name=f"star{n}")
+
+
+FMT_AUTO, FMT_DIMACS, FMT_SNAP, FMT_MTX, FMT_BINARY = 0, 1, 2, 3, 4
+ERR_IO, ERR_FORMAT = 3, 4
+
+
+class ReadError(RuntimeError):
+    def __init__(self, code: int, path: str):
+        super().__init__(f"{path}: cannot read graph (tcgen error {code})")
+        self.code = code
+
+
+def read_graph(path: str, fmt: int = FMT_AUTO, nthreads: int = 0) -> Csr:
+    """Read a DIMACS (.graph), SNAP (.txt), MatrixMarket (.mtx) or binary cache (.tccsr) file into
+    the symmetric, sorted, deduplicated CSR without self-loops (tcgen_read)."""
+    g = _Csr()
+    rc = _load().tcgen_read(os.fsencode(path), fmt, nthreads, ctypes.byref(g))
+    if rc != 0:
+        raise ReadError(rc, path)
+    return _take(rc, g, os.path.basename(path))
+
+
+def write_binary(g: Csr, path: str) -> None:
+    """Write g as the binary CSR cache that read_graph(path) reads back unchanged."""
+    off = np.ascontiguousarray(g.off, dtype=np.int64)
+    ind = np.ascontiguousarray(g.ind, dtype=np.int32)
+    c = _Csr(g.n, g.m, off.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+             ind.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    rc = _load().tcgen_write_binary(os.fsencode(path), ctypes.byref(c))
+    if rc != 0:
+        raise ReadError(rc, path)

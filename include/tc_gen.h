@@ -14,7 +14,8 @@
 extern "C" {
 #endif
 
-enum { TCGEN_OK = 0, TCGEN_ERR_ARG = 1, TCGEN_ERR_OOM = 2 };
+enum { TCGEN_OK = 0, TCGEN_ERR_ARG = 1, TCGEN_ERR_OOM = 2, TCGEN_ERR_IO = 3, TCGEN_ERR_FORMAT = 4 };
+enum { TCGEN_FMT_AUTO = 0, TCGEN_FMT_DIMACS = 1, TCGEN_FMT_SNAP = 2, TCGEN_FMT_MTX = 3, TCGEN_FMT_BINARY = 4 };
 
 typedef struct tcgen_csr {
   int32_t n;    /* vertices */
@@ -45,6 +46,19 @@ int tcgen_grid(int32_t side, double rewire, uint64_t seed, int nthreads, tcgen_c
 /* Symmetric sorted deduplicated CSR from k undirected pairs (self-loops dropped). */
 int tcgen_from_pairs(int32_t n, int64_t k, const int32_t* src, const int32_t* dst, int nthreads,
                      tcgen_csr* out);
+
+/* Read a graph file into the symmetric sorted deduplicated CSR (self-loops dropped; every input
+ * edge contributes both directions). Replaces the absent cuStinger core's readers that the
+ * reference drivers call (tests/cct.cpp:239-257):
+ *   TCGEN_FMT_DIMACS  METIS / DIMACS-10 adjacency (.graph; weights skipped as its fmt says)
+ *   TCGEN_FMT_SNAP    edge list "u v", '#' comments, 0-based ids (.txt)
+ *   TCGEN_FMT_MTX     MatrixMarket coordinate, 1-based (.mtx)
+ *   TCGEN_FMT_BINARY  the cache tcgen_write_binary writes (.tccsr), read back as is
+ *   TCGEN_FMT_AUTO    by the file name, as the reference driver chooses. */
+int tcgen_read(const char* path, int format, int nthreads, tcgen_csr* out);
+
+/* Write g as a binary CSR cache ("TCCSRv1\0", int64 n, int64 m, int64 off[n+1], int32 ind[m]). */
+int tcgen_write_binary(const char* path, const tcgen_csr* g);
 
 void tcgen_free(tcgen_csr* g);
 
