@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
     ap.add_argument("--stream-path", choices=["pipeline", "apply"], default="pipeline",
                     help="captured pipeline (tc_pipeline) or tc_apply_batch per batch")
+    ap.add_argument("--stream-sched", choices=["learned", "fixed"], default="learned",
+                    help="delta-kernel strategy table: trained network or the fixed ratio rule")
     return ap.parse_args()
 
 
@@ -420,8 +422,14 @@ def run_streaming(a, dev):
     dbat = [(torch.from_numpy(s).to(dev), torch.from_numpy(d).to(dev), torch.from_numpy(x).to(dev))
             for s, d, x in batches]
     pipe = None
+    sched, sched_desc = None, "fixed rule (search_ratio_x16 = 16)"
+    if getattr(a, "stream_sched", "learned") == "learned":
+        from custingeralg_b200 import sched_learn as L
+        if os.path.exists(L.STREAM_WEIGHTS):
+            sched = L.learned_stream_sched(L.load(L.STREAM_WEIGHTS))
+            sched_desc = "learned (custingeralg_b200/data/sched_mlp_stream.bin, nominal cell degrees)"
     if getattr(a, "stream_path", "pipeline") == "pipeline":
-        pipe = api.Pipeline(graph, max(s.numel() for s, _, _ in dbat))
+        pipe = api.Pipeline(graph, max(s.numel() for s, _, _ in dbat), sched=sched)
         pipe.prepare(per_vertex=pv, delta_dev=delta)  # pool headroom and captures, before timing
         pipe.autotune(24)   # the first 24 timed batches also try the candidate delta grids
     torch.cuda.synchronize()
@@ -433,7 +441,7 @@ def run_streaming(a, dev):
         if pipe is not None:
             pipe.apply(s, d, x, per_vertex=pv, delta_dev=delta)
         else:
-            graph.apply_batch(s, d, x, per_vertex=pv, delta_dev=delta, sync=False)
+            graph.apply_batch(s, d, x, per_vertex=pv, delta_dev=delta, sched=sched, sync=False)
         e1.record(stream)
         e1.synchronize()
         if pipe is not None:
@@ -454,6 +462,7 @@ def run_streaming(a, dev):
         pipe.close()
     return {"value": updates / (total_ms / 1e3), "unit": "update edges/s", "batches": len(dbat),
             "updates": updates, "ms_total": total_ms, "recount_checks": checked, "path": path,
+            "scheduler": sched_desc,
             "bins": [{"capacity": c, "delta_ctas_per_sm": b} for c, b in bins] if bins else None,
             "workload": f"R-MAT scale {a.stream_scale} ef 16 seed 4 base (slack 0.25), {len(dbat)} batches of "
                         "log-uniform size in [1, 2^20], 70% R-MAT insertions / 30% deletions of base edges; "

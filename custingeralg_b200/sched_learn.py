@@ -43,6 +43,7 @@ from . import api, generators as G, native as N
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 WEIGHTS = os.path.join(HERE, "data", "sched_mlp.bin")
+STREAM_WEIGHTS = os.path.join(HERE, "data", "sched_mlp_stream.bin")
 MIN_CELL_EDGES = 4000   # cells with fewer edges are not timed (their labels would be noise)
 MIN_CELL_MS = 0.002     # a cell whose time above the empty launch is below this gets no label
 
@@ -294,11 +295,161 @@ def forced_rule_choice(i: int, j: int, lane_max: int = None) -> int:
     return 1 if round(1.5 * (1 << j)) <= lane_max else 0
 
 
+
+# ---- streaming delta count ------------------------------------------------------------------
+#
+# The delta kernel intersects the full lists N(x), N(y) of each changed edge {x, y} by binary
+# search of the shorter list in the longer (network output 1, table entry 0) or by a partitioned
+# merge (output 2, table entry 1); the fixed rule searches when
+# 16 d_long > search_ratio_x16 * d_short (log2 d_long + 1). Cells are (log2 d_short, log2 d_long)
+# of the endpoints' degrees. The timings come from tc_count_batch (the cuStinger-path count of a
+# sorted batch) over a sample of the graph's own edges, which leaves the graph unchanged.
+
+def stream_sample(g, k: int, rng):
+    """A sorted symmetric batch of k existing undirected edges (device arrays for tc_count_batch)
+    and its per-cell statistics [256, 4]."""
+    import torch
+    src_of = np.repeat(np.arange(g.n, dtype=np.int32), np.diff(g.off))
+    und = np.nonzero(src_of < g.ind)[0]
+    pick = und[rng.choice(und.size, size=min(k, und.size), replace=False)]
+    u, v = src_of[pick], g.ind[pick]
+    deg = np.diff(g.off)
+    la = np.minimum(deg[u], deg[v]).astype(np.float64)
+    lb = np.maximum(deg[u], deg[v]).astype(np.float64)
+    cell = (np.minimum(np.floor(np.log2(np.maximum(la, 1))), 15) * 16 +
+            np.minimum(np.floor(np.log2(np.maximum(lb, 1))), 15)).astype(np.int64)
+    stats = np.zeros((256, 4))
+    np.add.at(stats[:, 0], cell, 1.0)
+    np.add.at(stats[:, 1], cell, np.log2(1 + la))
+    np.add.at(stats[:, 2], cell, np.log2(1 + lb))
+    np.add.at(stats[:, 3], cell, la / np.maximum(lb, 1))
+    s = np.concatenate([u, v]).astype(np.int32)
+    d = np.concatenate([v, u]).astype(np.int32)
+    ds, dd = torch.from_numpy(s).cuda(), torch.from_numpy(d).cuda()
+    off = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    dup = torch.zeros(max(s.size, 1), dtype=torch.int32, device="cuda")
+    N.check(N.lib().tc_batch_sort(g.n, ds.data_ptr(), dd.data_ptr(), s.size, off.data_ptr(), dup.data_ptr(), None))
+    return (ds, dd, off, dup, s.size), stats
+
+
+def count_batch_ms(graph, batch, sched, reps: int, pv) -> tuple[float, int]:
+    """Best event-timed tc_count_batch (sign +1) over reps after a warm-up, and its count."""
+    import torch
+    ds, dd, off, dup, b = batch
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    best = float("inf")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.current_stream()
+    for r in range(reps + 1):
+        delta.zero_()
+        e0.record(stream)
+        N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
+                                       b, 1, pv.data_ptr(), delta.data_ptr(),
+                                       ctypes.byref(sched) if sched is not None else None, stream.cuda_stream))
+        e1.record(stream)
+        e1.synchronize()
+        if r:
+            best = min(best, e0.elapsed_time(e1))
+    return best, int(delta.item())
+
+
+def stream_forced(table_entry: int, cell_filter: int = -1):
+    return forced(table_entry, cell_filter)
+
+
+def collect_stream_graph(spec, k: int = 200000, reps: int = 5, seed: int = 0):
+    import torch
+    g = make_graph(spec)
+    graph = api.Graph.from_csr(g)
+    pv = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    batch, stats = stream_sample(g, k, np.random.default_rng(seed))
+    feat = cell_features(stats)
+    t_none, _ = count_batch_ms(graph, batch, stream_forced(0, -2), reps, pv)
+    rows = []
+    for c in range(256):
+        cnt = stats[c, 0]
+        if cnt < MIN_CELL_EDGES / 2:
+            continue
+        ts = [count_batch_ms(graph, batch, stream_forced(e, c), reps, pv)[0] - t_none for e in (0, 1)]
+        if min(ts) < MIN_CELL_MS:
+            continue
+        for e in (0, 1):  # table entry 0 = search = network output 1, entry 1 = merge = output 2
+            rows.append((feat[c], e + 1, math.log2(ts[e] * 1e6 / cnt), c, cnt))
+    graph.close()
+    return rows, dict(n=g.n, m=g.m, t_none_ms=t_none)
+
+
+def learned_stream_sched(params: np.ndarray, feat=None, base=None):
+    """Streaming scheduler from the trained network (nominal cell degrees when feat is None)."""
+    import torch
+    s = base if base is not None else N.default_sched()
+    d_params = torch.from_numpy(np.ascontiguousarray(params, dtype=np.float32)).cuda()
+    N.check(N.lib().tc_sched_learned(d_params.data_ptr(), 1, feat.ctypes.data if feat is not None else None,
+                                     ctypes.byref(s), torch.cuda.current_stream().cuda_stream))
+    return s
+
+
+def evaluate_stream_graph(params, spec, k: int = 400000, reps: int = 5):
+    """Fixed rule vs learned table for the delta count of a batch of k of the graph's edges."""
+    import torch
+    g = make_graph(spec)
+    graph = api.Graph.from_csr(g)
+    pv = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
+    batch, stats = stream_sample(g, k, np.random.default_rng(99))
+    ls = learned_stream_sched(params, cell_features(stats))
+    t_fixed, c_fixed = count_batch_ms(graph, batch, None, reps, pv)
+    t_learned, c_learned = count_batch_ms(graph, batch, ls, reps, pv)
+    t_search, c_search = count_batch_ms(graph, batch, stream_forced(0), reps, pv)
+    t_merge, c_merge = count_batch_ms(graph, batch, stream_forced(1), reps, pv)
+    graph.close()
+    return dict(graph=spec_name(spec), n=g.n, m=g.m, batch_edges=int(batch[4] // 2), fixed_ms=round(t_fixed, 4),
+                learned_ms=round(t_learned, 4), gain=round(t_fixed / t_learned, 4),
+                always_search_ms=round(t_search, 4), always_merge_ms=round(t_merge, 4),
+                counts_equal=len({c_fixed, c_learned, c_search, c_merge}) == 1)
+
+
+STREAM_HELD_OUT = [("rmat", dict(scale=22, a=0.57, seed=4)), ("ba", dict(n_log=21, m0=16, seed=21)),
+                   ("er", dict(n_log=20, deg=32, seed=20))]
+
+
+def stream_main(a, report):
+    specs = [sp for i, sp in enumerate(training_specs(a.quick)) if i % 2 == 0]  # 32 graphs
+    ds_path = os.path.join(a.out_dir, "sched_stream_dataset.npz")
+    w_path = os.path.join(a.out_dir, "sched_mlp_stream.bin")
+    X, S, Y, meta = [], [], [], []
+    for i, spec in enumerate(specs):
+        t0 = time.time()
+        rows, info = collect_stream_graph(spec, reps=a.reps, seed=i)
+        for f, st, y, c, cnt in rows:
+            X.append(f)
+            S.append(st)
+            Y.append(y)
+            meta.append((i, c, cnt))
+        print(f"[stream collect] {i + 1}/{len(specs)} {spec_name(spec)} rows={len(rows)} {time.time() - t0:.1f}s",
+              flush=True)
+    X = np.asarray(X, np.float32).reshape(-1, 4)
+    S = np.asarray(S, np.int32)
+    Y = np.asarray(Y, np.float32)
+    meta = np.asarray(meta, np.float64).reshape(-1, 3)
+    np.savez(ds_path, X=X, S=S, Y=Y, meta=meta)
+    val = (meta[:, 0].astype(int) % 8) == 7
+    params, loss = train(X[~val], S[~val], Y[~val], epochs=a.epochs)
+    save(params, w_path)
+    report["stream_train"] = dict(graphs=len(specs), rows=int((~val).sum()), val_rows=int(val.sum()),
+                                  train_mse=round(loss, 4),
+                                  val_mse=round(mse(params, X[val], S[val], Y[val]), 4) if val.any() else None)
+    print(json.dumps(report["stream_train"]), flush=True)
+    report["stream_held_out"] = []
+    for spec in STREAM_HELD_OUT[:1] if a.quick else STREAM_HELD_OUT:
+        r = evaluate_stream_graph(params, spec)
+        report["stream_held_out"].append(r)
+        print(json.dumps(r), flush=True)
+
 # ---- driver ---------------------------------------------------------------------------------
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("cmd", choices=["collect", "train", "evaluate", "all"])
+    ap.add_argument("cmd", choices=["collect", "train", "evaluate", "all", "stream"])
     ap.add_argument("--out-dir", default=".")
     ap.add_argument("--quick", action="store_true", help="12 small training graphs (smoke run)")
     ap.add_argument("--reps", type=int, default=5)
@@ -309,6 +460,11 @@ def main(argv=None):
     ds_path = os.path.join(a.out_dir, "sched_dataset.npz")
     w_path = os.path.join(a.out_dir, "sched_mlp.bin")
     report = {}
+    if a.cmd == "stream":
+        stream_main(a, report)
+        with open(os.path.join(a.out_dir, "sched_stream_report.json"), "w") as f:
+            json.dump(report, f, indent=1)
+        return
     if a.cmd in ("collect", "all"):
         specs = training_specs(a.quick)
         X, S, Y, meta = collect(specs, a.reps)

@@ -89,3 +89,44 @@ def test_learned_table_is_exact_and_reports_gain(spec):
     assert r["triangles"] == O.fast_count(g.n, g.off, g.ind, per_vertex=False)[0] // 6
     # the fallback keeps the learned table from losing much where it departs from the rule
     assert r["learned_ms"] <= 1.15 * r["fixed_ms"] + 0.05
+
+
+needs_stream_weights = pytest.mark.skipif(not os.path.exists(L.STREAM_WEIGHTS),
+                                          reason="no trained streaming weights committed")
+
+
+@needs_stream_weights
+def test_learned_stream_table_is_exact_and_reports_gain():
+    params = L.load(L.STREAM_WEIGHTS)
+    r = L.evaluate_stream_graph(params, ("ba", dict(n_log=16, m0=16, seed=1601)), k=50000, reps=3)
+    print(json.dumps(r))
+    assert r["counts_equal"]
+
+
+def test_untrained_stream_network_keeps_the_pipeline_exact():
+    """A streaming table from an untrained network still gives the oracle's running count."""
+    torch = _torch()
+    params = np.zeros(N.MLP_PARAMS, dtype=np.float32)
+    N.check(N.lib().tc_mlp_init(params.ctypes.data, 321))
+    s = L.learned_stream_sched(params)
+    assert s.use_table == 1
+    rng = np.random.default_rng(8)
+    base = G.rmat(12, 16, seed=12)
+    graph = api.Graph.from_csr(base, slack=0.25)
+    pipe = api.Pipeline(graph, 1 << 12, sched=s)
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    src_of = np.repeat(np.arange(base.n, dtype=np.int32), np.diff(base.off))
+    for k in (300, 3000):
+        u = rng.integers(0, base.n, k).astype(np.int32)
+        v = rng.integers(0, base.n, k).astype(np.int32)
+        x = np.zeros(k, np.uint8)
+        idx = rng.integers(0, base.m, k // 3)
+        u[: k // 3], v[: k // 3], x[: k // 3] = src_of[idx], base.ind[idx], 1
+        pipe.apply(torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda(), torch.from_numpy(x).cuda(),
+                   delta_dev=delta)
+        pipe.sync()
+    pipe.close()
+    off, ind = graph.export()
+    tot, _ = O.fast_count(base.n, off, ind, per_vertex=False)
+    tot0, _ = O.fast_count(base.n, base.off, base.ind, per_vertex=False)
+    assert tot // 6 - tot0 // 6 == int(delta.item())
