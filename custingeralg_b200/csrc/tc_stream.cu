@@ -29,6 +29,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
+constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
 
 enum : unsigned { kErrRange = 1u, kErrPool = 2u };
 
@@ -45,6 +46,7 @@ struct BatchStatus {
   unsigned long long dir_added;   // directed entries inserted (cuStinger path)
   unsigned long long dir_removed; // directed entries deleted (cuStinger path)
   unsigned long long not_fitting;
+  unsigned long long n_long;      // insertion runs whose list is long (CTA kernel)
   unsigned int err;
   unsigned int pad;
 };
@@ -149,9 +151,11 @@ __global__ void k_classify(const SlackView g, const uint64_t* __restrict__ keys,
 
 // Heads of source-vertex runs in the sorted directed entries, and the pool slots the lists that
 // must move could take (computed on the pre-deletion lengths, an upper bound).
+// A run whose list will be long (used + new > kLongList) is stored as -1 - start and also listed
+// in long_runs for the CTA kernel; the warp kernel skips it.
 __global__ void k_dir_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ used,
                            const int32_t* __restrict__ cap, const int32_t slack_q10, int32_t* __restrict__ run_start,
-                           BatchStatus* __restrict__ st) {
+                           int32_t* __restrict__ long_runs, BatchStatus* __restrict__ st) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd_cap; i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = dk[i];
     if (k == kSentinel) continue;
@@ -161,8 +165,13 @@ __global__ void k_dir_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap
     while (j + 1 < nd_cap && dk[j + 1] != kSentinel && (uint32_t)(dk[j + 1] >> 32) == v) ++j;
     const int32_t c = (int32_t)(j - i + 1);
     const unsigned long long r = atomicAdd(&st->n_runs, 1ull);
-    run_start[r] = (int32_t)i;
     const int32_t need = used[v] + c;
+    if (need > kLongList) {
+      run_start[r] = -1 - (int32_t)i;
+      long_runs[atomicAdd(&st->n_long, 1ull)] = (int32_t)i;
+    } else {
+      run_start[r] = (int32_t)i;
+    }
     if (need > cap[v]) atomicAdd(&st->demand, (unsigned long long)slack_capacity(need, max(slack_q10, 256)));
   }
 }
@@ -181,6 +190,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
   const int64_t nruns = (int64_t)st->n_runs;
   for (int64_t r = gw; r < nruns; r += nw) {
     const int64_t i0 = run_start[r];
+    if (i0 < 0) continue;  // a long list: k_insert_long
     const int32_t v = (int32_t)(dk[i0] >> 32);
     int64_t i1 = i0;  // run end (exclusive), found cooperatively
     {
@@ -310,6 +320,7 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
   const unsigned lt = (1u << lane) - 1u;
   for (int64_t k = gw; k < cnt; k += nw) {
     const int32_t v = vlist[k];
+    if (used[v] > kLongList) continue;  // k_compact_long
     unsigned old = 0;
     if (lane == 0) old = atomicMax(&claim[v], epoch);
     __syncwarp();
@@ -338,6 +349,166 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
       used[v] = wp;
       atomicAdd(&st->dir_removed, (unsigned long long)(a - wp));
     }
+  }
+}
+
+
+// One CTA per long insertion run: the same merge as k_insert_runs (new entries' slots first, old
+// entries backwards in chunks, then the new entries into the holes), 256 entries per step. The
+// barrier between reading and writing a chunk keeps the in-place merge safe: targets never
+// precede their sources, so the writes of a chunk land on entries of that chunk (read before the
+// barrier) or of the chunks above it (already moved).
+__global__ void __launch_bounds__(kThreads) k_insert_long(
+    const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ long_runs,
+    int64_t* __restrict__ start, int32_t* __restrict__ used, int32_t* __restrict__ cap, int32_t* __restrict__ pool,
+    const int64_t pool_cap, uint8_t* __restrict__ mark, int64_t* __restrict__ slot,
+    unsigned long long* __restrict__ pool_top, const int32_t slack_q10, BatchStatus* __restrict__ st) {
+  __shared__ int64_t sh_i1, sh_new;
+  __shared__ int32_t sh_nc;
+  __shared__ int sh_state;  // 0 in place, 1 moved, 2 pool exhausted
+  const int64_t nlong = (int64_t)st->n_long;
+  for (int64_t r = blockIdx.x; r < nlong; r += gridDim.x) {
+    const int64_t i0 = long_runs[r];
+    const int32_t v = (int32_t)(dk[i0] >> 32);
+    const int32_t a = used[v];
+    const int64_t s_old = start[v];
+    if (threadIdx.x == 0) {
+      // run end: the first entry at or past i0 whose source is not v (sentinels sort last)
+      const uint64_t lim = ((uint64_t)(uint32_t)v + 1) << 32;
+      int64_t lo = i0, hi = nd_cap;
+      while (lo < hi) {
+        const int64_t mid = lo + ((hi - lo) >> 1);
+        if (dk[mid] < lim) lo = mid + 1;
+        else hi = mid;
+      }
+      sh_i1 = lo;
+      const int32_t c = (int32_t)(lo - i0);
+      sh_state = 0;
+      sh_new = s_old;
+      if (a + c > cap[v]) {
+        const int32_t nc = slack_capacity(a + c, max(slack_q10, 256));
+        const unsigned long long at = atomicAdd(pool_top, (unsigned long long)nc);
+        if ((int64_t)at + nc > pool_cap) {
+          atomicOr(&st->err, kErrPool);
+          sh_state = 2;
+        } else {
+          sh_new = (int64_t)at;
+          sh_nc = nc;
+          sh_state = 1;
+        }
+      }
+    }
+    __syncthreads();
+    const int64_t i1 = sh_i1;
+    const int state = sh_state;
+    const int64_t s_new = sh_new;
+    const int32_t c = (int32_t)(i1 - i0);
+    if (state == 2) {
+      for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) slot[j] = -1;
+      __syncthreads();
+      continue;
+    }
+    const int32_t* A = pool + s_old;
+    for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) {
+      const int32_t val = (int32_t)(uint32_t)dk[j];
+      int32_t lo = 0, hi = a;
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (A[mid] < val) lo = mid + 1;
+        else hi = mid;
+      }
+      slot[j] = (j - i0) + lo;
+    }
+    __syncthreads();
+    for (int32_t base = ((a - 1) / kThreads) * kThreads; base >= 0 && a > 0; base -= kThreads) {
+      const int32_t i = base + (int32_t)threadIdx.x;
+      int32_t val = 0;
+      int64_t pos = 0;
+      if (i < a) {
+        val = A[i];
+        int64_t lo = i0, hi = i1;
+        while (lo < hi) {
+          const int64_t mid = (lo + hi) >> 1;
+          if ((int32_t)(uint32_t)dk[mid] < val) lo = mid + 1;
+          else hi = mid;
+        }
+        pos = i + (lo - i0);
+      }
+      __syncthreads();
+      if (i < a) {
+        pool[s_new + pos] = val;
+        if (mark) mark[s_new + pos] = 0;
+      }
+      __syncthreads();
+    }
+    for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) {
+      const int64_t pos = s_new + slot[j];
+      pool[pos] = (int32_t)(uint32_t)dk[j];
+      if (mark) mark[pos] = 1;
+      slot[j] = pos;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      used[v] = a + c;
+      if (state == 1) {
+        start[v] = s_new;
+        cap[v] = sh_nc;
+        atomicAdd(&st->not_fitting, (unsigned long long)c);
+      }
+      atomicAdd(&st->dir_added, (unsigned long long)c);
+    }
+    __syncthreads();
+  }
+}
+
+// One CTA per long list with deletions: the compaction of k_compact_marked, 256 entries per
+// step with a block-wide prefix of the kept entries (targets never pass their sources).
+__global__ void __launch_bounds__(kThreads) k_compact_long(
+    const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
+    const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start, int32_t* __restrict__ used,
+    int32_t* __restrict__ pool, uint8_t* __restrict__ mark, unsigned* __restrict__ claim,
+    const unsigned* __restrict__ epoch_dev, BatchStatus* __restrict__ st) {
+  __shared__ unsigned sh_old;
+  __shared__ int32_t sh_wsum[kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned epoch = *epoch_dev;
+  const int64_t cnt = nv_dev ? (int64_t)(*nv_dev) * stride : nv_list;
+  for (int64_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+    const int32_t v = vlist[k];
+    const int32_t a = used[v];
+    if (a <= kLongList) continue;  // k_compact_marked's
+    if (threadIdx.x == 0) sh_old = atomicMax(&claim[v], epoch);
+    __syncthreads();
+    const unsigned old = sh_old;
+    __syncthreads();
+    if (old >= epoch) continue;
+    const int64_t s = start[v];
+    int32_t wp = 0;
+    for (int32_t base = 0; base < a; base += kThreads) {
+      const int32_t i = base + (int32_t)threadIdx.x;
+      const bool keep = i < a && mark[s + i] == 0;
+      const int32_t val = keep ? pool[s + i] : 0;
+      const unsigned m = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) sh_wsum[wid] = __popc(m);
+      __syncthreads();
+      int32_t before = 0, total = 0;
+      for (int w = 0; w < kThreads / 32; ++w) {
+        const int32_t x = sh_wsum[w];
+        if (w < wid) before += x;
+        total += x;
+      }
+      const int32_t at = wp + before + __popc(m & ((1u << lane) - 1u));
+      __syncthreads();
+      if (keep) pool[s + at] = val;
+      wp += total;
+      __syncthreads();
+    }
+    for (int32_t i = threadIdx.x; i < a; i += kThreads) mark[s + i] = 0;
+    if (threadIdx.x == 0) {
+      used[v] = wp;
+      atomicAdd(&st->dir_removed, (unsigned long long)(a - wp));
+    }
+    __syncthreads();
   }
 }
 
@@ -614,6 +785,7 @@ struct StreamWs {
   uint64_t* dk = nullptr;       // [2b]
   uint64_t* dk2 = nullptr;      // [2b]
   int32_t* run_start = nullptr; // [2b]
+  int32_t* long_runs = nullptr; // [2b] starts of the runs whose list is long
   int64_t* ins_slot = nullptr;  // [2b]
   int32_t* vlist = nullptr;     // [2b]
   unsigned* claim = nullptr;    // [n]
@@ -632,7 +804,8 @@ struct StreamWs {
 
 void StreamWs::release() {
   cudaFree(src); cudaFree(dst); cudaFree(isdel); cudaFree(keys); cudaFree(keys2); cudaFree(head);
-  cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(ins_slot);
+  cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(long_runs);
+  cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles);
   *this = StreamWs();
@@ -673,7 +846,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   if (b <= w.b_cap) return TC_OK;
   const int64_t nb = std::max<int64_t>(b, 1024);
   cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
-  cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
+  cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start); cudaFree(w.long_runs);
   cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
   w.cub_tmp = nullptr;
   TC_CUDA_TRY(cudaMalloc(&w.src, sizeof(int32_t) * nb));
@@ -687,6 +860,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   TC_CUDA_TRY(cudaMalloc(&w.dk, sizeof(uint64_t) * 2 * nb));
   TC_CUDA_TRY(cudaMalloc(&w.dk2, sizeof(uint64_t) * 2 * nb));
   TC_CUDA_TRY(cudaMalloc(&w.run_start, sizeof(int32_t) * 2 * nb));
+  TC_CUDA_TRY(cudaMalloc(&w.long_runs, sizeof(int32_t) * 2 * nb));
   TC_CUDA_TRY(cudaMalloc(&w.ins_slot, sizeof(int64_t) * 2 * nb));
   TC_CUDA_TRY(cudaMalloc(&w.vlist, sizeof(int32_t) * 2 * nb));
   size_t t1 = 0, t2 = 0;
@@ -740,6 +914,7 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
 }
 
 int delta_grid() { return device_info().sms * 8; }
+int long_grid() { return device_info().sms * 2; }
 
 }  // namespace
 }  // namespace tc
@@ -786,7 +961,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     size_t tb2 = w.cub_bytes;
     TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * b), 0, 64, s));
     k_dir_runs<<<grid_for(2 * b, kThreads), kThreads, 0, s>>>(w.dk2, 2 * b, g->used, g->cap, g->slack_q10, w.run_start,
-                                                               w.st);
+                                                               w.long_runs, w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
   // 2. one synchronisation: sizes and the pool demand
@@ -821,6 +996,8 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
         w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch, w.st);
+    k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used,
+                                                     g->pool, g->mark, w.claim, w.d_epoch, w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
   // 4. insertions: merge into the lists, count on the post-insertion graph, clear marks
@@ -828,6 +1005,9 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, 2 * b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, g->mark, w.ins_slot,
         g->d_pool_top, g->slack_q10, w.st);
+    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, 2 * b, w.long_runs, g->start, g->used, g->cap, g->pool,
+                                                    g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
+                                                    w.st);
     DeltaArgs A = delta_args(g, sp);
     A.ilist = w.ilist;
     A.count_dev = &w.st->n_ins;
@@ -923,7 +1103,7 @@ tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   k_flag_present<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, w.dk);
   size_t tb = w.cub_bytes;
   TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb, w.dk, w.dk2, (int)b, 0, 64, s));
-  k_dir_runs<<<grid_for(b, kThreads), kThreads, 0, s>>>(w.dk2, b, g->used, g->cap, g->slack_q10, w.run_start, w.st);
+  k_dir_runs<<<grid_for(b, kThreads), kThreads, 0, s>>>(w.dk2, b, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.st);
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaMemcpyAsync(&w.st_host->pool_top, g->d_pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -934,6 +1114,9 @@ tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, nullptr, w.ins_slot, g->d_pool_top,
         g->slack_q10, w.st);
+    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, b, w.long_runs, g->start, g->used, g->cap, g->pool,
+                                                    g->pool_cap, nullptr, w.ins_slot, g->d_pool_top, g->slack_q10,
+                                                    w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
@@ -961,6 +1144,8 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
   k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
                                                                    g->pool, g->mark, w.claim, w.d_epoch, w.st);
+  k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used, g->pool, g->mark,
+                                                   w.claim, w.d_epoch, w.st);
   TC_CUDA_TRY(cudaGetLastError());
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1154,7 +1339,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     size_t tb2 = w.cub_bytes;
     if ((e = cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * cap), 0, 64, s)) != cudaSuccess)
       break;
-    k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.st);
+    k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.st);
     // deletions: mark, count on the pre-deletion graph, compact
     k_mark_deletions<<<gb, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
     DeltaArgs A = delta_args(g, p->sp);
@@ -1167,9 +1352,14 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
                                              w.claim, w.d_epoch, w.st);
+    k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool,
+                                                     g->mark, w.claim, w.d_epoch, w.st);
     // insertions: merge, count on the post-insertion graph, clear the marks
     k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
                                           g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10, w.st);
+    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, 2 * cap, w.long_runs, g->start, g->used, g->cap, g->pool,
+                                                    g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
+                                                    w.st);
     DeltaArgs B = delta_args(g, p->sp);
     B.ilist = w.ilist;
     B.count_dev = &w.st->n_ins;

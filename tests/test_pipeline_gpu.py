@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from custingeralg_b200 import api, generators as G, native as N
-from tests.test_stream_gpu import random_batch
+from tests.test_stream_gpu import edge_set, expected_after, random_batch
 
 pytestmark = pytest.mark.gpu
 
@@ -106,3 +106,76 @@ def test_pipeline_rejects_oversize_batch_and_recaptures_on_new_outputs():
     T, _ = _recount(graph, n)
     assert T == T0 + total
     pipe.close()
+
+
+@pytest.mark.parametrize("path", ["pipeline", "apply"])
+def test_long_lists_insert_and_delete(path):
+    """Hub lists above 2048 entries take the CTA kernels (k_insert_long, k_compact_long)."""
+    torch = _torch()
+    rng = np.random.default_rng(21)
+    n = 12000
+    hub_nb = rng.choice(np.arange(1, n), 5000, replace=False).astype(np.int32)
+    ru = rng.integers(0, n, 40000).astype(np.int32)
+    rv = rng.integers(0, n, 40000).astype(np.int32)
+    src = np.concatenate([np.zeros(hub_nb.size, np.int32), ru, np.full(2500, 7, np.int32)])
+    dst = np.concatenate([hub_nb, rv, rng.integers(0, n, 2500).astype(np.int32)])
+    base = G.from_pairs(n, src, dst)
+    assert np.diff(base.off).max() > 2048
+    graph = api.Graph.from_csr(base, slack=0.1)
+    T0, pv0 = _recount(graph, n)
+    pipe = api.Pipeline(graph, 1 << 14) if path == "pipeline" else None
+    pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cur = base
+    for it in range(4):
+        k = 6000
+        s = np.where(rng.random(k) < 0.5, 0, rng.integers(0, n, k)).astype(np.int32)  # half touch the hub
+        d = rng.integers(0, n, k).astype(np.int32)
+        x = np.zeros(k, np.uint8)
+        src_of = np.repeat(np.arange(n, dtype=np.int32), np.diff(cur.off))
+        hub_edges = np.nonzero(src_of == 0)[0]
+        pick = rng.choice(hub_edges, 1500, replace=False)
+        s[:1500], d[:1500], x[:1500] = 0, cur.ind[pick], 1    # delete 1500 hub edges
+        ts, td, tx = _dev(torch, s, d, x)
+        if pipe is not None:
+            pipe.apply(ts, td, tx, per_vertex=pv, delta_dev=delta)
+            pipe.sync()
+        else:
+            graph.apply_batch(ts, td, tx, per_vertex=pv, delta_dev=delta)
+        want = expected_after(n, edge_set(cur), s, d, x)
+        off, ind = graph.export()
+        assert np.array_equal(off, want.off) and np.array_equal(ind, want.ind)
+        cur = G.Csr(n, off, ind)
+        T, pvn = _recount(graph, n)
+        assert T == T0 + int(delta.item())
+        assert torch.equal(pvn, (pv0.to(torch.int64) + pv[:n].to(torch.int64)).to(torch.int32))
+    if pipe is not None:
+        pipe.close()
+
+
+def test_custinger_path_long_lists_round_trip():
+    """edgeInsertionsSorted then edgeDeletionsSorted of the same batch on hub lists > 2048."""
+    torch = _torch()
+    rng = np.random.default_rng(33)
+    n = 9000
+    nb = rng.choice(np.arange(1, n), 4000, replace=False).astype(np.int32)
+    base = G.from_pairs(n, np.concatenate([np.zeros(nb.size, np.int32), rng.integers(0, n, 20000).astype(np.int32)]),
+                        np.concatenate([nb, rng.integers(0, n, 20000).astype(np.int32)]))
+    graph = api.Graph.from_csr(base, slack=0.0)
+    k = 3000
+    u = np.where(rng.random(k) < 0.6, 0, rng.integers(0, n, k)).astype(np.int32)
+    v = rng.integers(0, n, k).astype(np.int32)
+    s = np.concatenate([u, v])
+    d = np.concatenate([v, u])
+    ds = torch.from_numpy(s).cuda()
+    dd = torch.from_numpy(d).cuda()
+    off = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    dup = torch.zeros(s.size, dtype=torch.int32, device="cuda")
+    N.check(N.lib().tc_batch_sort(n, ds.data_ptr(), dd.data_ptr(), s.size, off.data_ptr(), dup.data_ptr(), None))
+    N.check(N.lib().tc_insert_sorted(graph.handle, ds.data_ptr(), dd.data_ptr(), s.size, dup.data_ptr(), None, None))
+    want = expected_after(n, edge_set(base), u, v, np.zeros(k, np.uint8))
+    o1, i1 = graph.export()
+    assert np.array_equal(o1, want.off) and np.array_equal(i1, want.ind)
+    N.check(N.lib().tc_delete_sorted(graph.handle, ds.data_ptr(), dd.data_ptr(), dup.data_ptr(), s.size, None))
+    o2, i2 = graph.export()
+    assert np.array_equal(o2, base.off) and np.array_equal(i2, base.ind)
