@@ -225,7 +225,7 @@ const char* tc_status_string(tc_status s) {
 void tc_sched_default(tc_sched* s) {
   if (!s) return;
   memset(s, 0, sizeof(*s));
-  s->warp_max_deg = 256;     // out-degree up to which one warp counts a vertex alone
+  s->warp_max_deg = 64;      // centre out-degree up to which one warp counts it alone
   s->search_ratio_x16 = 16;  // streaming: search when d_long > d_short (log2 d_long + 1)
   s->lane_max_deg = 8;       // static: one lane walks each list of at most 8 entries
   s->blocks_per_sm = 0;

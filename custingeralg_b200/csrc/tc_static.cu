@@ -14,22 +14,24 @@
 //     chunk moves the pieces together), then tiles of 32 vertex ids from another, so a
 //     degree-64k hub is neither one warp's serial tail nor a load imbalance. The same pass
 //     checks the input (ids in range, strictly ascending lists, no self-loops, a signed edge
-//     checksum for symmetry) and fills the tier queues of the count.
-//  2. Counting. k_count is a persistent grid over three tiers of source vertex u by its
-//     out-degree a = d+(u):
-//       L  a > warp_max:    one CTA per vertex; N+(u) staged in shared memory as a bucketized
-//                           hash set (1024 entries per pass);
-//       M  32 < a <= warp_max (<= 256): one warp per vertex from a queue, warp-private set;
-//       S  2 <= a <= 32:    one warp per vertex, claimed in chunks of vertex ids.
-//     The warp takes the out-neighbours v of u one at a time and streams N+(v) with coalesced
-//     loads (four per lane in flight), probing every element into the hash set ("probe"
-//     strategy); for an edge whose N+(v) is long next to N+(u) it binary-searches the entries
-//     of N+(u) into N+(v) instead ("search" strategy). The scheduler (threshold or learned
-//     per-degree-cell table) picks the strategy per edge.
-//  3. Attribution. Per-vertex counts never take a global atomic per triangle: the three
-//     vertices of a triangle found at u are u, v = A[i] and w = A[j], all in the staged list
-//     A, so they accumulate in registers / shared-memory counters and flush with at most one
-//     global atomic per oriented edge. The triangle total takes one global atomic per CTA.
+//     checksum for symmetry) and fills the work queues of the count.
+//  2. Counting. Every edge {c, o} is intersected once, at its centre c: the endpoint with the
+//     larger out-degree (ties to the smaller id). The centre's N+(c) is a shared-memory hash set
+//     of 4-slot buckets; the other list N+(o), the shorter one, goes through it, so the probe
+//     work is the sum over edges of min(d+u, d+v). k_count is a persistent grid; a centre walks
+//     its original neighbour list N(c) in groups of 32 and takes the neighbours it is centre
+//     for. Tiers by a = d+(c):
+//       CTA   a > warp_max: one CTA per item of 512 neighbours, N+(c) staged 1024 entries per
+//             pass in the full 2048-slot table (load <= 0.25 up to 512 entries);
+//       warp  1 <= a <= warp_max: one warp per centre (items of 256 neighbours for centres with
+//             more), a warp-private set of up to 512 slots.
+//     Per edge, the warp streams N+(o) with coalesced loads (four per lane in flight), or, for
+//     short lists, one lane walks it while the other lanes walk theirs; the scheduler
+//     (threshold or learned per-degree-cell table) picks.
+//  3. Attribution. Per-vertex counts never take a global atomic per triangle: the centre's count
+//     stays in registers, the other endpoint's is reduced once per list, and the third
+//     vertex's is a shared-memory counter of the staged entry; they flush with at most one
+//     global atomic per edge or staged entry. The triangle total takes one global atomic per CTA.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -446,8 +448,9 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
     uint32_t c_acc = 0;
     for (int cb = 0; cb < a; cb += kChunk) {
       const int clen = min(kChunk, a - cb);
-      int bits = 4;  // buckets: 4 * 2^bits slots >= 2 clen, load <= 0.5
-      while ((4 << bits) < 2 * clen) ++bits;
+      // the whole table whatever clen: load clen / kHashMax (<= 0.25 up to 512 entries, <= 0.5)
+      constexpr int bits = 9;
+      static_assert((4 << bits) == kHashMax, "CTA table size");
       const int S = 4 << bits;
       for (int s = threadIdx.x; s < S; s += kThreads) L.hkeys[s] = -1;
       for (int j = threadIdx.x; j < clen; j += kThreads) {
