@@ -21,7 +21,7 @@
 //     work is the sum over edges of min(d+u, d+v). k_count is a persistent grid; a centre walks
 //     its original neighbour list N(c) in groups of 32 and takes the neighbours it is centre
 //     for. Tiers by a = d+(c):
-//       CTA   a > warp_max: one CTA per item of 512 neighbours, N+(c) staged 1024 entries per
+//       CTA   a > warp_max: one CTA per item of 4096 neighbours, N+(c) staged 1024 entries per
 //             pass in the full 2048-slot table (load <= 0.25 up to 512 entries);
 //       warp  1 <= a <= warp_max: one warp per centre (items of 256 neighbours for centres with
 //             more), a warp-private set of up to 512 slots.
@@ -53,7 +53,7 @@ constexpr int kChunk = 1024;      // A entries staged per pass for an L-tier ver
 constexpr int kHashMax = 2048;    // hash slots for such a chunk (load <= 0.5)
 constexpr int kUnroll = 4;        // list elements a lane loads before probing (independent loads)
 constexpr int kWarpRange = 256;   // neighbours of a warp-tier centre per work item
-constexpr int kCtaRange = 512;    // neighbours of a CTA-tier centre per work item
+constexpr int kCtaRange = 4096;   // neighbours of a CTA-tier centre per work item
 static_assert(kWarpRange >= kItemRangeMin && kCtaRange >= kItemRangeMin, "queue sizing");
 constexpr int kMedSlots = 2 * kWarpTierMax;  // warp-private hash slots (load <= 0.25 up to a = 128, else <= 0.5)
 // Hash sets are bucketized: 4 slots per 16-byte bucket, probed with one 128-bit shared load,
