@@ -7,7 +7,15 @@
 
 #include <cuda_runtime.h>
 
+#include <iostream>
+#include <string>
+
 #include "cuStingerDefs.hpp"
+
+// The reference drivers use cout, endl and string unqualified (tests/cct.cpp:216, 240), relying
+// on the cuStinger core headers to open namespace std for them; this header does the same so
+// that they compile unchanged.
+using namespace std;
 
 void readGraphDIMACS(char* filePath, length_t** prmoff, vertexId_t** prmind, length_t* prmnv, length_t* prmne,
                      bool isRmat);
