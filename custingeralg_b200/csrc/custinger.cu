@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "cuStinger.hpp"
 #include "static_triangle_counting/cct.hpp"
@@ -46,7 +47,26 @@ length_t exactUpdateAllocater(length_t elements, length_t overLimit) { return el
 
 cuStinger::cuStinger(initAllocator ia, updateAllocator ua) : ia_(ia), ua_(ua) {}
 
-cuStinger::~cuStinger() { freecuStinger(); }
+cuStinger::cuStinger(const cuStinger& other)
+    : nv(other.nv), g_(other.g_), ia_(other.ia_), ua_(other.ua_), owns_graph_(false), status_(other.status_) {}
+
+cuStinger::~cuStinger() {
+  if (owns_graph_) freecuStinger();
+  else releaseView();
+}
+
+void cuStinger::releaseView() {
+  cudaFree(d_self_);
+  cudaFree(d_vd_);
+  cudaFree(d_edges_);
+  cudaFree(d_adj_);
+  d_self_ = nullptr;
+  d_vd_ = nullptr;
+  d_edges_ = nullptr;
+  d_adj_ = nullptr;
+  dVD = nullptr;
+  view_stale_ = true;
+}
 
 void cuStinger::initializeCuStinger(cuStingerInitConfig& cfg) {
   freecuStinger();
@@ -67,19 +87,10 @@ void cuStinger::initializeCuStinger(cuStingerInitConfig& cfg) {
 }
 
 void cuStinger::freecuStinger() {
-  if (g_) tc_graph_destroy(g_);
+  if (g_ && owns_graph_) tc_graph_destroy(g_);
   g_ = nullptr;
-  cudaFree(d_self_);
-  cudaFree(d_vd_);
-  cudaFree(d_edges_);
-  cudaFree(d_adj_);
-  d_self_ = nullptr;
-  d_vd_ = nullptr;
-  d_edges_ = nullptr;
-  d_adj_ = nullptr;
-  dVD = nullptr;
+  releaseView();
   nv = 0;
-  view_stale_ = true;
 }
 
 void cuStinger::refreshDeviceView() {
@@ -238,6 +249,35 @@ void BatchUpdate::sortDeviceBUD(const int blockdim) {
     cudaMemcpy(host_->indDuplicate_, dev_->indDuplicate_, sizeof(length_t) * b, cudaMemcpyDeviceToHost);
     cudaMemcpy(host_->offsets_, dev_->offsets_, sizeof(length_t) * ((size_t)dev_->nv_ + 1), cudaMemcpyDeviceToHost);
   }
+}
+
+// Sort check of the reference's sort test (declared and called at tests/cct_upd.cpp:30,173; its
+// definition is not in the reference tree): sort the batch on the device, then verify on the
+// host that the entries are ordered by (src, dst), that the batch CSR offsets over src match
+// them, and that exactly the self-loops and repeats are flagged. Prints one line.
+void testSort(length_t nv, BatchUpdate& bu, const int blockdim) {
+  bu.sortDeviceBUD(blockdim);
+  BatchUpdateData* d = bu.getDeviceBUD();
+  const length_t b = *bu.getHostBUD()->getBatchSize();
+  std::vector<vertexId_t> src((size_t)std::max(b, 1)), dst(src.size());
+  std::vector<length_t> dup(src.size()), off((size_t)nv + 1);
+  cudaMemcpy(src.data(), d->getSrc(), sizeof(vertexId_t) * (size_t)b, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dst.data(), d->getDst(), sizeof(vertexId_t) * (size_t)b, cudaMemcpyDeviceToHost);
+  cudaMemcpy(dup.data(), d->getIndDuplicate(), sizeof(length_t) * (size_t)b, cudaMemcpyDeviceToHost);
+  cudaMemcpy(off.data(), d->getOffsets(), sizeof(length_t) * ((size_t)nv + 1), cudaMemcpyDeviceToHost);
+  length_t bad = 0, dups = 0;
+  for (length_t i = 0; i < b; ++i) {
+    const bool repeat = i > 0 && src[i] == src[i - 1] && dst[i] == dst[i - 1];
+    const bool expect_dup = src[i] == dst[i] || repeat;
+    if (i > 0 && (src[i] < src[i - 1] || (src[i] == src[i - 1] && dst[i] < dst[i - 1]))) ++bad;
+    if ((dup[i] != 0) != expect_dup) ++bad;
+    dups += dup[i] != 0;
+  }
+  for (vertexId_t v = 0; v < nv; ++v)
+    for (length_t k = off[v]; k < off[v + 1]; ++k)
+      if (k < 0 || k >= b || src[k] != v) ++bad;
+  if (off[0] != 0 || off[nv] != b) ++bad;
+  printf("testSort: %d entries, %d flagged as duplicates, %s\n", b, dups, bad ? "NOT SORTED" : "sorted");
 }
 
 // ---- triangle counting entry points --------------------------------------------------------------

@@ -69,7 +69,9 @@ class cuStinger {
 
   explicit cuStinger(initAllocator ia = defaultInitAllocater, updateAllocator ua = defaultUpdateAllocater);
   ~cuStinger();
-  cuStinger(const cuStinger&) = delete;
+  // A copy (the reference drivers pass cuStinger by value, tests/cct_upd.cpp:124) is a view of
+  // the same graph: it reads and updates it, but freeing stays with the original.
+  cuStinger(const cuStinger& other);
   cuStinger& operator=(const cuStinger&) = delete;
 
   void initializeCuStinger(cuStingerInitConfig& cfg);
@@ -104,7 +106,9 @@ class cuStinger {
   cusEdgeData* d_edges_ = nullptr;
   cusEdgeData** d_adj_ = nullptr;
   bool view_stale_ = true;
+  bool owns_graph_ = true;
   tc_status status_ = TC_OK;
+  void releaseView();
   friend class BatchUpdate;
 };
 

@@ -68,4 +68,8 @@ class BatchUpdate {
   bool sorted_ = false;
 };
 
+// Sort the batch on the device and check the result on the host, printing one line (the
+// reference driver's sort test, tests/cct_upd.cpp:30,173).
+void testSort(length_t nv, BatchUpdate& bu, const int blockdim);
+
 #endif
