@@ -13,7 +13,7 @@ namespace tc {
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kHubChunk = 2048;     // orientation: list entries per warp work item of a hub
-constexpr int kWarpTierMax = 256;   // largest out-degree a single warp counts on its own
+constexpr int kWarpTierMax = 128;   // largest out-degree a single warp counts on its own
 constexpr int kItemRangeMin = 256;  // fewest neighbours of a count work item (queue sizing)
 
 // ---- error reporting -------------------------------------------------------------------

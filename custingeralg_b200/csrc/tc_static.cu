@@ -23,8 +23,9 @@
 //     for. Tiers by a = d+(c):
 //       CTA   a > warp_max: one CTA per item of 4096 neighbours, N+(c) staged 1024 entries per
 //             pass in the full 2048-slot table (load <= 0.25 up to 512 entries);
-//       warp  1 <= a <= warp_max: one warp per centre (items of 256 neighbours for centres with
-//             more), a warp-private set of up to 512 slots.
+//       warp  1 <= a <= warp_max (at most 128): one warp per centre (items of 256 neighbours for
+//             centres with more), a warp-private set of up to 256 slots.
+//     CTAs of 4 warps, 12 resident per SM (40 registers, 16 KB of shared memory each).
 //     Per edge, the warp streams N+(o) with coalesced loads (four per lane in flight), or, for
 //     short lists, one lane walks it while the other lanes walk theirs; the scheduler
 //     (threshold or learned per-degree-cell table) picks.
@@ -55,7 +56,7 @@ constexpr int kUnroll = 4;        // list elements a lane loads before probing (
 constexpr int kWarpRange = 256;   // neighbours of a warp-tier centre per work item
 constexpr int kCtaRange = 4096;   // neighbours of a CTA-tier centre per work item
 static_assert(kWarpRange >= kItemRangeMin && kCtaRange >= kItemRangeMin, "queue sizing");
-constexpr int kMedSlots = 2 * kWarpTierMax;  // warp-private hash slots (load <= 0.25 up to a = 128, else <= 0.5)
+constexpr int kMedSlots = 2 * kWarpTierMax;  // warp-private hash slots (load <= 0.25 up to a = 64, else <= 0.5)
 // Hash sets are bucketized: 4 slots per 16-byte bucket, probed with one 128-bit shared load,
 // so a lookup ends after one bucket unless that bucket is full (rare at these loads).
 constexpr int kScanThreads = 256;
@@ -99,10 +100,10 @@ struct WarpTable {
   uint8_t hidx[kMedSlots];
 };
 
-// CTA-shared staging of one chunk of a CTA-tier centre's N+(c).
+// CTA-shared staging of one chunk of a CTA-tier centre's N+(c). The entries themselves are read
+// from global memory (L2) when inserted and flushed, which keeps the table at 16 KB.
 struct BlockTable {
   alignas(16) int32_t hkeys[kHashMax];
-  int32_t sA[kChunk];
   uint32_t cnt[kChunk];
   int16_t hidx[kHashMax];
 };
@@ -408,7 +409,7 @@ __device__ __forceinline__ unsigned long long make_item(int32_t c, int32_t k0) {
 }
 
 template <int PV>
-__global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const int32_t* __restrict__ ind,
+__global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const int32_t* __restrict__ ind,
                                                     const int32_t* __restrict__ degv,
                                                     const int32_t* __restrict__ dplus,
                                                     const int64_t* __restrict__ offp,
@@ -454,13 +455,12 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
       const int S = 4 << bits;
       for (int s = threadIdx.x; s < S; s += kThreads) L.hkeys[s] = -1;
       for (int j = threadIdx.x; j < clen; j += kThreads) {
-        L.sA[j] = __ldg(Ag + cb + j);
         L.cnt[j] = 0;
       }
       if (threadIdx.x == 0) sm.gctr = 0;
       __syncwarp();
       __syncthreads();
-      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, L.hidx, bits, L.sA[j], j);
+      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, L.hidx, bits, __ldg(Ag + cb + j), j);
       __syncwarp();
       __syncthreads();
       const int ngroups = (k1 - k0 + kWarp - 1) / kWarp;
@@ -479,7 +479,7 @@ __global__ void __launch_bounds__(kThreads, 10) k_count(const int32_t n, const i
       if (PV != TC_PV_NONE) {
         for (int j = threadIdx.x; j < clen; j += kThreads) {
           const uint32_t x = L.cnt[j];
-          if (x) atomicAdd(&out[L.sA[j]], x * flush_mult<PV>());
+          if (x) atomicAdd(&out[__ldg(Ag + cb + j)], x * flush_mult<PV>());
         }
       }
       __syncwarp();

@@ -40,7 +40,7 @@ int ilog2(int64_t x) {
 
 std::vector<tc_sched> candidates() {
   std::vector<tc_sched> out;
-  const int warp_max[] = {64, 128, 256};
+  const int warp_max[] = {32, 64, 128};
   const int lane_max[] = {0, 4, 8, 16};
   const int chunk[] = {32, 128};
   const int bps[] = {0, 6};

@@ -59,7 +59,7 @@ enum { TC_MEM_DEVICE = 0, TC_MEM_HOST = 1 };
  * tc_sched_default() fills the fixed degree-threshold heuristic. */
 typedef struct tc_sched {
   int32_t warp_max_deg;   /* static count: a centre (the edge endpoint whose N+ is hashed) with
-                             out-degree up to this is counted by one warp (<= 256), above by a CTA */
+                             out-degree up to this is counted by one warp (<= 128), above by a CTA */
   int32_t search_ratio_x16; /* streaming delta count: edge {x,y} binary-searches the shorter list
                                into the longer one when 16 d_long > ratio * d_short (log2 d_long + 1),
                                else merges */
