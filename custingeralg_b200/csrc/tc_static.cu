@@ -30,9 +30,10 @@
 //     short lists, one lane walks it while the other lanes walk theirs; the scheduler
 //     (threshold or learned per-degree-cell table) picks.
 //  3. Attribution. Per-vertex counts never take a global atomic per triangle: the centre's count
-//     stays in registers, the other endpoint's is reduced once per list, and the third
-//     vertex's is a shared-memory counter of the staged entry; they flush with at most one
-//     global atomic per edge or staged entry. The triangle total takes one global atomic per CTA.
+//     stays in registers, the other endpoint's is reduced once per list (one redux.sync), and
+//     the third vertex's is a shared-memory counter beside the hash slot that the probe found;
+//     they flush with at most one global atomic per edge or staged entry. The triangle total
+//     takes one global atomic per CTA.
 #include <algorithm>
 #include <climits>
 #include <cstring>
@@ -92,20 +93,18 @@ __device__ unsigned long long* tc_dbg_kern = nullptr;
   } while (0)
 #endif
 
-// Warp-private staging of one centre's N+(c) (warp tier).
+// Hash sets of staged entries of N+(c). The third-vertex counter of an entry sits beside its
+// slot: cnt[s] counts the triangles found through the key hkeys[s], so a hit adds to the slot
+// it found with no indirection. Warp-private set (warp tier):
 struct WarpTable {
   alignas(16) int32_t hkeys[kMedSlots];
-  int32_t sA[kWarpTierMax];
-  uint32_t cnt[kWarpTierMax];
-  uint8_t hidx[kMedSlots];
+  uint32_t cnt[kMedSlots];
 };
 
-// CTA-shared staging of one chunk of a CTA-tier centre's N+(c). The entries themselves are read
-// from global memory (L2) when inserted and flushed, which keeps the table at 16 KB.
+// CTA-shared set of one chunk of a CTA-tier centre's N+(c) (16 KB):
 struct BlockTable {
   alignas(16) int32_t hkeys[kHashMax];
-  uint32_t cnt[kChunk];
-  int16_t hidx[kHashMax];
+  uint32_t cnt[kHashMax];
 };
 
 struct CountSmem {
@@ -143,22 +142,17 @@ __device__ __forceinline__ uint32_t hash_bucket(int32_t key, int bbits) {
   return ((uint32_t)key * 0x9E3779B1u) >> (32 - bbits);
 }
 
-// Insert key (unique) with payload idx into a table of 2^bbits buckets of 4 slots (load <= 0.5,
-// so a bucket with a free slot is always found within 2^bbits steps). Slots of a bucket fill in
-// order and are never freed, so a key that moved on found every slot before it taken.
-template <typename IdxT>
-__device__ __forceinline__ void hash_insert(int32_t* keys, IdxT* idx, int bbits, int32_t key, int j) {
+// Insert key (unique) into a table of 2^bbits buckets of 4 slots (load <= 0.5, so a bucket with
+// a free slot is always found within 2^bbits steps). Slots of a bucket fill in order and are
+// never freed, so a key that moved on found every slot before it taken.
+__device__ __forceinline__ void hash_insert(int32_t* keys, int bbits, int32_t key) {
   const uint32_t bmask = (1u << bbits) - 1;
   uint32_t b = hash_bucket(key, bbits);
   for (uint32_t it = 0; it <= bmask; ++it) {
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int32_t prev = atomicCAS(&keys[4 * b + t], -1, key);
-      if (prev == -1) {
-        idx[4 * b + t] = (IdxT)j;
-        return;
-      }
-      if (prev == key) return;
+      if (prev == -1 || prev == key) return;
     }
     b = (b + 1) & bmask;
   }
@@ -213,13 +207,13 @@ __device__ __forceinline__ bool centre_of(int32_t c, int a, int32_t o, int b) {
 }
 
 // Probe one entry key of the list owned by o into the hash set; returns 1 on a hit. Per hit, the
-// third vertex's counter cnt[hidx[slot]] gets its weight; vacc and c_acc collect the weights of
+// third vertex's counter cnt[slot] gets its weight; vacc and c_acc collect the weights of
 // o and of the centre c (TC_PV_CSR only: in handle mode all weights are 1 and the caller counts
 // the hits instead).
-template <int PV, typename IdxT>
+template <int PV>
 __device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c, const int32_t o,
-                                              const int32_t* hkeys, const IdxT* hidx, const int bits,
-                                              uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+                                              const int32_t* hkeys, const int bits, uint32_t* cnt,
+                                              uint32_t& c_acc, uint32_t& vacc) {
   // First bucket in one 128-bit load; the common case (a miss in a bucket with a free slot)
   // ends here without computing a slot.
   const uint32_t bk = hash_bucket(key, bits);
@@ -230,23 +224,23 @@ __device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c
                     : hash_find_after(hkeys, bits, key, bk);
   if (s < 0) return 0;
   if (PV == TC_PV_HANDLE) {
-    atomicAdd(&cnt[hidx[s]], 1u);
+    atomicAdd(&cnt[s], 1u);
   } else if (PV == TC_PV_CSR) {
     uint32_t wc, wo, ww;
     tri_weights<PV>(c, o, key, wc, wo, ww);
     c_acc += wc;
     vacc += wo;
-    if (ww) atomicAdd(&cnt[hidx[s]], ww);
+    if (ww) atomicAdd(&cnt[s], ww);
   }
   return 1;
 }
 
 // The warp streams the list lst[0 .. len) through the hash set with coalesced loads, kUnroll
 // per lane in flight; returns this lane's hits.
-template <int PV, typename IdxT>
+template <int PV>
 __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
-                                               const int32_t o, const int32_t* hkeys, const IdxT* hidx,
-                                               const int bits, uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+                                               const int32_t o, const int32_t* hkeys, const int bits,
+                                               uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
   const int lane = threadIdx.x & (kWarp - 1);
   uint32_t hits = 0;
   for (int k0 = lane; k0 < len; k0 += kUnroll * kWarp) {
@@ -271,13 +265,13 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, 
         if (s >= 0) {
           ++hits;
           if (PV == TC_PV_HANDLE) {
-            atomicAdd(&cnt[hidx[s]], 1u);
+            atomicAdd(&cnt[s], 1u);
           } else if (PV == TC_PV_CSR) {
             uint32_t wc, wo, ww;
             tri_weights<PV>(c, o, key, wc, wo, ww);
             c_acc += wc;
             vacc += wo;
-            if (ww) atomicAdd(&cnt[hidx[s]], ww);
+            if (ww) atomicAdd(&cnt[s], ww);
           }
         }
       }
@@ -289,10 +283,10 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, 
 // One lane walks a whole (short) list lst[0 .. len), kUnroll entries in flight; returns the
 // hits. The lanes of a warp walk different lists at once, so short lists do not leave most of
 // the warp idle.
-template <int PV, typename IdxT>
+template <int PV>
 __device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
-                                              const int32_t o, const int32_t* hkeys, const IdxT* hidx,
-                                              const int bits, uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+                                              const int32_t o, const int32_t* hkeys, const int bits,
+                                              uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
   uint32_t hits = 0;
   for (int k0 = 0; k0 < len; k0 += kUnroll) {
     int32_t w[kUnroll];
@@ -300,23 +294,22 @@ __device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, c
     for (int j = 0; j < kUnroll; ++j) w[j] = k0 + j < len ? __ldg(lst + k0 + j) : -1;
 #pragma unroll
     for (int j = 0; j < kUnroll; ++j)
-      if (w[j] >= 0) hits += probe_one<PV>(w[j], c, o, hkeys, hidx, bits, cnt, c_acc, vacc);
+      if (w[j] >= 0) hits += probe_one<PV>(w[j], c, o, hkeys, bits, cnt, c_acc, vacc);
   }
   return hits;
 }
 
 // One warp takes the neighbours o = nbr[0 .. gcount) of centre c (out-degree a) and
 // intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), goes
-// through the hash set of the staged chunk of N+(c) (2^bits buckets, hidx[slot] = entry,
-// cnt[entry] its counter). Per edge the scheduler picks how (table cell, else b <= lane_max):
+// through the hash set of the staged chunk of N+(c) (2^bits buckets, cnt[slot] the counter of
+// the key in that slot). Per edge the scheduler picks how (table cell, else b <= lane_max):
 //   lane: each such lane walks its own list, all at once (short lists);
 //   warp: the lists are taken one at a time and the warp streams each with coalesced loads, so
 //         o, its list and its count stay warp-uniform.
-template <int PV, typename IdxT>
+template <int PV>
 __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, const int a,
                                               const int32_t* __restrict__ nbr, const int gcount,
-                                              const int32_t* hkeys, const IdxT* hidx,
-                                              const int bits, uint32_t* cnt, const int32_t* __restrict__ dplus,
+                                              const int32_t* hkeys, const int bits, uint32_t* cnt, const int32_t* __restrict__ dplus,
                                               const int64_t* __restrict__ offp, const int32_t* __restrict__ indp,
                                               uint32_t* __restrict__ out, const SchedParams& sp, uint32_t& tri,
                                               uint32_t& c_acc) {
@@ -334,7 +327,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
   if (__any_sync(kFull, by_lane)) {
     if (by_lane) {
       uint32_t vacc = 0;
-      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, hidx, bits, cnt, c_acc, vacc);
+      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
       tri += hits;
       if (PV == TC_PV_HANDLE) {
         c_acc += hits;
@@ -352,14 +345,14 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     const int sb = __shfl_sync(kFull, b, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
     uint32_t vacc = 0;
-    const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, hidx, bits, cnt, c_acc, vacc);
+    const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
     tri += hits;
     if (PV == TC_PV_HANDLE) {
       c_acc += hits;
       vacc = hits;
     }
     if (PV != TC_PV_NONE) {
-      vacc = warp_sum(vacc);
+      vacc = __reduce_add_sync(kFull, vacc);
       if (lane == 0 && vacc) atomicAdd(&out[so], vacc * flush_mult<PV>());
     }
   }
@@ -379,25 +372,24 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
   int bits = 4;  // buckets: 4 * 2^bits slots >= 4a (load <= 0.25) while they fit in kMedSlots
   while ((1 << bits) < a && (8 << bits) <= kMedSlots) ++bits;
   const int S = 4 << bits;
-  for (int s = lane; s < S; s += kWarp) t.hkeys[s] = -1;
-  for (int j = lane; j < a; j += kWarp) {
-    t.sA[j] = __ldg(Ag + j);
-    t.cnt[j] = 0;
+  for (int s = lane; s < S; s += kWarp) {
+    t.hkeys[s] = -1;
+    t.cnt[s] = 0;
   }
   __syncwarp();
-  for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, t.hidx, bits, t.sA[j], j);
+  for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, bits, __ldg(Ag + j));
   __syncwarp();
   uint32_t c_acc = 0;
   for (int g = k0; g < k1; g += kWarp)
-    process_group<PV>(n, c, a, ind + start + g, min(kWarp, k1 - g), t.hkeys, t.hidx, bits, t.cnt, dplus, offp,
-                      indp, out, sp, tri, c_acc);
+    process_group<PV>(n, c, a, ind + start + g, min(kWarp, k1 - g), t.hkeys, bits, t.cnt, dplus, offp, indp, out,
+                      sp, tri, c_acc);
   if (PV != TC_PV_NONE) {
-    for (int j = lane; j < a; j += kWarp) {
-      const uint32_t x = t.cnt[j];
-      if (x) atomicAdd(&out[t.sA[j]], x * flush_mult<PV>());
+    for (int s = lane; s < S; s += kWarp) {
+      const uint32_t x = t.cnt[s];
+      if (x) atomicAdd(&out[t.hkeys[s]], x * flush_mult<PV>());
     }
     __syncwarp();
-    c_acc = warp_sum(c_acc);
+    c_acc = __reduce_add_sync(kFull, c_acc);
     if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
   }
   __syncwarp();
@@ -453,14 +445,14 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
       constexpr int bits = 9;
       static_assert((4 << bits) == kHashMax, "CTA table size");
       const int S = 4 << bits;
-      for (int s = threadIdx.x; s < S; s += kThreads) L.hkeys[s] = -1;
-      for (int j = threadIdx.x; j < clen; j += kThreads) {
-        L.cnt[j] = 0;
+      for (int s = threadIdx.x; s < S; s += kThreads) {
+        L.hkeys[s] = -1;
+        L.cnt[s] = 0;
       }
       if (threadIdx.x == 0) sm.gctr = 0;
       __syncwarp();
       __syncthreads();
-      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, L.hidx, bits, __ldg(Ag + cb + j), j);
+      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, bits, __ldg(Ag + cb + j));
       __syncwarp();
       __syncthreads();
       const int ngroups = (k1 - k0 + kWarp - 1) / kWarp;
@@ -471,22 +463,22 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
         const int gk = k0 + g * kWarp;
-        process_group<PV>(n, c, a, ind + start + gk, min(kWarp, k1 - gk), L.hkeys, L.hidx, bits, L.cnt, dplus,
-                          offp, indp, out, sp, tri, c_acc);
+        process_group<PV>(n, c, a, ind + start + gk, min(kWarp, k1 - gk), L.hkeys, bits, L.cnt, dplus, offp, indp,
+                          out, sp, tri, c_acc);
       }
       __syncwarp();
       __syncthreads();
       if (PV != TC_PV_NONE) {
-        for (int j = threadIdx.x; j < clen; j += kThreads) {
-          const uint32_t x = L.cnt[j];
-          if (x) atomicAdd(&out[__ldg(Ag + cb + j)], x * flush_mult<PV>());
+        for (int s = threadIdx.x; s < S; s += kThreads) {
+          const uint32_t x = L.cnt[s];
+          if (x) atomicAdd(&out[L.hkeys[s]], x * flush_mult<PV>());
         }
       }
       __syncwarp();
       __syncthreads();
     }
     if (PV != TC_PV_NONE) {
-      c_acc = warp_sum(c_acc);
+      c_acc = __reduce_add_sync(kFull, c_acc);
       if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
     }
   }
