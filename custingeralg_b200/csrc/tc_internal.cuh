@@ -13,6 +13,8 @@ namespace tc {
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kHubChunk = 2048;     // orientation: list entries per warp work item of a hub
+constexpr int kHubMin = 256;        // orientation: lists longer than this are oriented as hubs
+static_assert(kHubMin <= kHubChunk, "a hub has at least one chunk");
 constexpr int kWarpTierMax = 128;   // largest out-degree a single warp counts on its own
 constexpr int kItemRangeMin = 256;  // fewest neighbours of a count work item (queue sizing)
 
@@ -84,6 +86,8 @@ struct DevStatus {
   unsigned int n_hub_chunks;
   unsigned int q_orient_hub;             // orientation work-queue heads: hub chunks,
   unsigned int q_orient_vtx;             // vertex ids
+  unsigned int cls_cnt[32];              // CTA-queue items per work class
+  unsigned int cls_pos[32];              // and their fill cursors
 };
 
 // ---- scheduler parameters as the kernels see them --------------------------------------
@@ -128,8 +132,8 @@ struct Workspace {
   tc_status ensure(int64_t n, int64_t m_directed, int64_t extent = -1);
   void release();
   // Hub arrays needed for a graph of m directed edges.
-  static int64_t hubs_for(int64_t m) { return m / kHubChunk + 1; }
-  static int64_t chunks_for(int64_t m) { return 2 * (m / kHubChunk) + 2; }
+  static int64_t hubs_for(int64_t m) { return m / kHubMin + 1; }
+  static int64_t chunks_for(int64_t m) { return m / kHubMin + m / kHubChunk + 2; }
   // Count work items of one queue: at most one per vertex plus one per kItemRangeMin neighbours.
   static constexpr int64_t items_for(int64_t n, int64_t m) { return n + m / kItemRangeMin + 1; }
 };

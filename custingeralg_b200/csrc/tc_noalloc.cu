@@ -24,8 +24,8 @@ namespace {
 constexpr int64_t kMaxNv = TC_NOALLOC_MAX_NV;
 constexpr int64_t kMaxEdges = TC_NOALLOC_MAX_EDGES;
 
-constexpr int64_t kMaxHubs = kMaxEdges / kHubChunk + 1;
-constexpr int64_t kMaxChunks = 2 * (kMaxEdges / kHubChunk) + 2;
+constexpr int64_t kMaxHubs = kMaxEdges / kHubMin + 1;
+constexpr int64_t kMaxChunks = kMaxEdges / kHubMin + kMaxEdges / kHubChunk + 2;
 
 // Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | dplus, degv
 // int32[maxnv+1] | large, medium uint64[items] | hub_u, hub_base, hub_done int32[hubs]

@@ -5,14 +5,16 @@
 // lists of every directed edge with a merge path split across 1-32 lanes and one block
 // reduction per source vertex. Here:
 //
-//  1. Orientation (one pass). k_find_hubs registers the vertices with more than kHubChunk
-//     neighbours; k_orient then builds the degree orientation G+ (u -> v iff
+//  1. Orientation (one pass). k_find_hubs registers the vertices with more than kHubMin = 256
+//     neighbours (hubs); k_orient then builds the degree orientation G+ (u -> v iff
 //     (deg u, u) < (deg v, v)) in the input's own index space: N+(u) is written, ascending by
 //     id, at indp[start(u) ...], so no offsets scan is needed. Every triangle {x < y < z in
 //     that order} is found exactly once: at x, on edge x->y, as the common element z of N+(x)
-//     and N+(y). Warps take hub chunks from one queue (the warp that finishes a hub's last
-//     chunk moves the pieces together), then tiles of 32 vertex ids from another, so a
-//     degree-64k hub is neither one warp's serial tail nor a load imbalance. The same pass
+//     and N+(y). Warps take hub chunks of up to 2048 entries from one queue (the warp that
+//     finishes a hub's last chunk moves the pieces together), then tiles of 32 vertex ids from
+//     another, walking a tile's concatenated lists (at most 32 x 256 entries), so neither a
+//     degree-64k hub nor a run of low-id vertices of degree 2000 (R-MAT) is one warp's serial
+//     tail. The same pass
 //     checks the input (ids in range, strictly ascending lists, no self-loops, a signed edge
 //     checksum for symmetry) and fills the work queues of the count.
 //  2. Counting. Every edge {c, o} is intersected once, at its centre c: the endpoint with the
@@ -590,27 +592,8 @@ __device__ __forceinline__ int orient_range(const View& g, const int32_t n, cons
   return cnt;
 }
 
-// Append the work items (u, k0) for k0 = 0, range, 2 range, ... < d to a queue (warp-wide,
-// warp-uniform arguments). Only centres with many neighbours or a large out-degree are queued;
-// they are few, so one atomic per vertex is cheap.
-__device__ __forceinline__ void push_items(const int32_t u, const int32_t d, const int range,
-                                           unsigned long long* __restrict__ q, unsigned* head, const int64_t cap,
-                                           unsigned& bad) {
-  const int lane = threadIdx.x & (kWarp - 1);
-  const int nit = (d + range - 1) / range;
-  unsigned at = 0;
-  if (lane == 0) at = atomicAdd(head, (unsigned)nit);
-  __syncwarp();
-  at = __shfl_sync(kFull, at, 0);
-  if ((int64_t)at + nit > cap) {
-    bad |= kBadCapacity;
-    return;
-  }
-  for (int j = lane; j < nit; j += kWarp) q[at + j] = make_item(u, j * range);
-}
-
 // Orientation bookkeeping of a finished vertex u with degree d and out-degree a (warp-uniform
-// call): its offset, degree and out-degree, the work figures and its count work items.
+// call): its offset, degree and out-degree and the work figures.
 struct OrientAcc {
   unsigned long long work = 0, ei = 0;
   unsigned mx = 0;
@@ -618,10 +601,8 @@ struct OrientAcc {
 
 __device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, const int64_t s, const int32_t a,
                                               int32_t* __restrict__ dplus, int64_t* __restrict__ offp,
-                                              int32_t* __restrict__ degv, unsigned long long* __restrict__ large,
-                                              unsigned long long* __restrict__ medium, const int64_t item_cap,
-                                              DevStatus* __restrict__ st, const int warp_max, const int shard,
-                                              const int nshards, OrientAcc& acc, unsigned& bad) {
+                                              int32_t* __restrict__ degv, const int shard, const int nshards,
+                                              OrientAcc& acc) {
   const int lane = threadIdx.x & (kWarp - 1);
   const bool mine = (u % nshards) == shard;
   if (lane == 0) {
@@ -633,15 +614,12 @@ __device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, 
     if (mine) acc.work += (unsigned long long)a * (unsigned long long)d;
     acc.mx = max(acc.mx, (unsigned)a);
   }
-  if (mine && a > 0) {
-    if (a > warp_max) push_items(u, d, kCtaRange, large, &st->n_large, item_cap, bad);
-    else if (d > kWarpRange) push_items(u, d, kWarpRange, medium, &st->n_medium, item_cap, bad);
-  }
 }
 
-// Register the vertices whose list is longer than kHubChunk: they are oriented in chunks that
-// separate warps take. One thread per vertex; hubs are rare. A hub starts with out-degree 0,
-// so a hub that is never completed (capacity error) leaves nothing for the count to read.
+// Register the vertices whose list is longer than kHubMin: they are oriented in chunks of up to
+// kHubChunk entries that separate warps take. One thread per vertex. A hub starts with
+// out-degree 0, so a hub that is never completed (capacity error) leaves nothing for the count
+// to read.
 template <class View>
 __global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n, int32_t* __restrict__ dplus,
                                                    int64_t* __restrict__ offp, int32_t* __restrict__ degv,
@@ -652,7 +630,7 @@ __global__ void __launch_bounds__(256) k_find_hubs(const View g, const int32_t n
   for (int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; uu < n; uu += (int64_t)gridDim.x * blockDim.x) {
     const int32_t u = (int32_t)uu;
     const int32_t d = g.len(u);
-    if (d <= kHubChunk) continue;
+    if (d <= kHubMin) continue;
     dplus[u] = 0;
     offp[u] = 0;
     degv[u] = 0;
@@ -680,13 +658,11 @@ template <class View, bool kWrite>
 __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, int32_t* __restrict__ dplus,
                                                 int64_t* __restrict__ offp, int32_t* __restrict__ degv,
                                                 int32_t* __restrict__ indp, const int64_t e_cap,
-                                                unsigned long long* __restrict__ large,
-                                                unsigned long long* __restrict__ medium, const int64_t item_cap,
                                                 const int32_t* __restrict__ hub_u,
                                                 const int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_cnt,
                                                 int32_t* __restrict__ hub_done, const int32_t* __restrict__ chunk_hub,
                                                 const int64_t hub_cap, const int64_t chunk_cap, DevStatus* __restrict__ st,
-                                                const int warp_max, const int shard, const int nshards) {
+                                                const int shard, const int nshards) {
   const int lane = threadIdx.x & (kWarp - 1);
   const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
   const unsigned nhubs = (unsigned)min((long long)st->n_hubs, (long long)hub_cap);
@@ -743,39 +719,106 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
       }
       a += cn;
     }
-    finish_vertex(u, d, s, a, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc, bad);
+    finish_vertex(u, d, s, a, dplus, offp, degv, shard, nshards, acc);
   }
 
-  // Vertex tiles (hubs skipped: done above).
+  // Vertex tiles (hubs skipped: done above). The warp walks the concatenated lists of a tile's
+  // 32 vertices, 32 entries per step: short lists leave no lane idle, and a step is one round of
+  // coalesced loads instead of one dependent round per vertex. Lane i keeps vertex t0 + i; the
+  // owner of entry k is the last vertex whose list starts at or before k (a binary search over
+  // the lanes' exclusive prefix of the lengths). An out-neighbour's rank in N+(u) is its vertex's
+  // count from earlier steps (per-warp shared counter) plus the predecessors in its segment.
   constexpr int kTile = 32;
+  __shared__ int32_t s_out[256 / kWarp][kTile];
+  int32_t* const my_out = s_out[threadIdx.x / kWarp];
+  const unsigned lt = lanemask_lt();
   while (true) {
     unsigned t0 = 0;
     if (lane == 0) t0 = atomicAdd(&st->q_orient_vtx, (unsigned)kTile);
     __syncwarp();
     t0 = __shfl_sync(kFull, t0, 0);
     if (t0 >= (unsigned)n) break;
-    const int32_t uu = (int32_t)t0 + lane;
-    const int32_t dl = uu < n ? g.len(uu) : 0;
-    const int64_t sl = uu < n ? g.start(uu) : 0;
-    const int cnt_t = min(kTile, n - (int32_t)t0);
-    for (int i = 0; i < cnt_t; ++i) {
-      const int32_t u = (int32_t)t0 + i;
-      const int32_t d = __shfl_sync(kFull, dl, i);
-      const int64_t s = __shfl_sync(kFull, sl, i);
-      if (d > kHubChunk) continue;
-      if (s < 0 || s + d > e_cap) {
-        bad |= kBadCapacity;
-        finish_vertex(u, 0, 0, 0, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc,
-                      bad);
-        continue;
+    const int32_t u_l = (int32_t)t0 + lane;
+    const bool in_t = u_l < n;
+    const int32_t d_l = in_t ? g.len(u_l) : 0;
+    const int64_t s_l = in_t ? g.start(u_l) : 0;
+    const bool own_l = in_t && d_l <= kHubMin;  // hubs were completed by the chunk loop
+    const bool cap_bad = own_l && (s_l < 0 || s_l + d_l > e_cap);
+    if (cap_bad) bad |= kBadCapacity;
+    const int32_t len_l = own_l && !cap_bad ? d_l : 0;
+    int32_t incl = len_l;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+      const int32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int32_t excl_l = incl - len_l;
+    const int32_t total = __shfl_sync(kFull, incl, kWarp - 1);
+    my_out[lane] = 0;
+    __syncwarp();
+    int32_t last = INT32_MIN;
+    for (int32_t k0 = 0; k0 < total; k0 += kWarp) {
+      const int32_t k = k0 + lane;
+      const bool in = k < total;
+      int i = 0;  // owner lane: the largest i with excl_i <= k (its list is non-empty)
+#pragma unroll
+      for (int step = kWarp / 2; step > 0; step >>= 1) {
+        const int32_t e = __shfl_sync(kFull, excl_l, i + step);  // i + step <= 31
+        if (e <= k) i += step;
       }
-      const int a = d > 0 ? orient_range<View, kWrite>(g, n, u, d, s, 0, d, indp, s, chk, bad) : 0;
-      finish_vertex(u, d, s, a, dplus, offp, degv, large, medium, item_cap, st, warp_max, shard, nshards, acc, bad);
+      const int32_t d = __shfl_sync(kFull, d_l, i);
+      const int64_t s = __shfl_sync(kFull, s_l, i);
+      const int32_t pos = k - __shfl_sync(kFull, excl_l, i);
+      const int32_t u = (int32_t)t0 + i;
+      const int32_t v = in ? g.ind[s + pos] : INT32_MAX;
+      int32_t prev = __shfl_up_sync(kFull, v, 1);
+      if (lane == 0) prev = last;
+      last = __shfl_sync(kFull, v, kWarp - 1);
+      bool pred = false;
+      if (in) {
+        if (v < 0 || v >= n) {
+          bad |= kBadRange;
+        } else {
+          if (pos > 0 && prev >= v) bad |= kBadOrder;
+          if (v == u) bad |= kBadSelfLoop;
+          pred = precedes(d, u, g.len(v), v);
+          const uint64_t h = (u < v) ? sym_hash((uint32_t)u, (uint32_t)v) : sym_hash((uint32_t)v, (uint32_t)u);
+          chk += (u < v) ? h : (0ull - h);
+        }
+      }
+      const unsigned msk = __ballot_sync(kFull, pred);
+      const bool head = in && (pos == 0 || lane == 0);  // first entry of its vertex in this step
+      const unsigned heads = __ballot_sync(kFull, head);
+      const int seg0 = 31 - __clz(heads & (lt | (1u << lane)));
+      const int prior = in ? my_out[i] : 0;
+      __syncwarp();
+      if (kWrite && pred) indp[s + prior + __popc(msk & lt & ~((1u << seg0) - 1u))] = v;
+      if (head) {
+        const unsigned above = heads & ~(lt | (1u << lane));
+        const unsigned below_next = above ? ((1u << (__ffs(above) - 1)) - 1u) : ~0u;
+        my_out[i] = prior + __popc(msk & below_next & ~((1u << lane) - 1u));
+      }
+      __syncwarp();
+    }
+    const int32_t a_l = own_l ? my_out[lane] : 0;
+    __syncwarp();
+    // Finish the tile's vertices, one per lane (the bookkeeping of finish_vertex).
+    if (own_l) {
+      dplus[u_l] = a_l;
+      offp[u_l] = cap_bad ? 0 : s_l;
+      degv[u_l] = cap_bad ? 0 : d_l;
+      const int32_t dd = cap_bad ? 0 : d_l;
+      if (dd >= 2) acc.ei += (unsigned long long)a_l;
+      if ((u_l % nshards) == shard) acc.work += (unsigned long long)a_l * (unsigned long long)dd;
+      acc.mx = max(acc.mx, (unsigned)a_l);
     }
   }
 
   __syncwarp();
   chk = warp_sum(chk);
+  acc.work = warp_sum(acc.work);
+  acc.ei = warp_sum(acc.ei);
+  acc.mx = __reduce_max_sync(kFull, acc.mx);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
   if (lane == 0) {
@@ -784,6 +827,105 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
     if (acc.work) atomicAdd(&st->oriented_work, acc.work);
     if (acc.ei) atomicAdd(&st->edges_intersected, acc.ei);
     if (acc.mx) atomicMax(&st->max_dplus, acc.mx);
+  }
+}
+
+// The count's work queues, filled after the orientation. A centre with out-degree a > warp_max
+// gets CTA items of kCtaRange neighbours; one with a <= warp_max and more than kWarpRange
+// neighbours gets warp items of kWarpRange (the other centres are claimed by id ranges). The CTA
+// queue is ordered by estimated item work, largest first, so the persistent grid does not end
+// on a few long items: the work class of a centre's items is log2(a * min(d, kCtaRange)), and
+// classes are laid out in decreasing order, each in vertex-id order (which on R-MAT keeps
+// centres with shared neighbours together). k_push_items counts the items per class and fills
+// the warp queue; k_fill_items places the CTA items.
+constexpr int kWorkClasses = 32;
+
+__device__ __forceinline__ int work_class(const int32_t a, const int32_t d) {
+  const unsigned long long w = (unsigned long long)a * (unsigned long long)min(d, kCtaRange);
+  return min(kWorkClasses - 1, 63 - __clzll(max(w, 1ull)));
+}
+
+__device__ __forceinline__ bool cta_centre(const int32_t u, const int32_t a, const int warp_max, const int shard,
+                                           const int nshards) {
+  return a > warp_max && (u % nshards) == shard;
+}
+
+__global__ void __launch_bounds__(256) k_push_items(const int32_t n, const int32_t* __restrict__ dplus,
+                                                    const int32_t* __restrict__ degv,
+                                                    unsigned long long* __restrict__ medium, const int64_t item_cap,
+                                                    DevStatus* __restrict__ st, const int warp_max, const int shard,
+                                                    const int nshards) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+  unsigned bad = 0;
+  for (int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp; t * kWarp < n; t += nwarps) {
+    const int64_t uu = t * kWarp + lane;
+    const bool in = uu < n;
+    const int32_t u = (int32_t)uu;
+    const int32_t a = in ? dplus[u] : 0;
+    const int32_t d = in ? degv[u] : 0;
+    if (in && cta_centre(u, a, warp_max, shard, nshards))
+      atomicAdd(&st->cls_cnt[work_class(a, d)], (unsigned)((d + kCtaRange - 1) / kCtaRange));
+    const bool wrp = in && a > 0 && a <= warp_max && d > kWarpRange && (u % nshards) == shard;
+    const int x = wrp ? (d + kWarpRange - 1) / kWarpRange : 0;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int tot = __shfl_sync(kFull, incl, kWarp - 1);
+    if (tot == 0) continue;
+    unsigned base = 0;
+    if (lane == 0) base = atomicAdd(&st->n_medium, (unsigned)tot);
+    base = __shfl_sync(kFull, base, 0);
+    if ((int64_t)base + tot > item_cap) {
+      bad |= kBadCapacity;
+      continue;
+    }
+    for (int j = 0; j < x; ++j) medium[base + (incl - x) + j] = make_item(u, j * kWarpRange);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad |= __shfl_xor_sync(kFull, bad, o);
+  if (lane == 0 && bad) atomicOr(&st->bad_flags, bad);
+}
+
+__global__ void __launch_bounds__(256) k_fill_items(const int32_t n, const int32_t* __restrict__ dplus,
+                                                    const int32_t* __restrict__ degv,
+                                                    unsigned long long* __restrict__ large, const int64_t item_cap,
+                                                    DevStatus* __restrict__ st, const int warp_max, const int shard,
+                                                    const int nshards) {
+  __shared__ unsigned cls_base[kWorkClasses];
+  __shared__ unsigned total;
+  if (threadIdx.x < kWarp) {
+    // exclusive scan over the classes in decreasing order: class c starts after all classes > c
+    const int lane = threadIdx.x;
+    const unsigned x = st->cls_cnt[kWorkClasses - 1 - lane];
+    unsigned incl = x;
+#pragma unroll
+    for (int o = 1; o < kWarp; o <<= 1) {
+      const unsigned y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    cls_base[kWorkClasses - 1 - lane] = incl - x;
+    if (lane == kWarp - 1) total = incl;
+  }
+  __syncthreads();
+  const unsigned n_items = (unsigned)min((long long)total, (long long)item_cap);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->n_large = n_items;
+    if ((long long)total > item_cap) atomicOr(&st->bad_flags, kBadCapacity);
+  }
+  for (int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; uu < n; uu += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t u = (int32_t)uu;
+    const int32_t a = dplus[u];
+    if (!cta_centre(u, a, warp_max, shard, nshards)) continue;
+    const int32_t d = degv[u];
+    const int cls = work_class(a, d);
+    const int nit = (d + kCtaRange - 1) / kCtaRange;
+    const unsigned at = cls_base[cls] + atomicAdd(&st->cls_pos[cls], (unsigned)nit);
+    if ((int64_t)at + nit > (int64_t)n_items) continue;  // only past a capacity error
+    for (int j = 0; j < nit; ++j) large[at + j] = make_item(u, j * kCtaRange);
   }
 }
 
@@ -949,16 +1091,23 @@ tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& 
   if (write) TC_TRY((resident_grid<k_orient<View, true>>(256, &grid)));
   else TC_TRY((resident_grid<k_orient<View, false>>(256, &grid)));
   if (write)
-    k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap, ws.large,
-                                                   ws.medium, ws.item_cap, ws.hub_u, ws.hub_base, ws.hub_cnt,
-                                                   ws.hub_done, ws.chunk_hub, ws.hub_cap, ws.chunk_cap, ws.st,
-                                                   sp.warp_max, sp.shard, sp.nshards);
+    k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap,
+                                                   ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
+                                                   ws.hub_cap, ws.chunk_cap, ws.st, sp.shard, sp.nshards);
   else
     k_orient<View, false><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap,
-                                                    ws.large, ws.medium, ws.item_cap, ws.hub_u, ws.hub_base,
-                                                    ws.hub_cnt, ws.hub_done, ws.chunk_hub, ws.hub_cap, ws.chunk_cap,
-                                                    ws.st, sp.warp_max, sp.shard, sp.nshards);
+                                                    ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
+                                                    ws.hub_cap, ws.chunk_cap, ws.st, sp.shard, sp.nshards);
   TC_CUDA_TRY(cudaGetLastError());
+  if (write) {
+    // the count's work queues (only a count reads them)
+    k_push_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.medium, ws.item_cap, ws.st, sp.warp_max,
+                                                   sp.shard, sp.nshards);
+    TC_CUDA_TRY(cudaGetLastError());
+    k_fill_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.large, ws.item_cap, ws.st, sp.warp_max,
+                                                   sp.shard, sp.nshards);
+    TC_CUDA_TRY(cudaGetLastError());
+  }
   return TC_OK;
 }
 

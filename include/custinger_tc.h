@@ -144,7 +144,7 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
  * region, processes whose allocator forbids device allocation after start-up, or services
  * that budget every byte of device memory up front. Its working memory is a fixed array inside
  * this library's device image, sized for at most TC_NOALLOC_MAX_NV vertices and
- * TC_NOALLOC_MAX_EDGES directed edges (about 32 MB, held by every GPU that loads the library
+ * TC_NOALLOC_MAX_EDGES directed edges (about 49 MB, held by every GPU that loads the library
  * until the process exits); larger graphs are rejected with TC_ERR_CAPACITY. All calls share
  * that array, so calls that overlap on the GPU race: issue them on one stream or order them
  * with events. The first call on a device looks up the array's device address with that
