@@ -61,6 +61,9 @@ def parse():
                     help="captured pipeline (tc_pipeline) or tc_apply_batch per batch")
     ap.add_argument("--stream-sched", choices=["learned", "fixed"], default="learned",
                     help="delta-kernel strategy table: trained network or the fixed ratio rule")
+    ap.add_argument("--static-sched", choices=["learned", "fixed"], default="learned",
+                    help="static count strategy table: trained network (from the first count's degree "
+                         "cells) or the fixed length thresholds")
     return ap.parse_args()
 
 
@@ -246,6 +249,13 @@ def run_ours(a, rank, world, local_rank):
                 raise SystemExit("per-vertex counts differ from the known answer's digest")
             checks = {"triangles": "equals the known answer", "per_vertex_2t": "digest equals the known answer"}
     assert info.edges_intersected == e_int, (info.edges_intersected, e_int)
+    d = N.default_sched()
+    static_sched_desc = f"fixed rule (lane walk up to {d.lane_max_deg}, packed up to {d.packed_max_deg})"
+    if a.static_sched == "learned":
+        from custingeralg_b200 import sched_learn as L
+        if os.path.exists(L.WEIGHTS):
+            sched = L.learned_sched(L.load(L.WEIGHTS), graph, base=sched)  # cells of the count above
+            static_sched_desc = "learned (custingeralg_b200/data/sched_mlp.bin, this graph's degree cells)"
 
     def step():
         graph.count(N.TC_PV_HANDLE, out, tri, sched=sched, sync=False)
@@ -327,13 +337,17 @@ def run_ours(a, rank, world, local_rank):
               "phase_ms": {"orient": round(statistics.mean(orient_ms), 4),
                            "count": round(statistics.mean(count_ms), 4)},
               "clocks": clocks.summary(t_wall0, t_wall1)}
+    result["config"]["static_scheduler"] = static_sched_desc
     if world > 1:
         result["config"]["parallelism"] = f"vertex shards over {world} GPUs + NCCL all-reduce"
 
     # End to end through the C ABI with host buffers: H2D of the CSR from pinned memory, the count
     # (callDeviceAllTrianglesCSR path with per-vertex output), D2H of the per-vertex counts and T.
     if not a.no_e2e:
-        h_off = torch.from_numpy(g.off).pin_memory()
+        # int32 offsets while they fit: the reference's raw-CSR boundary types them as length_t
+        # (int32, tests/cct_csr.cu:279-285); int64 beyond 2^31 - 1 directed edges
+        off_host = g.off.astype(np.int32) if g.m < 2**31 else g.off
+        h_off = torch.from_numpy(off_host).pin_memory()
         h_ind = torch.from_numpy(g.ind).pin_memory()
         d_off = torch.empty_like(h_off, device=dev)
         d_ind = torch.empty_like(h_ind, device=dev)
@@ -370,11 +384,11 @@ def run_ours(a, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_step_s = float(t.item()) / a.steps / 1e3
         result["e2e"] = {"value": e_int / e2e_step_s, "unit": UNIT,
-                         "h2d_bytes_per_step": int(h_off.numel() * 8 + h_ind.numel() * 4),
+                         "h2d_bytes_per_step": int(h_off.numel() * h_off.element_size() + h_ind.numel() * 4),
                          "d2h_bytes_per_step": int(h_out.numel() * 4 + 8),
                          "ms_per_step": e2e_step_s * 1e3,
-                         "path": "tc_count_csr64 (callDeviceAllTrianglesCSR boundary), pinned host CSR in, "
-                                 "per-vertex counts out"}
+                         "path": ("tc_count_csr32" if h_off.dtype == torch.int32 else "tc_count_csr64")
+                                 + " (callDeviceAllTrianglesCSR boundary), pinned host CSR in, per-vertex counts out"}
 
     if rank == 0 and world == 1 and not a.no_streaming:
         result["streaming"] = run_streaming(a, dev)

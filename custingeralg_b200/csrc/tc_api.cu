@@ -228,6 +228,7 @@ void tc_sched_default(tc_sched* s) {
   s->warp_max_deg = 64;      // centre out-degree up to which one warp counts it alone
   s->search_ratio_x16 = 16;  // streaming: search when d_long > d_short (log2 d_long + 1)
   s->lane_max_deg = 8;       // static: one lane walks each list of at most 8 entries
+  s->packed_max_deg = 32;    // static: longer lists up to 32 entries walked packed
   s->blocks_per_sm = 0;
   s->chunk = 64;
   s->use_table = 0;

@@ -293,27 +293,37 @@ tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_fe
   cudaFree(dy);
   if (rc != TC_OK) return rc;
   // Output ids: static count 0 = the warp streams the list through the hash set, 1 = one lane
-  // walks it; streaming 1 = binary search, 2 = merge. Table entry 1 selects the second of the
-  // pair. The outputs are predicted log2 costs per edge. A cell departs from the fixed rule
-  // (static: lane_max_deg; streaming: search_ratio_x16; applied to the cell's mean degrees) only
-  // when the network predicts the other strategy at least kMargin cheaper; otherwise the rule's
-  // choice stays (the fallback).
+  // walks it, 2 = packed walk (the table entry is the output id); streaming 1 = binary search,
+  // 2 = merge (table entries 0 and 1). The outputs are predicted log2 costs per edge. A cell
+  // departs from the fixed rule (static: lane_max_deg / packed_max_deg; streaming:
+  // search_ratio_x16; applied to the cell's mean degrees) only when the network predicts another
+  // strategy at least kMargin cheaper; otherwise the rule's choice stays (the fallback).
   constexpr double kMargin = 0.05;
   const float log_keep = (float)std::log2(1.0 - kMargin);
-  const int s0 = kind == 0 ? 0 : 1, s1 = kind == 0 ? 1 : 2;
   const long long ratio = std::max(0, sch->search_ratio_x16);
   const long long lane_max = std::max(0, sch->lane_max_deg);
+  const long long packed_max = std::max(0, sch->packed_max_deg);
   for (int c = 0; c < 256; ++c) {
     const double a = std::max(1.0, std::exp2((double)feat[c * kIn + 0]) - 1.0);
     const double b = std::max(1.0, std::exp2((double)feat[c * kIn + 1]) - 1.0);
     const long long ai = (long long)std::llround(a), bi = (long long)std::llround(b);
     int lg = 0;
     for (long long t = bi; t > 0; t >>= 1) ++lg;
-    // static: 1 = one lane walks the list (b <= lane_max); streaming: 1 = merge (no search)
-    const int rule = kind == 0 ? (bi <= lane_max ? 1 : 0) : (16LL * bi > ratio * ai * lg ? 0 : 1);
-    const float c0 = y[c * kOut + s0], c1 = y[c * kOut + s1];
-    const float c_rule = rule ? c1 : c0, c_other = rule ? c0 : c1;
-    const int pick = (c_other < c_rule + log_keep) ? 1 - rule : rule;
+    // table entries: static 0 = warp, 1 = lane, 2 = packed; streaming 0 = search, 1 = merge
+    const int rule = kind == 0 ? (bi <= lane_max ? 1 : bi <= packed_max ? 2 : 0)
+                               : (16LL * bi > ratio * ai * lg ? 0 : 1);
+    const int nstrat = kind == 0 ? 3 : 2;
+    const int out0 = kind == 0 ? 0 : 1;  // network output of table entry 0
+    const float c_rule = y[c * kOut + out0 + rule];
+    int pick = rule;
+    float c_best = c_rule + log_keep;
+    for (int e = 0; e < nstrat; ++e) {
+      const float ce = y[c * kOut + out0 + e];
+      if (e != rule && ce < c_best) {
+        c_best = ce;
+        pick = e;
+      }
+    }
     sch->table[c / 16][c % 16] = (uint8_t)pick;
   }
   sch->use_table = 1;

@@ -304,10 +304,14 @@ __device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, c
 // One warp takes the neighbours o = nbr[0 .. gcount) of centre c (out-degree a) and
 // intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), goes
 // through the hash set of the staged chunk of N+(c) (2^bits buckets, cnt[slot] the counter of
-// the key in that slot). Per edge the scheduler picks how (table cell, else b <= lane_max):
-//   lane: each such lane walks its own list, all at once (short lists);
-//   warp: the lists are taken one at a time and the warp streams each with coalesced loads, so
-//         o, its list and its count stay warp-uniform.
+// the key in that slot). Per edge the scheduler picks how (table cell, else the thresholds
+// b <= lane_max, b <= packed_max):
+//   lane:   each such lane walks its own list, all at once (short lists);
+//   packed: the warp walks all such lists of the group concatenated, 32 entries per step (the
+//           owner of an entry by binary search over the lanes' length prefix), so a group of
+//           mid-size lists takes a few rounds of coalesced loads instead of one per list;
+//   warp:   the lists are taken one at a time and the warp streams each with coalesced loads,
+//           so o, its list and its count stay warp-uniform.
 template <int PV>
 __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, const int a,
                                               const int32_t* __restrict__ nbr, const int gcount,
@@ -324,8 +328,11 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
                     (sp.cell_filter == -1 ||
                      (sp.cell_filter >= 0 && log2_cell(a) * 16 + log2_cell(b) == sp.cell_filter));
   const int64_t base = mine ? __ldg(offp + o) : 0;
-  const bool by_lane =
-      mine && (sp.use_table ? sp.table[log2_cell(a)][log2_cell(b)] == 1 : b <= sp.lane_max);
+  const int strat = !mine ? -1
+                    : sp.use_table ? sp.table[log2_cell(a)][log2_cell(b)]
+                                   : (b <= sp.lane_max ? 1 : b <= sp.packed_max ? 2 : 0);
+  const bool by_lane = strat == 1;
+  const bool by_pack = strat == 2;
   if (__any_sync(kFull, by_lane)) {
     if (by_lane) {
       uint32_t vacc = 0;
@@ -339,7 +346,53 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     }
     __syncwarp();
   }
-  unsigned todo = __ballot_sync(kFull, mine && !by_lane);
+  if (__any_sync(kFull, by_pack)) {
+    const int len_l = by_pack ? b : 0;
+    int incl = len_l;
+#pragma unroll
+    for (int d = 1; d < kWarp; d <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, d);
+      if (lane >= d) incl += y;
+    }
+    const int excl_l = incl - len_l;
+    const int total = __shfl_sync(kFull, incl, kWarp - 1);
+    for (int k0 = 0; k0 < total; k0 += kWarp) {
+      const int k = k0 + lane;
+      const bool in = k < total;
+      int i = 0;  // owner lane: the largest i with excl_i <= k (its list is non-empty)
+#pragma unroll
+      for (int step = kWarp / 2; step > 0; step >>= 1) {
+        const int e = __shfl_sync(kFull, excl_l, i + step);  // i + step <= 31
+        if (e <= k) i += step;
+      }
+      const int64_t pbase = __shfl_sync(kFull, base, i);
+      const int pos = k - __shfl_sync(kFull, excl_l, i);
+      const int32_t po = __shfl_sync(kFull, o, i);
+      const int32_t key = in ? __ldg(indp + pbase + pos) : -1;
+      uint32_t vw = 0;  // o's weight of this entry's triangle
+      const uint32_t h = key >= 0 ? probe_one<PV>(key, c, po, hkeys, bits, cnt, c_acc, vw) : 0u;
+      tri += h;
+      if (PV == TC_PV_HANDLE) {
+        c_acc += h;
+        vw = h;
+      }
+      if (PV != TC_PV_NONE) {
+        // o's counter: the first lane of each list's segment in this step adds the segment's sum
+        const bool head = in && (pos == 0 || lane == 0);
+        const unsigned heads = __ballot_sync(kFull, head);
+        const unsigned w0 = __ballot_sync(kFull, vw & 1u);
+        const unsigned w1 = PV == TC_PV_CSR ? __ballot_sync(kFull, vw & 2u) : 0u;
+        if (head && (w0 | w1)) {
+          const unsigned above = heads & ~((2u << lane) - 1u);  // heads of later lanes (lane 31: none)
+          const unsigned seg = (above ? (1u << (__ffs(above) - 1)) - 1u : ~0u) & ~((1u << lane) - 1u);
+          const uint32_t sum = __popc(w0 & seg) + 2u * __popc(w1 & seg);
+          if (sum) atomicAdd(&out[po], sum * flush_mult<PV>());
+        }
+      }
+    }
+    __syncwarp();
+  }
+  unsigned todo = __ballot_sync(kFull, mine && !by_lane && !by_pack);
   while (todo) {
     const int sl = __ffs(todo) - 1;
     todo &= todo - 1;
@@ -1144,6 +1197,7 @@ SchedParams to_params(const tc_sched* s) {
   p.shard = std::min(std::max(0, s->shard), p.nshards - 1);
   p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
   p.lane_max = std::min(64, std::max(0, s->lane_max_deg));
+  p.packed_max = std::max(0, s->packed_max_deg);
   memcpy(p.table, s->table, sizeof(p.table));
   return p;
 }

@@ -41,17 +41,19 @@ int ilog2(int64_t x) {
 std::vector<tc_sched> candidates() {
   std::vector<tc_sched> out;
   const int warp_max[] = {32, 64, 128};
-  const int lane_max[] = {0, 4, 8, 16};
+  // (lane_max, packed_max): lists up to lane_max walked by a lane, up to packed_max packed
+  const int list_rule[][2] = {{8, 0}, {0, 64}, {4, 32}, {8, 32}, {16, 128}};
   const int chunk[] = {32, 128};
   const int bps[] = {0, 6};
   for (int w : warp_max)
-    for (int r : lane_max)
+    for (const auto& r : list_rule)
       for (int c : chunk)
         for (int b : bps) {
           tc_sched s;
           tc_sched_default(&s);
           s.warp_max_deg = w;
-          s.lane_max_deg = r;
+          s.lane_max_deg = r[0];
+          s.packed_max_deg = r[1];
           s.chunk = c;
           s.blocks_per_sm = b;
           out.push_back(s);
@@ -132,11 +134,11 @@ tc_status tc_autotune_save(const char* path) {
   FILE* f = fopen(path, "w");
   if (!f) return fail(TC_ERR_INVALID_ARG, "cannot write %s", path);
   std::lock_guard<std::mutex> lk(cache().mu);
-  fprintf(f, "# tc autotune v2: log2n log2m log2maxdplus warp_max lane_max chunk blocks_per_sm\n");
+  fprintf(f, "# tc autotune v3: log2n log2m log2maxdplus warp_max lane_max chunk blocks_per_sm packed_max\n");
   for (const auto& kv : cache().entries) {
     const tc_sched& s = kv.second;
-    fprintf(f, "%d %d %d %d %d %d %d\n", std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
-            s.warp_max_deg, s.lane_max_deg, s.chunk, s.blocks_per_sm);
+    fprintf(f, "%d %d %d %d %d %d %d %d\n", std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first),
+            s.warp_max_deg, s.lane_max_deg, s.chunk, s.blocks_per_sm, s.packed_max_deg);
   }
   fclose(f);
   return TC_OK;
@@ -151,12 +153,15 @@ tc_status tc_autotune_load(const char* path) {
   std::lock_guard<std::mutex> lk(cache().mu);
   while (fgets(line, sizeof(line), f)) {
     if (line[0] == '#') continue;
-    int a, b, c, w, r, ch, bp;
-    if (sscanf(line, "%d %d %d %d %d %d %d", &a, &b, &c, &w, &r, &ch, &bp) == 7) {
+    int a, b, c, w, r, ch, bp, pk = 0;
+    // v3 lines carry packed_max last; v2 lines (7 fields) get no packed walks
+    const int got = sscanf(line, "%d %d %d %d %d %d %d %d", &a, &b, &c, &w, &r, &ch, &bp, &pk);
+    if (got == 7 || got == 8) {
       tc_sched s;
       tc_sched_default(&s);
       s.warp_max_deg = w;
       s.lane_max_deg = r;
+      s.packed_max_deg = got == 8 ? pk : 0;
       s.chunk = ch;
       s.blocks_per_sm = bp;
       cache().entries[Key{a, b, c}] = s;

@@ -2,9 +2,10 @@
 
 The count kernel intersects each edge at its centre (the endpoint with the larger out-degree
 a): the other endpoint's list N+(o), b <= a entries, goes through the centre's shared-memory
-hash set by one of two strategies: the warp streams it with coalesced loads (one list at a
-time), or one lane walks it (the lanes of a warp walk different short lists at once). The fixed
-heuristic picks by a length threshold (lane_max_deg). Here a 3-layer FP32 MLP of width 64
+hash set by one of three strategies: the warp streams it with coalesced loads (one list at a
+time), one lane walks it (the lanes of a warp walk different short lists at once), or the warp
+walks all such lists of a group of 32 neighbours concatenated (packed). The fixed heuristic
+picks by length thresholds (lane_max_deg, packed_max_deg). Here a 3-layer FP32 MLP of width 64
 predicts the cost per edge of each strategy from the features of the edge's degree cell
 (log2 a, log2 b buckets): mean log2(1 + a), mean log2(1 + b), mean b/a and cell id / 255. The
 cell's choice goes into the scheduler table; the fixed rule stays the fallback for cells where
@@ -77,7 +78,7 @@ def training_specs(quick: bool = False):
 
 
 HELD_OUT = [("rmat", dict(scale=23, a=0.57, seed=23)), ("ba", dict(n_log=22, m0=16, seed=22)),
-            ("rmat", dict(scale=20, a=0.57, seed=2))]
+            ("rmat", dict(scale=20, a=0.57, seed=2)), ("er", dict(n_log=20, deg=32, seed=20))]
 HELD_OUT_QUICK = [("rmat", dict(scale=16, a=0.57, seed=23)), ("ba", dict(n_log=16, m0=16, seed=22))]
 
 
@@ -135,6 +136,16 @@ def cell_features(stats: np.ndarray) -> np.ndarray:
     return feat
 
 
+STRATEGIES = (0, 1, 2)  # static table entries (= network outputs): warp, lane, packed
+
+
+def two_rule_sched():
+    """The fixed rule before packed walks existed: lane walks up to lane_max_deg, else warp."""
+    s = N.default_sched()
+    s.packed_max_deg = 0
+    return s
+
+
 def forced(strategy: int, cell_filter: int = -1):
     s = N.default_sched()
     s.use_table = 1
@@ -173,10 +184,10 @@ def collect_graph(spec, reps: int = 5):
         cnt = stats[c, 0]
         if cnt < MIN_CELL_EDGES:
             continue
-        ts = [count_ms(graph, out, forced(strategy, c), reps)[0] - t_none for strategy in (0, 1)]
+        ts = [count_ms(graph, out, forced(strategy, c), reps)[0] - t_none for strategy in STRATEGIES]
         if min(ts) < MIN_CELL_MS:
             continue  # below the timing resolution: no label
-        for strategy in (0, 1):
+        for strategy in STRATEGIES:
             rows.append((feat[c], strategy, math.log2(ts[strategy] * 1e6 / cnt), c, cnt))
     graph.close()
     return rows, dict(n=g.n, m=g.m, t_none_ms=t_none, cells=int((stats[:, 0] >= MIN_CELL_EDGES).sum()))
@@ -280,23 +291,28 @@ def evaluate_graph(params, spec, reps: int = 5):
     t_fixed, T_fixed = times(None, out_fixed)
     t_learned, T_learned = times(ls, out_learned)
     same = bool(torch.equal(out_fixed, out_learned)) and T_fixed == T_learned
+    t_two, T_two = times(two_rule_sched(), out_learned)
     t_warp, T_warp = times(forced(0), out_learned)
     t_lane, T_lane = times(forced(1), out_learned)
-    same = same and T_warp == T_fixed and T_lane == T_fixed
+    t_pack, T_pack = times(forced(2), out_learned)
+    same = same and T_warp == T_fixed and T_lane == T_fixed and T_pack == T_fixed and T_two == T_fixed
     changed = int(sum(ls.table[c // 16][c % 16] != rule_choice(stats_b[c])
                       for c in range(256) if stats_n[c] > 0))
     graph.close()
     return dict(graph=spec_name(spec), n=g.n, m=g.m, triangles=T_fixed, fixed_ms=round(t_fixed, 4),
                 learned_ms=round(t_learned, 4), gain=round(t_fixed / t_learned, 4),
-                always_warp_ms=round(t_warp, 4), always_lane_ms=round(t_lane, 4), counts_equal=same,
-                cells_with_edges_off_the_rule=changed)
+                two_rule_ms=round(t_two, 4), gain_vs_two_rule=round(t_two / t_learned, 4),
+                always_warp_ms=round(t_warp, 4), always_lane_ms=round(t_lane, 4),
+                always_packed_ms=round(t_pack, 4), counts_equal=same, cells_with_edges_off_the_rule=changed)
 
 
-def rule_choice(mean_b: float, lane_max: int = None) -> int:
+def rule_choice(mean_b: float, lane_max: int = None, packed_max: int = None) -> int:
     """The fixed rule's choice for a cell whose lists have mean length mean_b (reporting only)."""
-    if lane_max is None:
-        lane_max = N.default_sched().lane_max_deg
-    return 1 if round(max(mean_b, 1.0)) <= lane_max else 0
+    d = N.default_sched()
+    lane_max = d.lane_max_deg if lane_max is None else lane_max
+    packed_max = d.packed_max_deg if packed_max is None else packed_max
+    b = round(max(mean_b, 1.0))
+    return 1 if b <= lane_max else 2 if b <= packed_max else 0
 
 
 

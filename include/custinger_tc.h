@@ -68,8 +68,8 @@ typedef struct tc_sched {
   int32_t use_table;      /* 1 = the per-degree-cell strategy table below overrides the rules */
   uint8_t table[16][16];  /* strategy per cell [log2 d_a][log2 d_b]. Static count (a = the centre's
                              out-degree, b = the other endpoint's): 0 = the warp streams N+(b)
-                             through the hash set, 1 = one lane walks it. Streaming: 0 = search,
-                             1 = merge */
+                             through the hash set, 1 = one lane walks it, 2 = packed (see
+                             packed_max_deg). Streaming: 0 = search, 1 = merge */
   int32_t shard;          /* count only the edges whose centre c has c % nshards == shard */
   int32_t nshards;        /* (multi-GPU work split; 1 = everything) */
   int32_t cell_filter;    /* timing mode for scheduler training: -1 = intersect every edge (normal),
@@ -77,6 +77,10 @@ typedef struct tc_sched {
                              counts are partial unless -1 */
   int32_t lane_max_deg;   /* static count rule without a table: lists of at most this many entries
                              are walked by one lane each (several lists per warp step) */
+  int32_t packed_max_deg; /* static count rule without a table: lists longer than lane_max_deg and
+                             of at most this many entries are packed: the warp walks all such lists
+                             of a group of 32 neighbours concatenated, 32 entries per step
+                             (0 = never); longer lists are streamed one at a time */
 } tc_sched;
 
 typedef struct tc_graph tc_graph;

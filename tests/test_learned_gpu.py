@@ -44,7 +44,7 @@ def test_forced_strategies_and_cell_filters_keep_the_count():
     out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
     T_ref, _ = graph.count(N.TC_PV_HANDLE, out)
     ref = out.clone()
-    for strategy in (0, 1):
+    for strategy in L.STRATEGIES:
         T, _ = graph.count(N.TC_PV_HANDLE, out, sched=L.forced(strategy))
         assert T == T_ref and torch.equal(out, ref)
     # the per-cell filters partition the work: their triangle totals add up

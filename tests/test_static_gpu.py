@@ -18,7 +18,13 @@ def _torch():
 def sched(**kw):
     s = N.default_sched()
     for k, v in kw.items():
-        setattr(s, k, v)
+        if k == "table_all":
+            s.use_table = 1
+            for i in range(16):
+                for j in range(16):
+                    s.table[i][j] = v
+        else:
+            setattr(s, k, v)
     return s
 
 
@@ -29,6 +35,9 @@ SCHEDS = {
     "warp2": dict(warp_max_deg=2),
     "warp8_chunk32": dict(warp_max_deg=8, chunk=32),
     "one_block_per_sm": dict(blocks_per_sm=1),
+    "packed_up_to_64": dict(lane_max_deg=4, packed_max_deg=64),
+    "packed_everywhere": dict(table_all=2),
+    "packed_warp2": dict(warp_max_deg=2, lane_max_deg=0, packed_max_deg=1 << 20),
 }
 
 
