@@ -30,6 +30,10 @@ namespace {
 constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
+constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
+constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
+constexpr int64_t kDeltaItems = 1 << 20;  // capacity of the split-item queue
+constexpr unsigned long long kNoItem = ~0ull;
 
 enum : unsigned { kErrRange = 1u, kErrPool = 2u };
 
@@ -47,6 +51,7 @@ struct BatchStatus {
   unsigned long long dir_removed; // directed entries deleted (cuStinger path)
   unsigned long long not_fitting;
   unsigned long long n_long;      // insertion runs whose list is long (CTA kernel)
+  unsigned long long n_split[2];  // split-intersection items queued (deletions, insertions)
   unsigned int err;
   unsigned int pad;
 };
@@ -538,6 +543,9 @@ struct DeltaArgs {
   int only_present;  // skip entries whose edge is absent (cuStinger deletion count)
   int use_table;     // per-cell strategy table: 0 = search, 1 = merge
   int cell_filter;   // -1 all, -2 none, c >= 0 only edges of cell c (timing mode)
+  // split queue: (entry << 24 | chunk) items of long intersections (NULL = no splitting)
+  unsigned long long* split_items;
+  unsigned long long* split_cnt;  // zero before the first pass
   uint8_t table[256];
 };
 
@@ -559,6 +567,102 @@ __device__ __forceinline__ bool changed(const DeltaArgs& A, int32_t owner, int64
   return l < hi && A.bl.dst[l] == w && A.bl.dup[l] == 0;
 }
 
+// Entry e of the changed-edge list: its endpoints and whether it adds to the total (the
+// cuStinger-style batch holds both directions of every edge; the total counts one).
+template <int PRED>
+__device__ __forceinline__ bool delta_entry(const DeltaArgs& A, int64_t e, int32_t& x, int32_t& y, bool& count_total) {
+  count_total = true;
+  if (PRED == kPredMark) {
+    if (A.dlist) {
+      const int4 d = A.dlist[e];
+      x = d.x;
+      y = d.y;
+    } else {
+      const int2 d = A.ilist[e];
+      x = d.x;
+      y = d.y;
+    }
+    return true;
+  }
+  if (A.bl.dup[e]) return false;
+  x = A.bl.src[e];
+  y = A.bl.dst[e];
+  count_total = x < y;
+  return x != y;
+}
+
+// The two lists of edge {x, y} as the intersection takes them: A the shorter, B the longer.
+struct DeltaPair {
+  int32_t oa, ob, la, lb;
+  int64_t sa, sb;
+  uint64_t key;
+  bool search;
+  int cell;
+};
+
+__device__ __forceinline__ DeltaPair delta_pair(const DeltaArgs& A, int32_t x, int32_t y, int32_t lx, int32_t ly,
+                                                int64_t sx, int64_t sy) {
+  DeltaPair P;
+  const bool xs = lx <= ly;
+  P.oa = xs ? x : y;
+  P.ob = xs ? y : x;
+  P.sa = xs ? sx : sy;
+  P.sb = xs ? sy : sx;
+  P.la = xs ? lx : ly;
+  P.lb = xs ? ly : lx;
+  P.key = ekey(x, y);
+  P.cell = cell_of(P.la, P.lb);
+  const int lg = 32 - __clz(P.lb);
+  P.search = A.use_table ? A.table[P.cell] == 0 : 16LL * P.lb > (long long)A.search_ratio_x16 * P.la * lg;
+  return P;
+}
+
+// The warp intersects entries [i_begin, i_end) of the shorter list with the longer one and
+// returns (in every lane) the triangles kept there; each kept common neighbour w gets its
+// per-vertex update here, the endpoints get theirs from the caller.
+template <int PRED>
+__device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaPair& P, int32_t i_begin,
+                                                int32_t i_end, uint32_t* __restrict__ pv) {
+  const int lane = threadIdx.x & 31;
+  const int32_t* L = A.g.ind;
+  uint32_t c = 0;
+  auto on_match = [&](int64_t ia, int64_t ib, int32_t w) {
+    const bool ca = changed<PRED>(A, P.oa, P.sa + ia, w);
+    const bool cb = changed<PRED>(A, P.ob, P.sb + ib, w);
+    const bool keep = (!ca || P.key < ekey(P.oa, w)) && (!cb || P.key < ekey(P.ob, w));
+    if (keep) {
+      ++c;
+      atomicAdd(&pv[w], A.weight * (uint32_t)A.sign);
+    }
+  };
+  const int64_t sb = P.sb, eb = P.sb + P.lb;
+  if (P.search) {
+    for (int32_t i = i_begin + lane; i < i_end; i += 32) {
+      const int32_t w = L[P.sa + i];
+      const int64_t p = lower_bound(L, sb, eb, w);
+      if (p < eb && L[p] == w) on_match(i, p - sb, w);
+    }
+  } else {
+    const int32_t len = i_end - i_begin;
+    const int32_t per = (len + 31) / 32;
+    const int32_t i0 = i_begin + min(len, lane * per), i1 = min(i_end, i0 + per);
+    if (i0 < i1) {
+      int64_t p = lower_bound(L, sb, eb, L[P.sa + i0]);
+      for (int32_t i = i0; i < i1 && p < eb; ++i) {
+        const int32_t w = L[P.sa + i];
+        while (p < eb && L[p] < w) ++p;
+        if (p < eb && L[p] == w) on_match(i, p - sb, w);
+      }
+    }
+  }
+  __syncwarp();
+  return warp_sum(c);
+}
+
+// The triangle delta of the changed edges, one warp per edge. An edge whose shorter list is
+// longer than kDeltaSplit (two hubs) would be one warp's serial tail of the whole launch: when
+// A.split_items is set it is queued instead as items of kDeltaChunk entries of its shorter list,
+// which k_delta_split spreads over all warps (a full queue leaves the edge to this warp).
 template <int PRED>
 __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
                                                     unsigned long long* __restrict__ tri_out) {
@@ -571,24 +675,8 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
   unsigned long long tri_acc = 0;
   for (int64_t e = gw; e < cnt; e += nw) {
     int32_t x, y;
-    bool count_total = true;
-    if (PRED == kPredMark) {
-      if (A.dlist) {
-        const int4 d = A.dlist[e];
-        x = d.x;
-        y = d.y;
-      } else {
-        const int2 d = A.ilist[e];
-        x = d.x;
-        y = d.y;
-      }
-    } else {
-      if (A.bl.dup[e]) continue;
-      x = A.bl.src[e];
-      y = A.bl.dst[e];
-      if (x == y) continue;
-      count_total = x < y;  // symmetric batch: each undirected edge appears in both directions
-    }
+    bool count_total;
+    if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
     const int32_t lx = A.g.len(x), ly = A.g.len(y);
     if (lx < 2 || ly < 2) continue;
     const int64_t sx = A.g.start(x), sy = A.g.start(y);
@@ -602,47 +690,62 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
       __syncwarp();
       if (!__shfl_sync(kFull, pres, 0)) continue;
     }
-    const uint64_t key = ekey(x, y);
-    // A = shorter list, B = longer.
-    const bool xs = lx <= ly;
-    const int32_t oa = xs ? x : y, ob = xs ? y : x;
-    const int64_t sa = xs ? sx : sy, sb = xs ? sy : sx;
-    const int32_t la = xs ? lx : ly, lb = xs ? ly : lx;
-    const int32_t* L = A.g.ind;
-    uint32_t c = 0;
-    auto on_match = [&](int64_t ia, int64_t ib, int32_t w) {
-      const bool ca = changed<PRED>(A, oa, sa + ia, w);
-      const bool cb = changed<PRED>(A, ob, sb + ib, w);
-      const bool keep = (!ca || key < ekey(oa, w)) && (!cb || key < ekey(ob, w));
-      if (keep) {
-        ++c;
-        atomicAdd(&pv[w], A.weight * (uint32_t)A.sign);
-      }
-    };
-    const int cell = cell_of(la, lb);
-    if (A.cell_filter == -2 || (A.cell_filter >= 0 && cell != A.cell_filter)) continue;
-    const int lg = 32 - __clz(lb);
-    const bool search = A.use_table ? A.table[cell] == 0 : 16LL * lb > (long long)A.search_ratio_x16 * la * lg;
-    if (search) {
-      for (int32_t i = lane; i < la; i += 32) {
-        const int32_t w = L[sa + i];
-        const int64_t p = lower_bound(L, sb, sb + lb, w);
-        if (p < sb + lb && L[p] == w) on_match(i, p - sb, w);
-      }
-    } else {
-      const int32_t per = (la + 31) / 32;
-      const int32_t i0 = min(la, lane * per), i1 = min(la, i0 + per);
-      if (i0 < i1) {
-        int64_t p = lower_bound(L, sb, sb + lb, L[sa + i0]);
-        for (int32_t i = i0; i < i1 && p < sb + lb; ++i) {
-          const int32_t w = L[sa + i];
-          while (p < sb + lb && L[p] < w) ++p;
-          if (p < sb + lb && L[p] == w) on_match(i, p - sb, w);
-        }
-      }
+    const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
+    if (A.cell_filter == -2 || (A.cell_filter >= 0 && P.cell != A.cell_filter)) continue;
+    if (A.split_items && P.la > kDeltaSplit) {
+      const int nch = (P.la + kDeltaChunk - 1) / kDeltaChunk;
+      unsigned long long at = 0;
+      if (lane == 0) at = atomicAdd(A.split_cnt, (unsigned long long)nch);
+      at = __shfl_sync(kFull, at, 0);
+      const bool fits = at + (unsigned long long)nch <= (unsigned long long)kDeltaItems;
+      for (int j = lane; j < nch; j += 32)
+        if (at + j < (unsigned long long)kDeltaItems)
+          A.split_items[at + j] = fits ? ((unsigned long long)e << 24) | (unsigned long long)j : kNoItem;
+      if (fits) continue;
     }
-    __syncwarp();
-    c = warp_sum(c);
+    const uint32_t c = delta_range<PRED>(A, P, 0, P.la, pv);
+    if (lane == 0 && c) {
+      atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
+      atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
+      if (count_total) tri_acc += c;
+    }
+  }
+  if (lane == 0) s_tri[wid] = tri_acc;
+  __syncwarp();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long s = 0;
+    for (int w = 0; w < kThreads / 32; ++w) s += s_tri[w];
+    if (s) atomicAdd(tri_out, s);
+  }
+}
+
+// The queued chunks of the split intersections, one warp per item. An item's edge passed every
+// check of k_delta already; its endpoints' per-vertex updates and the total add up per chunk.
+template <int PRED>
+__global__ void __launch_bounds__(kThreads) k_delta_split(const DeltaArgs A, uint32_t* __restrict__ pv,
+                                                          unsigned long long* __restrict__ tri_out) {
+  __shared__ unsigned long long s_tri[kThreads / 32];
+  const int lane = threadIdx.x & 31;
+  const int wid = threadIdx.x >> 5;
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t cnt = (int64_t)min(*A.split_cnt, (unsigned long long)kDeltaItems);
+  unsigned long long tri_acc = 0;
+  for (int64_t q = gw; q < cnt; q += nw) {
+    const unsigned long long item = A.split_items[q];
+    if (item == kNoItem) continue;
+    const int64_t e = (int64_t)(item >> 24);
+    const int32_t k = (int32_t)(item & 0xffffffu);
+    int32_t x, y;
+    bool count_total;
+    if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
+    const int32_t lx = A.g.len(x), ly = A.g.len(y);
+    const int64_t sx = A.g.start(x), sy = A.g.start(y);
+    const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
+    const int32_t i0 = k * kDeltaChunk;
+    if (i0 >= P.la) continue;
+    const uint32_t c = delta_range<PRED>(A, P, i0, min(P.la, i0 + kDeltaChunk), pv);
     if (lane == 0 && c) {
       atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
       atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
@@ -799,6 +902,7 @@ struct StreamWs {
   int32_t* cnt = nullptr;       // [n+1] per-source counts (cuStinger sort)
   int64_t* scan64 = nullptr;    // [n+1]
   int64_t* tiles = nullptr;
+  unsigned long long* split_items = nullptr;  // [kDeltaItems] queued chunks of long intersections
   void release();
 };
 
@@ -807,7 +911,7 @@ void StreamWs::release() {
   cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(long_runs);
   cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
-  cudaFree(cnt); cudaFree(scan64); cudaFree(tiles);
+  cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
   *this = StreamWs();
 }
 
@@ -842,6 +946,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     TC_CUDA_TRY(cudaMalloc(&w.st, sizeof(BatchStatus)));
     TC_CUDA_TRY(cudaMallocHost(&w.st_host, sizeof(BatchStatus)));
     TC_CUDA_TRY(cudaMalloc(&w.counter, sizeof(unsigned long long)));
+    TC_CUDA_TRY(cudaMalloc(&w.split_items, sizeof(unsigned long long) * kDeltaItems));
   }
   if (b <= w.b_cap) return TC_OK;
   const int64_t nb = std::max<int64_t>(b, 1024);
@@ -991,7 +1096,10 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.count_dev = &w.st->n_del;
     A.sign = -1;
     A.weight = 2;
+    A.split_items = w.split_items;
+    A.split_cnt = &w.st->n_split[0];
     k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
+    k_delta_split<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
     k_endpoints<<<gd, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
@@ -1013,7 +1121,10 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.count_dev = &w.st->n_ins;
     A.sign = 1;
     A.weight = 2;
+    A.split_items = w.split_items;
+    A.split_cnt = &w.st->n_split[1];
     k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
+    k_delta_split<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
     k_clear_slots<<<grid_for(2 * (int64_t)h.n_ins, kThreads), kThreads, 0, s>>>(w.ins_slot, 2 * (int64_t)h.n_ins,
                                                                                   nullptr, g->mark);
     TC_CUDA_TRY(cudaGetLastError());
@@ -1170,7 +1281,12 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
     A.sign = sign;
     A.weight = 1;
     A.only_present = sign < 0;
+    A.split_items = w.split_items;
+    A.split_cnt = &w.st->n_split[0];
+    TC_CUDA_TRY(cudaMemsetAsync(A.split_cnt, 0, sizeof(unsigned long long), s));
     k_delta<kPredBatch><<<delta_grid(), kThreads, 0, s>>>(A, reinterpret_cast<uint32_t*>(per_vertex), w.counter);
+    k_delta_split<kPredBatch><<<delta_grid(), kThreads, 0, s>>>(A, reinterpret_cast<uint32_t*>(per_vertex),
+                                                                 w.counter);
     TC_CUDA_TRY(cudaGetLastError());
   }
   if (delta_dev) {
@@ -1347,7 +1463,10 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.count_dev = &w.st->n_del;
     A.sign = -1;
     A.weight = 2;
+    A.split_items = w.split_items;
+    A.split_cnt = &w.st->n_split[0];
     k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
+    k_delta_split<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
     k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
@@ -1365,7 +1484,10 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     B.count_dev = &w.st->n_ins;
     B.sign = 1;
     B.weight = 2;
+    B.split_items = w.split_items;
+    B.split_cnt = &w.st->n_split[1];
     k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
+    k_delta_split<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
     k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);
     k_add_delta<<<1, 32, 0, s>>>(delta, &w.st->tri_added, &w.st->tri_removed);
     cudaMemcpyAsync(p->h_st, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s);

@@ -179,3 +179,66 @@ def test_custinger_path_long_lists_round_trip():
     N.check(N.lib().tc_delete_sorted(graph.handle, ds.data_ptr(), dd.data_ptr(), dup.data_ptr(), s.size, None))
     o2, i2 = graph.export()
     assert np.array_equal(o2, base.off) and np.array_equal(i2, base.ind)
+
+
+def _hub_graph(rng, n, hubs, per_hub, pool_size, extra):
+    """Hubs 0 .. hubs-1, each adjacent to per_hub vertices of one shared pool (so two hubs share
+    most of their neighbours and every hub-hub edge closes thousands of triangles), plus random
+    edges."""
+    pool = rng.choice(np.arange(hubs, n), pool_size, replace=False).astype(np.int32)
+    src, dst = [], []
+    for h in range(hubs):
+        nb = rng.choice(pool, per_hub, replace=False)
+        src.append(np.full(per_hub, h, np.int32))
+        dst.append(nb)
+    src.append(rng.integers(0, n, extra).astype(np.int32))
+    dst.append(rng.integers(0, n, extra).astype(np.int32))
+    return G.from_pairs(n, np.concatenate(src), np.concatenate(dst))
+
+
+@pytest.mark.parametrize("path", ["pipeline", "apply"])
+def test_split_intersections_between_hubs(path):
+    """Edges whose both lists exceed 2048 entries are split into queued chunks (k_delta_split):
+    inserting and deleting hub-hub edges must still give the recount, total and per vertex."""
+    torch = _torch()
+    rng = np.random.default_rng(77)
+    n, hubs = 16000, 6
+    base = _hub_graph(rng, n, hubs, 6000, 8000, 30000)
+    assert np.sort(np.diff(base.off))[-hubs] > 2048
+    graph = api.Graph.from_csr(base, slack=0.25)
+    T0, pv0 = _recount(graph, n)
+    pipe = api.Pipeline(graph, 1 << 14) if path == "pipeline" else None
+    pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cur = base
+    es = edge_set(base)
+    hub_pairs = [(a, b) for a in range(hubs) for b in range(a + 1, hubs)]
+    for it in range(4):
+        k = 4000
+        s = rng.integers(0, n, k).astype(np.int32)
+        d = rng.integers(0, n, k).astype(np.int32)
+        x = np.zeros(k, np.uint8)
+        # hub-hub edges: insert the absent ones, delete the present ones (both lists > 2048)
+        for j, (a, b) in enumerate(hub_pairs):
+            s[j], d[j] = (a, b) if j % 2 else (b, a)
+            x[j] = 1 if (min(a, b), max(a, b)) in es else 0
+        # hub - pool edges on both sides of the attribution rule
+        m = len(hub_pairs)
+        s[m:m + 500] = rng.integers(0, hubs, 500)
+        d[m:m + 500] = rng.integers(hubs, n, 500)
+        ts, td, tx = _dev(torch, s, d, x)
+        if pipe is not None:
+            pipe.apply(ts, td, tx, per_vertex=pv, delta_dev=delta)
+            pipe.sync()
+        else:
+            graph.apply_batch(ts, td, tx, per_vertex=pv, delta_dev=delta)
+        want = expected_after(n, es, s, d, x)
+        off, ind = graph.export()
+        assert np.array_equal(off, want.off) and np.array_equal(ind, want.ind)
+        cur = G.Csr(n, off, ind)
+        es = edge_set(cur)
+        T, pvn = _recount(graph, n)
+        assert T == T0 + int(delta.item())
+        assert torch.equal(pvn, (pv0.to(torch.int64) + pv[:n].to(torch.int64)).to(torch.int32))
+    if pipe is not None:
+        pipe.close()

@@ -204,3 +204,44 @@ def test_custinger_path_matches_reference_kernels(seed):
     o3, i3 = graph.export()
     assert np.array_equal(o3, base.off) and np.array_equal(i3, base.ind)
     assert np.array_equal(pv2[:n].cpu().numpy(), (-want.astype(np.int64)).astype(np.int32))
+
+
+def test_custinger_path_splits_hub_hub_intersections():
+    """callDeviceNewTriangles on hub-hub edges (both lists > 2048, counted in queued chunks)
+    equals the reference's K1 + K2 - K3 on the oracle, per vertex; the deletion count of the same
+    edges gives the negative."""
+    torch = _torch()
+    rng = np.random.default_rng(91)
+    n, hubs = 9000, 4
+    pool = rng.choice(np.arange(hubs, n), 4000, replace=False).astype(np.int32)
+    src = np.concatenate([np.full(3000, h, np.int32) for h in range(hubs)] + [rng.integers(0, n, 8000).astype(np.int32)])
+    dst = np.concatenate([rng.choice(pool, 3000, replace=False) for _ in range(hubs)] +
+                         [rng.integers(0, n, 8000).astype(np.int32)])
+    base = G.from_pairs(n, src, dst)
+    pairs = np.array([(a, b) for a in range(hubs) for b in range(a + 1, hubs)], np.int32)
+    s = np.concatenate([pairs[:, 0], rng.integers(0, n, 50).astype(np.int32)])
+    d = np.concatenate([pairs[:, 1], rng.integers(0, n, 50).astype(np.int32)])
+    bs = np.concatenate([s, d]).astype(np.int32)
+    bd = np.concatenate([d, s]).astype(np.int32)
+    graph = api.Graph.from_csr(base, slack=0.5)
+    ds, dd, off, dup = _cus_batch(n, bs, bd, graph)
+    ss, sd, boff, odup = O.sort_batch(n, base.off, base.ind, bs, bd)
+    N.check(N.lib().tc_insert_sorted(graph.handle, ds.data_ptr(), dd.data_ptr(), bs.size, dup.data_ptr(), None, None))
+    after = G.from_pairs(n, np.concatenate([np.repeat(np.arange(n, dtype=np.int32), np.diff(base.off)), ss]),
+                         np.concatenate([base.ind, sd]))
+    assert min(np.diff(after.off)[:hubs]) > 2048
+    pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
+                                   bs.size, 1, pv.data_ptr(), delta.data_ptr(), None, None))
+    want = O.new_triangles(n, after.off, after.ind, ss, sd, boff, odup)
+    assert np.array_equal(pv[:n].cpu().numpy(), want)
+    t_after = O.host_count_triangles(n, after.off, after.ind)[0] // 6
+    t_base = O.host_count_triangles(n, base.off, base.ind)[0] // 6
+    assert int(delta.item()) == t_after - t_base > 0
+    pv2 = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    delta2 = torch.zeros(1, dtype=torch.int64, device="cuda")
+    N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
+                                   bs.size, -1, pv2.data_ptr(), delta2.data_ptr(), None, None))
+    assert np.array_equal(pv2[:n].cpu().numpy(), -want)
+    assert int(delta2.item()) == -(t_after - t_base)
