@@ -30,6 +30,7 @@ namespace {
 constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
+constexpr int kRunStage = 4096;  // new entries of one long list staged in shared memory
 constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
 constexpr int64_t kDeltaItems = 1 << 20;  // capacity of the split-item queue
@@ -371,6 +372,7 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
   __shared__ int64_t sh_i1, sh_new;
   __shared__ int32_t sh_nc;
   __shared__ int sh_state;  // 0 in place, 1 moved, 2 pool exhausted
+  __shared__ int32_t sh_run[kRunStage];
   const int64_t nlong = (int64_t)st->n_long;
   for (int64_t r = blockIdx.x; r < nlong; r += gridDim.x) {
     const int64_t i0 = long_runs[r];
@@ -414,8 +416,12 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
       continue;
     }
     const int32_t* A = pool + s_old;
+    // the run's new entries, staged in shared memory when they fit (the existing entries each
+    // look up how many new ones sort before them)
+    const bool staged = c <= kRunStage;
     for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) {
       const int32_t val = (int32_t)(uint32_t)dk[j];
+      if (staged) sh_run[j - i0] = val;
       int32_t lo = 0, hi = a;
       while (lo < hi) {
         const int32_t mid = (lo + hi) >> 1;
@@ -425,24 +431,38 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
       slot[j] = (j - i0) + lo;
     }
     __syncthreads();
-    for (int32_t base = ((a - 1) / kThreads) * kThreads; base >= 0 && a > 0; base -= kThreads) {
-      const int32_t i = base + (int32_t)threadIdx.x;
-      int32_t val = 0;
-      int64_t pos = 0;
-      if (i < a) {
-        val = A[i];
-        int64_t lo = i0, hi = i1;
-        while (lo < hi) {
-          const int64_t mid = (lo + hi) >> 1;
-          if ((int32_t)(uint32_t)dk[mid] < val) lo = mid + 1;
-          else hi = mid;
+    // Existing entries move up by the number of new entries below them, from the list's end
+    // down, kInsPer per thread per step: a step reads all its entries before any is written,
+    // and its targets lie at or above its own start, where every entry was read already.
+    constexpr int kInsPer = 4;
+    constexpr int kStep = kThreads * kInsPer;
+    for (int32_t base = ((a - 1) / kStep) * kStep; base >= 0 && a > 0; base -= kStep) {
+      int32_t val[kInsPer];
+      int64_t pos[kInsPer];
+#pragma unroll
+      for (int q = 0; q < kInsPer; ++q) {
+        const int32_t i = base + q * kThreads + (int32_t)threadIdx.x;
+        val[q] = 0;
+        pos[q] = -1;
+        if (i < a) {
+          val[q] = A[i];
+          int32_t lo = 0, hi = c;
+          while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            const int32_t x = staged ? sh_run[mid] : (int32_t)(uint32_t)dk[i0 + mid];
+            if (x < val[q]) lo = mid + 1;
+            else hi = mid;
+          }
+          pos[q] = i + lo;
         }
-        pos = i + (lo - i0);
       }
       __syncthreads();
-      if (i < a) {
-        pool[s_new + pos] = val;
-        if (mark) mark[s_new + pos] = 0;
+#pragma unroll
+      for (int q = 0; q < kInsPer; ++q) {
+        if (pos[q] >= 0) {
+          pool[s_new + pos[q]] = val[q];
+          if (mark) mark[s_new + pos[q]] = 0;
+        }
       }
       __syncthreads();
     }
@@ -489,12 +509,29 @@ __global__ void __launch_bounds__(kThreads) k_compact_long(
     if (old >= epoch) continue;
     const int64_t s = start[v];
     int32_t wp = 0;
-    for (int32_t base = 0; base < a; base += kThreads) {
-      const int32_t i = base + (int32_t)threadIdx.x;
-      const bool keep = i < a && mark[s + i] == 0;
-      const int32_t val = keep ? pool[s + i] : 0;
-      const unsigned m = __ballot_sync(0xffffffffu, keep);
-      if (lane == 0) sh_wsum[wid] = __popc(m);
+    // kCmpPer consecutive entries per thread per step; a step reads all its entries before the
+    // barrier, and its targets lie below the next step's start (targets never pass sources)
+    constexpr int kCmpPer = 4;
+    for (int32_t base = 0; base < a; base += kThreads * kCmpPer) {
+      const int32_t i0 = base + (int32_t)threadIdx.x * kCmpPer;
+      int32_t val[kCmpPer];
+      int kept = 0;
+      unsigned keepm = 0;
+#pragma unroll
+      for (int q = 0; q < kCmpPer; ++q) {
+        const int32_t i = i0 + q;
+        const bool keep = i < a && mark[s + i] == 0;
+        val[q] = keep ? pool[s + i] : 0;
+        keepm |= (unsigned)keep << q;
+        kept += keep;
+      }
+      int incl = kept;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane == 31) sh_wsum[wid] = incl;
       __syncthreads();
       int32_t before = 0, total = 0;
       for (int w = 0; w < kThreads / 32; ++w) {
@@ -502,9 +539,10 @@ __global__ void __launch_bounds__(kThreads) k_compact_long(
         if (w < wid) before += x;
         total += x;
       }
-      const int32_t at = wp + before + __popc(m & ((1u << lane) - 1u));
-      __syncthreads();
-      if (keep) pool[s + at] = val;
+      int32_t at = wp + before + incl - kept;
+#pragma unroll
+      for (int q = 0; q < kCmpPer; ++q)
+        if (keepm >> q & 1u) pool[s + at++] = val[q];
       wp += total;
       __syncthreads();
     }
