@@ -165,7 +165,7 @@ tc_status count_csr(int32_t nv, const OffT* d_off, const int32_t* d_ind, int pv_
     return fail(TC_ERR_INVALID_ARG, "invalid CSR (nv=%d)", nv);
   if (pv_mode != TC_PV_NONE && nv > 0 && !per_vertex)
     return fail(TC_ERR_INVALID_ARG, "per_vertex output required for mode %d", pv_mode);
-  if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_CSR) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
+  if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_HANDLE64) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
   cudaStream_t s = (cudaStream_t)stream;
   int dev = 0;
   TC_CUDA_TRY(cudaGetDevice(&dev));

@@ -84,7 +84,7 @@ extern "C" tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, co
                                             int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
                                             const tc_sched* sched, void* stream) {
   if (nv < 0 || (nv > 0 && (!d_off || !d_ind))) return fail(TC_ERR_INVALID_ARG, "invalid CSR (nv=%d)", nv);
-  if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_CSR) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
+  if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_HANDLE64) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
   if (pv_mode != TC_PV_NONE && nv > 0 && !per_vertex)
     return fail(TC_ERR_INVALID_ARG, "per_vertex output required for mode %d", pv_mode);
   if ((int64_t)nv > kMaxNv)

@@ -198,7 +198,23 @@ __device__ __forceinline__ void tri_weights(int32_t u, int32_t v, int32_t w, uin
 
 template <int PV>
 __host__ __device__ constexpr uint32_t flush_mult() {
-  return PV == TC_PV_HANDLE ? 2u : 1u;
+  return PV == TC_PV_HANDLE || PV == TC_PV_HANDLE64 ? 2u : 1u;
+}
+
+// Handle conventions (every triangle weighs 1 per vertex, doubled at flush): int32 or int64 output.
+template <int PV>
+__host__ __device__ constexpr bool handle_like() {
+  return PV == TC_PV_HANDLE || PV == TC_PV_HANDLE64;
+}
+
+// Flush x triangles (weights) of vertex v into the per-vertex output: int32 entries, or int64
+// entries for TC_PV_HANDLE64 (the output pointer then addresses int64[nv]).
+template <int PV>
+__device__ __forceinline__ void out_add(uint32_t* __restrict__ out, const int32_t v, const uint32_t x) {
+  if (PV == TC_PV_HANDLE64)
+    atomicAdd(reinterpret_cast<unsigned long long*>(out) + v, (unsigned long long)x * flush_mult<PV>());
+  else
+    atomicAdd(out + v, x * flush_mult<PV>());
 }
 
 // Is the edge {c, o} intersected at c? At the endpoint with the larger out-degree (its list is
@@ -225,7 +241,7 @@ __device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c
   const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
                     : hash_find_after(hkeys, bits, key, bk);
   if (s < 0) return 0;
-  if (PV == TC_PV_HANDLE) {
+  if (handle_like<PV>()) {
     atomicAdd(&cnt[s], 1u);
   } else if (PV == TC_PV_CSR) {
     uint32_t wc, wo, ww;
@@ -266,7 +282,7 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, 
                           : hash_find_after(hkeys, bits, key, bk);
         if (s >= 0) {
           ++hits;
-          if (PV == TC_PV_HANDLE) {
+          if (handle_like<PV>()) {
             atomicAdd(&cnt[s], 1u);
           } else if (PV == TC_PV_CSR) {
             uint32_t wc, wo, ww;
@@ -338,11 +354,11 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
       uint32_t vacc = 0;
       const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
       tri += hits;
-      if (PV == TC_PV_HANDLE) {
+      if (handle_like<PV>()) {
         c_acc += hits;
         vacc = hits;
       }
-      if (PV != TC_PV_NONE && vacc) atomicAdd(&out[o], vacc * flush_mult<PV>());
+      if (PV != TC_PV_NONE && vacc) out_add<PV>(out, o, vacc);
     }
     __syncwarp();
   }
@@ -372,7 +388,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
       uint32_t vw = 0;  // o's weight of this entry's triangle
       const uint32_t h = key >= 0 ? probe_one<PV>(key, c, po, hkeys, bits, cnt, c_acc, vw) : 0u;
       tri += h;
-      if (PV == TC_PV_HANDLE) {
+      if (handle_like<PV>()) {
         c_acc += h;
         vw = h;
       }
@@ -386,7 +402,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
           const unsigned above = heads & ~((2u << lane) - 1u);  // heads of later lanes (lane 31: none)
           const unsigned seg = (above ? (1u << (__ffs(above) - 1)) - 1u : ~0u) & ~((1u << lane) - 1u);
           const uint32_t sum = __popc(w0 & seg) + 2u * __popc(w1 & seg);
-          if (sum) atomicAdd(&out[po], sum * flush_mult<PV>());
+          if (sum) out_add<PV>(out, po, sum);
         }
       }
     }
@@ -402,13 +418,13 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     uint32_t vacc = 0;
     const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
     tri += hits;
-    if (PV == TC_PV_HANDLE) {
+    if (handle_like<PV>()) {
       c_acc += hits;
       vacc = hits;
     }
     if (PV != TC_PV_NONE) {
       vacc = __reduce_add_sync(kFull, vacc);
-      if (lane == 0 && vacc) atomicAdd(&out[so], vacc * flush_mult<PV>());
+      if (lane == 0 && vacc) out_add<PV>(out, so, vacc);
     }
   }
   __syncwarp();
@@ -441,11 +457,11 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
   if (PV != TC_PV_NONE) {
     for (int s = lane; s < S; s += kWarp) {
       const uint32_t x = t.cnt[s];
-      if (x) atomicAdd(&out[t.hkeys[s]], x * flush_mult<PV>());
+      if (x) out_add<PV>(out, t.hkeys[s], x);
     }
     __syncwarp();
     c_acc = __reduce_add_sync(kFull, c_acc);
-    if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
+    if (lane == 0 && c_acc) out_add<PV>(out, c, c_acc);
   }
   __syncwarp();
 }
@@ -526,7 +542,7 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
       if (PV != TC_PV_NONE) {
         for (int s = threadIdx.x; s < S; s += kThreads) {
           const uint32_t x = L.cnt[s];
-          if (x) atomicAdd(&out[L.hkeys[s]], x * flush_mult<PV>());
+          if (x) out_add<PV>(out, L.hkeys[s], x);
         }
       }
       __syncwarp();
@@ -534,7 +550,7 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
     }
     if (PV != TC_PV_NONE) {
       c_acc = __reduce_add_sync(kFull, c_acc);
-      if (lane == 0 && c_acc) atomicAdd(&out[c], c_acc * flush_mult<PV>());
+      if (lane == 0 && c_acc) out_add<PV>(out, c, c_acc);
     }
   }
 
@@ -1207,7 +1223,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
                        int64_t* triangles_dev, const SchedParams& sp, cudaStream_t stream) {
   TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
   if (pv_mode != TC_PV_NONE && n > 0)
-    TC_CUDA_TRY(cudaMemsetAsync(per_vertex, 0, sizeof(int32_t) * (size_t)n, stream));
+    TC_CUDA_TRY(cudaMemsetAsync(per_vertex, 0, (pv_mode == TC_PV_HANDLE64 ? 8 : 4) * (size_t)n, stream));
   if (n > 0) {
     prof_mark(0, stream);
     TC_TRY(orient(view, n, ws, sp, true, stream));
@@ -1217,6 +1233,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
       case TC_PV_NONE: TC_TRY(launch_count<TC_PV_NONE>(n, view.ind, ws, out, sp, stream)); break;
       case TC_PV_HANDLE: TC_TRY(launch_count<TC_PV_HANDLE>(n, view.ind, ws, out, sp, stream)); break;
       case TC_PV_CSR: TC_TRY(launch_count<TC_PV_CSR>(n, view.ind, ws, out, sp, stream)); break;
+      case TC_PV_HANDLE64: TC_TRY(launch_count<TC_PV_HANDLE64>(n, view.ind, ws, out, sp, stream)); break;
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);

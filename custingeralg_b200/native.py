@@ -32,6 +32,7 @@ NOALLOC_MAX_EDGES = 1 << 22
 TC_PV_NONE = 0
 TC_PV_HANDLE = 1
 TC_PV_CSR = 2
+TC_PV_HANDLE64 = 3
 
 TC_MEM_DEVICE = 0
 TC_MEM_HOST = 1

@@ -49,8 +49,10 @@ enum {
   TC_ERR_STATE = 8          /* call out of order (e.g. counting a batch that was not applied) */
 };
 
-/* Per-vertex output conventions. */
-enum { TC_PV_NONE = 0, TC_PV_HANDLE = 1, TC_PV_CSR = 2 };
+/* Per-vertex output conventions. TC_PV_HANDLE64 is TC_PV_HANDLE (2 t(v)) into int64 entries,
+ * which do not wrap where 2 t(v) passes 2^31 (R-MAT 24 hubs): the per_vertex argument then
+ * points to int64_t[nv] (cast to int32_t*). No reference counterpart: its outputs are int32. */
+enum { TC_PV_NONE = 0, TC_PV_HANDLE = 1, TC_PV_CSR = 2, TC_PV_HANDLE64 = 3 };
 
 /* Memory space of caller pointers. */
 enum { TC_MEM_DEVICE = 0, TC_MEM_HOST = 1 };

@@ -191,3 +191,23 @@ def test_shards_sum_to_full(nshards):
         acc += out
     assert total == rec["triangles"]
     assert digest(acc[: g.n].cpu().numpy()) == rec["per_vertex_handle_digest"]
+
+
+@pytest.mark.parametrize("name", ["rmat12_ef16_s2", "K70", "ba4096_m8_s1"])
+def test_int64_per_vertex_mode(name):
+    """TC_PV_HANDLE64 writes 2 t(v) into int64 entries (no wrap): the oracle's per-vertex counts,
+    through the handle and through the raw-CSR entry point; entry nv stays untouched."""
+    torch = _torch()
+    g = golden_graph(name)
+    _, want = O.fast_count(g.n, g.off, g.ind)
+    graph = api.Graph.from_csr(g)
+    out = torch.full((g.n + 1,), -7, dtype=torch.int64, device="cuda")
+    T, _ = graph.count(N.TC_PV_HANDLE64, out)
+    assert T == GOLD[name]["triangles"]
+    assert np.array_equal(out[: g.n].cpu().numpy(), want.astype(np.int64))
+    assert int(out[g.n].item()) == -7
+    d_off = torch.from_numpy(g.off.astype(np.int32)).cuda()
+    d_ind = torch.from_numpy(g.ind).cuda()
+    out2 = torch.zeros(g.n, dtype=torch.int64, device="cuda")
+    T2, _ = api.count_all_triangles_csr(g.n, d_off, d_ind, out2, pv_mode=N.TC_PV_HANDLE64)
+    assert T2 == T and torch.equal(out2, out[: g.n])
