@@ -74,6 +74,9 @@ class cuStinger {
   cuStinger(const cuStinger& other);
   cuStinger& operator=(const cuStinger&) = delete;
 
+  // Vertex count, readable on the device copy (devicePtr()) by traversal kernels.
+  CUS_HD length_t getMaxNV() const { return nv; }
+
   void initializeCuStinger(cuStingerInitConfig& cfg);
   void freecuStinger();
 

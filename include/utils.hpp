@@ -1,12 +1,15 @@
-// utils.hpp - the graph readers and event timers the reference drivers take from the cuStinger
-// core (tests/cct.cpp:9, 239-257, 189-201), which is absent from the reference tree. The readers
-// live in libtcgen.so (custingeralg_b200/csrc/tcgen_io.cpp) and return the symmetric, sorted,
+// utils.hpp - the graph readers, event timers and array helpers the reference drivers and
+// algorithms take from the cuStinger core (tests/cct.cpp:9, 239-257, 189-201;
+// src/static_breadth_first_search/bfs_top_down.cu:26-31), which is absent from the reference
+// tree. The readers live in libtcgen.so (custingeralg_b200/csrc/tcgen_io.cpp) and return the symmetric, sorted,
 // deduplicated CSR without self-loops in malloc'd arrays the caller frees with free().
 #ifndef CUSTINGER_UTILS_HPP_
 #define CUSTINGER_UTILS_HPP_
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
+#include <cstdlib>
 #include <iostream>
 #include <string>
 
@@ -40,6 +43,34 @@ inline float end_clock(cudaEvent_t& start, cudaEvent_t& stop) {
   cudaEventDestroy(start);
   cudaEventDestroy(stop);
   return ms;
+}
+
+// Array helpers of the cuStinger core that algorithms and the operator library call
+// (allocDeviceArray(hostBfsData.nv, sizeof(vertexId_t)), copyArrayHostToDevice(&host, dev, 1,
+// sizeof(T)), ...: source first, destination second, then element count and size). Blocking
+// copies on the default stream; a failed CUDA call is reported on stderr.
+inline void cus_report(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) fprintf(stderr, "%s: %s\n", what, cudaGetErrorString(e));
+}
+inline void* allocDeviceArray(length_t elements, int32_t eleSize) {
+  void* p = nullptr;
+  cus_report(cudaMalloc(&p, (size_t)elements * (size_t)eleSize), "allocDeviceArray");
+  return p;
+}
+inline void freeDeviceArray(void* p) { cus_report(cudaFree(p), "freeDeviceArray"); }
+inline void* allocHostArray(length_t elements, int32_t eleSize) { return malloc((size_t)elements * (size_t)eleSize); }
+inline void freeHostArray(void* p) { free(p); }
+inline void copyArrayHostToDevice(const void* hostSrc, void* devDst, length_t elements, int32_t eleSize) {
+  cus_report(cudaMemcpy(devDst, hostSrc, (size_t)elements * (size_t)eleSize, cudaMemcpyHostToDevice),
+             "copyArrayHostToDevice");
+}
+inline void copyArrayDeviceToHost(const void* devSrc, void* hostDst, length_t elements, int32_t eleSize) {
+  cus_report(cudaMemcpy(hostDst, devSrc, (size_t)elements * (size_t)eleSize, cudaMemcpyDeviceToHost),
+             "copyArrayDeviceToHost");
+}
+inline void copyArrayDeviceToDevice(const void* devSrc, void* devDst, length_t elements, int32_t eleSize) {
+  cus_report(cudaMemcpy(devDst, devSrc, (size_t)elements * (size_t)eleSize, cudaMemcpyDeviceToDevice),
+             "copyArrayDeviceToDevice");
 }
 
 #endif
