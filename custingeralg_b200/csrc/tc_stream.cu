@@ -1057,7 +1057,7 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
 }
 
 int delta_grid() { return device_info().sms * 8; }
-int long_grid() { return device_info().sms * 2; }
+int long_grid() { return device_info().sms * 8; }
 
 }  // namespace
 }  // namespace tc
