@@ -675,10 +675,27 @@ __device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaP
   };
   const int64_t sb = P.sb, eb = P.sb + P.lb;
   if (P.search) {
-    for (int32_t i = i_begin + lane; i < i_end; i += 32) {
-      const int32_t w = L[P.sa + i];
-      const int64_t p = lower_bound(L, sb, eb, w);
-      if (p < eb && L[p] == w) on_match(i, p - sb, w);
+    // The first five search levels come from 32 evenly spaced samples of the longer list, one
+    // per lane (a single coalesced load): a lane counts the samples below its key with
+    // shuffles, then searches memory only inside that bucket.
+    const int64_t step = ((int64_t)P.lb + 31) / 32;
+    const int32_t smp = (int64_t)lane * step < P.lb ? L[sb + (int64_t)lane * step] : INT32_MAX;
+    const int32_t s31 = __shfl_sync(kFull, smp, 31);
+    for (int32_t base = i_begin; base < i_end; base += 32) {
+      const int32_t i = base + lane;
+      const bool in = i < i_end;
+      const int32_t w = in ? L[P.sa + i] : INT32_MAX;
+      int pos = 0;  // samples below w (they ascend with the lane)
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1)
+        if (__shfl_sync(kFull, smp, pos + st - 1) < w) pos += st;
+      if (pos == 31 && s31 < w) pos = 32;
+      if (in) {
+        const int64_t lo = pos > 0 ? (int64_t)(pos - 1) * step + 1 : 0;
+        const int64_t hi = pos < 32 ? min((int64_t)pos * step, (int64_t)P.lb) : (int64_t)P.lb;
+        const int64_t p = lower_bound(L, sb + lo, sb + hi, w);
+        if (p < eb && L[p] == w) on_match(i, p - sb, w);
+      }
     }
   } else {
     const int32_t len = i_end - i_begin;
@@ -702,7 +719,7 @@ __device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaP
 // A.split_items is set it is queued instead as items of kDeltaChunk entries of its shorter list,
 // which k_delta_split spreads over all warps (a full queue leaves the edge to this warp).
 template <int PRED>
-__global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
+__global__ void __launch_bounds__(kThreads, 6) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
                                                     unsigned long long* __restrict__ tri_out) {
   __shared__ unsigned long long s_tri[kThreads / 32];
   const int lane = threadIdx.x & 31;
@@ -761,7 +778,7 @@ __global__ void __launch_bounds__(kThreads) k_delta(const DeltaArgs A, uint32_t*
 // The queued chunks of the split intersections, one warp per item. An item's edge passed every
 // check of k_delta already; its endpoints' per-vertex updates and the total add up per chunk.
 template <int PRED>
-__global__ void __launch_bounds__(kThreads) k_delta_split(const DeltaArgs A, uint32_t* __restrict__ pv,
+__global__ void __launch_bounds__(kThreads, 6) k_delta_split(const DeltaArgs A, uint32_t* __restrict__ pv,
                                                           unsigned long long* __restrict__ tri_out) {
   __shared__ unsigned long long s_tri[kThreads / 32];
   const int lane = threadIdx.x & 31;
