@@ -28,9 +28,10 @@
 //       warp  1 <= a <= warp_max (at most 128): one warp per centre (items of 256 neighbours for
 //             centres with more), a warp-private set of up to 256 slots.
 //     CTAs of 4 warps, 12 resident per SM (40 registers, 16 KB of shared memory each).
-//     Per edge, the warp streams N+(o) with coalesced loads (four per lane in flight), or, for
-//     short lists, one lane walks it while the other lanes walk theirs; the scheduler
-//     (threshold or learned per-degree-cell table) picks.
+//     Per edge, the warp streams N+(o) with coalesced loads (four per lane in flight); or, for
+//     short lists, one lane walks it while the other lanes walk theirs; or, for mid-size lists,
+//     the warp walks all such lists of its group of neighbours concatenated (packed); the
+//     scheduler (thresholds or learned per-degree-cell table) picks.
 //  3. Attribution. Per-vertex counts never take a global atomic per triangle: the centre's count
 //     stays in registers, the other endpoint's is reduced once per list (one redux.sync), and
 //     the third vertex's is a shared-memory counter beside the hash slot that the probe found;
