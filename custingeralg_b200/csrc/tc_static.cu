@@ -1238,7 +1238,7 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);
-    prof_launches(3);
+    prof_launches(5);  // k_find_hubs, k_orient, k_push_items, k_fill_items, k_count
   }
   (void)m;
   if (triangles_dev)
