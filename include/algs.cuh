@@ -39,6 +39,10 @@ class Queue {
   Queue() {}
   explicit Queue(length_t length) { Init(length); }
   ~Queue() { release(); }
+  // The queue owns its device arrays: no C++ copies (algorithms move it to the device and back
+  // as plain bytes, inside their metadata structs).
+  Queue(const Queue&) = delete;
+  Queue& operator=(const Queue&) = delete;
 
   void Init(length_t length) {
     if (alreadyInit_ && length == maxLen_) return;
