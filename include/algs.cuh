@@ -86,6 +86,9 @@ class Queue {
     q2->queueEnd_ = e;
   }
 
+  // Release the arrays now (the destructor would otherwise do it); Init() may follow.
+  void freeQueue() { release(); }
+
   Queue<T>* devPtr() { return devQueue_; }
   void SyncHostWithDevice() {
     Queue<T> tmp_bytes_only;  // receives the device copy's fields, then only the indices are kept

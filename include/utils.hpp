@@ -10,6 +10,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <iostream>
 #include <string>
 
@@ -67,6 +68,9 @@ inline void copyArrayHostToDevice(const void* hostSrc, void* devDst, length_t el
 inline void copyArrayDeviceToHost(const void* devSrc, void* hostDst, length_t elements, int32_t eleSize) {
   cus_report(cudaMemcpy(hostDst, devSrc, (size_t)elements * (size_t)eleSize, cudaMemcpyDeviceToHost),
              "copyArrayDeviceToHost");
+}
+inline void copyArrayHostToHost(const void* hostSrc, void* hostDst, length_t elements, int32_t eleSize) {
+  memcpy(hostDst, hostSrc, (size_t)elements * (size_t)eleSize);
 }
 inline void copyArrayDeviceToDevice(const void* devSrc, void* devDst, length_t elements, int32_t eleSize) {
   cus_report(cudaMemcpy(devDst, devSrc, (size_t)elements * (size_t)eleSize, cudaMemcpyDeviceToDevice),

@@ -64,3 +64,14 @@ def test_operator_headers_compile(tmp_path):
                         os.path.join(ROOT, "include"), str(src), "-o", str(tmp_path / "ops_user.o")],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+
+
+def test_every_reference_algorithm_compiles_on_these_headers():
+    """The reference's BFS, connected components, PageRank, betweenness centrality and static and
+    streaming Katz sources (its src/ tree) compile unmodified against include/ (oracle/Makefile
+    target algs_check; skipped where the reference tree is absent)."""
+    r = subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "algs_check"],
+                       capture_output=True, text=True, timeout=900)
+    if "reference not present" in r.stdout:
+        pytest.skip("reference tree absent")
+    assert r.returncode == 0 and "all reference algorithms compile" in r.stdout, r.stdout[-3000:] + r.stderr[-3000:]
