@@ -209,6 +209,22 @@ bool configure_mlp() {
 
 using namespace tc;
 
+// The 256 cells' network inputs: the caller's features, or each cell's nominal degrees
+// (a = 1.5 * 2^(c/16), b = 1.5 * 2^(c%16)) when there are none.
+static void cell_feature_rows(const float* cell_features, float* feat) {
+  for (int c = 0; c < 256; ++c) {
+    if (cell_features) {
+      for (int k = 0; k < kIn; ++k) feat[c * kIn + k] = cell_features[c * kIn + k];
+    } else {
+      const double a = 1.5 * (double)(1 << (c / 16)), b = 1.5 * (double)(1 << (c % 16));
+      feat[c * kIn + 0] = (float)std::log2(1.0 + a);
+      feat[c * kIn + 1] = (float)std::log2(1.0 + b);
+      feat[c * kIn + 2] = (float)(std::min(a, b) / std::max(a, b));
+      feat[c * kIn + 3] = (float)c / 255.f;
+    }
+  }
+}
+
 extern "C" {
 
 tc_status tc_mlp_init(float* params_host, uint64_t seed) {
@@ -263,35 +279,10 @@ tc_status tc_mlp_adam_step(float* d_params, const float* d_grad, float* d_m, flo
   return TC_OK;
 }
 
-tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* sch, void* stream) {
-  if (!d_params || !sch || (kind != 0 && kind != 1)) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+tc_status tc_sched_from_costs(int kind, const float* cell_features, const float* costs, tc_sched* sch) {
+  if (!sch || !costs || (kind != 0 && kind != 1)) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
   std::vector<float> feat(256 * kIn);
-  for (int c = 0; c < 256; ++c) {
-    if (cell_features) {
-      for (int k = 0; k < kIn; ++k) feat[c * kIn + k] = cell_features[c * kIn + k];
-    } else {
-      const double a = 1.5 * (double)(1 << (c / 16)), b = 1.5 * (double)(1 << (c % 16));
-      feat[c * kIn + 0] = (float)std::log2(1.0 + a);
-      feat[c * kIn + 1] = (float)std::log2(1.0 + b);
-      feat[c * kIn + 2] = (float)(std::min(a, b) / std::max(a, b));
-      feat[c * kIn + 3] = (float)c / 255.f;
-    }
-  }
-  cudaStream_t s = (cudaStream_t)stream;
-  float *dx = nullptr, *dy = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&dx, sizeof(float) * feat.size()));
-  TC_CUDA_TRY(cudaMalloc(&dy, sizeof(float) * 256 * kOut));
-  std::vector<float> y(256 * kOut);
-  tc_status rc = TC_OK;
-  if (cudaMemcpyAsync(dx, feat.data(), sizeof(float) * feat.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
-    rc = fail(TC_ERR_CUDA, "copy failed");
-  if (rc == TC_OK) rc = tc_mlp_forward(d_params, dx, 256, dy, stream);
-  if (rc == TC_OK && (cudaMemcpyAsync(y.data(), dy, sizeof(float) * y.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-                      cudaStreamSynchronize(s) != cudaSuccess))
-    rc = fail(TC_ERR_CUDA, "copy failed");
-  cudaFree(dx);
-  cudaFree(dy);
-  if (rc != TC_OK) return rc;
+  cell_feature_rows(cell_features, feat.data());
   // Output ids: static count 0 = the warp streams the list through the hash set, 1 = one lane
   // walks it, 2 = packed walk (the table entry is the output id); streaming 1 = binary search,
   // 2 = merge (table entries 0 and 1). The outputs are predicted log2 costs per edge. A cell
@@ -314,11 +305,11 @@ tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_fe
                                : (16LL * bi > ratio * ai * lg ? 0 : 1);
     const int nstrat = kind == 0 ? 3 : 2;
     const int out0 = kind == 0 ? 0 : 1;  // network output of table entry 0
-    const float c_rule = y[c * kOut + out0 + rule];
+    const float c_rule = costs[c * kOut + out0 + rule];
     int pick = rule;
     float c_best = c_rule + log_keep;
     for (int e = 0; e < nstrat; ++e) {
-      const float ce = y[c * kOut + out0 + e];
+      const float ce = costs[c * kOut + out0 + e];
       if (e != rule && ce < c_best) {
         c_best = ce;
         pick = e;
@@ -328,6 +319,28 @@ tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_fe
   }
   sch->use_table = 1;
   return TC_OK;
+}
+
+tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* sch, void* stream) {
+  if (!d_params || !sch || (kind != 0 && kind != 1)) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  std::vector<float> feat(256 * kIn);
+  cell_feature_rows(cell_features, feat.data());
+  cudaStream_t s = (cudaStream_t)stream;
+  float *dx = nullptr, *dy = nullptr;
+  TC_CUDA_TRY(cudaMalloc(&dx, sizeof(float) * feat.size()));
+  TC_CUDA_TRY(cudaMalloc(&dy, sizeof(float) * 256 * kOut));
+  std::vector<float> y(256 * kOut);
+  tc_status rc = TC_OK;
+  if (cudaMemcpyAsync(dx, feat.data(), sizeof(float) * feat.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
+    rc = fail(TC_ERR_CUDA, "copy failed");
+  if (rc == TC_OK) rc = tc_mlp_forward(d_params, dx, 256, dy, stream);
+  if (rc == TC_OK && (cudaMemcpyAsync(y.data(), dy, sizeof(float) * y.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+                      cudaStreamSynchronize(s) != cudaSuccess))
+    rc = fail(TC_ERR_CUDA, "copy failed");
+  cudaFree(dx);
+  cudaFree(dy);
+  if (rc != TC_OK) return rc;
+  return tc_sched_from_costs(kind, feat.data(), y.data(), sch);
 }
 
 tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strategy, const float* d_label, int32_t n,

@@ -104,6 +104,7 @@ SIGNATURES = {
     "tc_autotune_load": (ctypes.c_int, [ctypes.c_char_p]),
     "tc_cell_stats": (ctypes.c_int, [_P, _P, _P]),
     "tc_sched_learned": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(Sched), _P]),
+    "tc_sched_from_costs": (ctypes.c_int, [ctypes.c_int, _P, _P, ctypes.POINTER(Sched)]),
     "tc_mlp_init": (ctypes.c_int, [_P, ctypes.c_uint64]),
     "tc_mlp_forward": (ctypes.c_int, [_P, _P, _i32, _P, _P]),
     "tc_mlp_backward": (ctypes.c_int, [_P, _P, _P, _P, _i32, _P, _P, _P]),

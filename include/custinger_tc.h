@@ -292,15 +292,19 @@ tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strat
                        int32_t epochs, float lr, float* loss_host, void* stream);
 
 /* Fill a scheduler from a trained MLP (device parameters) whose outputs are predicted log2
- * costs per edge of each strategy: for every degree cell, the choice between the two strategies
- * of `kind` (0 = static count: the warp streams the shorter list or one lane walks it; 1 =
- * streaming delta: search or merge) goes into s->table and s->use_table = 1. The fixed rule
- * (static: s->lane_max_deg; streaming: s->search_ratio_x16; on the cell's mean degrees) is the
- * fallback: a cell takes the other strategy only when the network predicts it at least 5%
- * cheaper. cell_features (host, 256 x TC_MLP_IN floats: mean log2(1 + a), mean log2(1 + b),
- * mean b/a, cell id / 255, as tc_cell_stats files the cells) describe each cell; NULL uses the
- * cells' nominal degrees. */
+ * costs per edge of each strategy: for every degree cell, the choice among the strategies of
+ * `kind` (0 = static count: the warp streams the shorter list, one lane walks it, or the warp
+ * walks the group's lists packed: table entries 0, 1, 2 = network outputs 0, 1, 2; 1 = streaming
+ * delta: search or merge, table entries 0, 1 = outputs 1, 2) goes into s->table and
+ * s->use_table = 1. The fixed rule (static: s->lane_max_deg and s->packed_max_deg; streaming:
+ * s->search_ratio_x16; on the cell's mean degrees) is the fallback: a cell takes another
+ * strategy only when the network predicts it at least 5% cheaper than the rule's. cell_features
+ * (host, 256 x TC_MLP_IN floats: mean log2(1 + a), mean log2(1 + b), mean b/a, cell id / 255, as
+ * tc_cell_stats files the cells) describe each cell; NULL uses the cells' nominal degrees. */
 tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_features, tc_sched* s, void* stream);
+/* The decision step of tc_sched_learned alone, on the host (no GPU): costs (host, 256 x TC_MLP_OUT
+ * floats) are the network's outputs for the 256 cells. */
+tc_status tc_sched_from_costs(int kind, const float* cell_features, const float* costs, tc_sched* s);
 
 /* Phase timing of counts issued by the calling thread: CUDA events recorded on the launching
  * stream around the orientation passes and around the intersection kernel (off by default;
