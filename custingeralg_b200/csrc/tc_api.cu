@@ -239,11 +239,13 @@ void tc_sched_default(tc_sched* s) {
 
 tc_status tc_count_csr32(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode, int32_t* per_vertex,
                          int64_t* triangles_dev, tc_count_info* info, const tc_sched* sched, void* stream) {
+  tc::TraceRange trace_range("tc_count_csr32");
   return count_csr<Csr32View>(nv, d_off, d_ind, pv_mode, per_vertex, triangles_dev, info, sched, stream);
 }
 
 tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind, int pv_mode, int32_t* per_vertex,
                          int64_t* triangles_dev, tc_count_info* info, const tc_sched* sched, void* stream) {
+  tc::TraceRange trace_range("tc_count_csr64");
   return count_csr<Csr64View>(nv, d_off, d_ind, pv_mode, per_vertex, triangles_dev, info, sched, stream);
 }
 

@@ -267,6 +267,7 @@ tc_status tc_graph_validate(tc_graph* g, void* stream) {
 
 tc_status tc_count_static(tc_graph* g, int pv_mode, int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
                           const tc_sched* sched, void* stream) {
+  tc::TraceRange trace_range("tc_count_static");
   if (!g) return fail(TC_ERR_INVALID_ARG, "graph is NULL");
   if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_HANDLE64) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
   if (pv_mode != TC_PV_NONE && g->n > 0 && !per_vertex)

@@ -6,9 +6,20 @@
 #include <cstdio>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/custinger_tc.h"
 
 namespace tc {
+
+// A named NVTX range over a scope: the public entry points mark themselves on the timelines of
+// tools such as Nsight Systems; with no tool attached the calls return at once.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
 
 constexpr int kWarp = 32;
 constexpr unsigned kFull = 0xffffffffu;

@@ -1086,6 +1086,7 @@ extern "C" {
 tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, const uint8_t* is_delete, int64_t b,
                          int mem, int32_t* per_vertex, int64_t* delta_dev, tc_batch_info* info, const tc_sched* sched,
                          void* stream) {
+  tc::TraceRange trace_range("tc_apply_batch");
   if (!g) return fail(TC_ERR_INVALID_ARG, "graph is NULL");
   if (b < 0 || (b > 0 && (!src || !dst)) || (mem != TC_MEM_HOST && mem != TC_MEM_DEVICE))
     return fail(TC_ERR_INVALID_ARG, "invalid batch arguments");
@@ -1323,6 +1324,7 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
 tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst, const int32_t* d_offsets,
                          const int32_t* d_dup, int64_t b, int sign, int32_t* per_vertex, int64_t* delta_dev,
                          const tc_sched* sched, void* stream) {
+  tc::TraceRange trace_range("tc_count_batch");
   if (!g || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup || !d_offsets)) || (sign != 1 && sign != -1) || !per_vertex)
     return fail(TC_ERR_INVALID_ARG, "invalid arguments");
   cudaStream_t s = (cudaStream_t)stream;
@@ -1626,6 +1628,7 @@ tc_status tc_pipeline_destroy(tc_pipeline* p) {
 
 tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t* d_dst, const uint8_t* d_is_delete,
                             int64_t b, int32_t* per_vertex, int64_t* delta_dev, void* stream) {
+  tc::TraceRange trace_range("tc_pipeline_apply");
   if (!p || b < 0 || (b > 0 && (!d_src || !d_dst))) return fail(TC_ERR_INVALID_ARG, "invalid batch arguments");
   if (b > p->b_max)
     return fail(TC_ERR_CAPACITY, "batch of %lld updates exceeds the pipeline's %lld", (long long)b,
