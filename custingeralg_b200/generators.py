@@ -173,3 +173,81 @@ def write_binary(g: Csr, path: str) -> None:
     rc = _load().tcgen_write_binary(os.fsencode(path), ctypes.byref(c))
     if rc != 0:
         raise ReadError(rc, path)
+
+
+def write_dimacs(g: Csr, path: str) -> None:
+    """Write g as a METIS / DIMACS-10 adjacency file (.graph): "n m" (m undirected edges), then one
+    line per vertex with its 1-based neighbours; read_graph(path) reads it back unchanged."""
+    off = np.asarray(g.off, dtype=np.int64)
+    ids = (np.asarray(g.ind, dtype=np.int64) + 1).astype(str)
+    with open(path, "w") as f:
+        f.write(f"{g.n} {int(off[-1]) // 2}\n")
+        for v in range(g.n):
+            f.write(" ".join(ids[off[v]:off[v + 1]]) + "\n")
+
+
+def write_snap(g: Csr, path: str) -> None:
+    """Write g as a SNAP edge list (.txt): each undirected edge once, "u<TAB>v" with 0-based ids."""
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(np.asarray(g.off, dtype=np.int64)))
+    dst = np.asarray(g.ind, dtype=np.int64)
+    keep = src < dst
+    with open(path, "w") as f:
+        f.write(f"# Undirected graph: {g.n} nodes, {int(keep.sum())} edges\n# FromNodeId\tToNodeId\n")
+        np.savetxt(f, np.stack([src[keep], dst[keep]], axis=1), fmt="%d", delimiter="\t")
+
+
+def write_mtx(g: Csr, path: str) -> None:
+    """Write g as a MatrixMarket coordinate pattern file (.mtx), symmetric, lower triangle, 1-based."""
+    src = np.repeat(np.arange(g.n, dtype=np.int64), np.diff(np.asarray(g.off, dtype=np.int64)))
+    dst = np.asarray(g.ind, dtype=np.int64)
+    keep = src > dst
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate pattern symmetric\n")
+        f.write(f"{g.n} {g.n} {int(keep.sum())}\n")
+        np.savetxt(f, np.stack([src[keep] + 1, dst[keep] + 1], axis=1), fmt="%d")
+
+
+def write_graph(g: Csr, path: str) -> None:
+    """Write g in the format its file name names, as the reference drivers pick their reader:
+    .graph (DIMACS), .txt (SNAP), .mtx (MatrixMarket), anything else the binary cache."""
+    if path.endswith(".graph"):
+        write_dimacs(g, path)
+    elif path.endswith(".txt"):
+        write_snap(g, path)
+    elif path.endswith(".mtx"):
+        write_mtx(g, path)
+    else:
+        write_binary(g, path)
+
+
+def main(argv=None) -> None:
+    """python -m custingeralg_b200.generators {rmat,er,ba,grid} [options] --out FILE"""
+    import argparse
+    ap = argparse.ArgumentParser(description="Write a seeded synthetic graph (symmetric, sorted, no self-loops)")
+    ap.add_argument("family", choices=["rmat", "er", "ba", "grid"])
+    ap.add_argument("--scale", type=int, default=16, help="rmat: 2^scale vertices")
+    ap.add_argument("--edge-factor", type=int, default=16, help="rmat: generated pairs per vertex")
+    ap.add_argument("--abc", type=float, nargs=3, default=[0.57, 0.19, 0.19], help="rmat quadrant weights a b c")
+    ap.add_argument("--n", type=int, default=1 << 14, help="er, ba: vertices")
+    ap.add_argument("--degree", type=float, default=16.0, help="er: average degree")
+    ap.add_argument("--m0", type=int, default=8, help="ba: edges per new vertex")
+    ap.add_argument("--side", type=int, default=256, help="grid: side x side vertices")
+    ap.add_argument("--rewire", type=float, default=0.05, help="grid: rewiring probability")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--out", required=True, help=".graph, .txt, .mtx or a binary cache (.tccsr)")
+    a = ap.parse_args(argv)
+    if a.family == "rmat":
+        g = rmat(a.scale, a.edge_factor, *a.abc, seed=a.seed)
+    elif a.family == "er":
+        g = erdos_renyi(a.n, a.degree / a.n, seed=a.seed)
+    elif a.family == "ba":
+        g = barabasi_albert(a.n, a.m0, seed=a.seed)
+    else:
+        g = grid_rewired(a.side, a.rewire, seed=a.seed)
+    write_graph(g, a.out)
+    print(f"{a.out}: n={g.n} directed edges={g.m}")
+
+
+if __name__ == "__main__":
+    main()
+
