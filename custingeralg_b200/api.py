@@ -151,11 +151,33 @@ class Pipeline:
         N.check(N.lib().tc_pipeline_autotune(self._p, batches))
 
     def info(self):
+        """[(bin capacity, delta-kernel CTAs per SM)] per bin."""
         nb = ctypes.c_int32(0)
-        caps = (ctypes.c_int64 * 8)()
-        blocks = (ctypes.c_int32 * 8)()
+        caps = (ctypes.c_int64 * 16)()
+        blocks = (ctypes.c_int32 * 16)()
         N.check(N.lib().tc_pipeline_info(self._p, ctypes.byref(nb), caps, blocks))
         return [(int(caps[i]), int(blocks[i])) for i in range(nb.value)]
+
+    def plan(self) -> "N.PipelinePlan":
+        """The tuned bins (which graph serves each bin) and delta-kernel tile shapes."""
+        p = N.PipelinePlan()
+        N.check(N.lib().tc_pipeline_plan_get(self._p, ctypes.byref(p)))
+        return p
+
+    def set_plan(self, plan) -> None:
+        N.check(N.lib().tc_pipeline_plan_set(self._p, ctypes.byref(plan)))
+
+    def profile(self, on: bool = True) -> None:
+        """Record the delta kernels' event times and algorithmic bytes (before prepare())."""
+        N.check(N.lib().tc_pipeline_profile(self._p, int(on)))
+
+    def stats(self) -> dict:
+        b, ms, by = ctypes.c_int64(), ctypes.c_double(), ctypes.c_int64()
+        N.check(N.lib().tc_pipeline_stats(self._p, ctypes.byref(b), ctypes.byref(ms), ctypes.byref(by)))
+        return {"batches": b.value, "delta_ms": ms.value, "delta_bytes": by.value}
+
+    def set_wait_bound(self, wait_ns: int, extra_arrivals: int = 0) -> None:
+        N.check(N.lib().tc_pipeline_set_wait_bound(self._p, wait_ns, extra_arrivals))
 
     def close(self):
         if self._p:
@@ -185,3 +207,14 @@ def count_all_triangles_csr(n: int, d_off, d_ind, out, pv_mode: int = N.TC_PV_CS
             ctypes.byref(sched) if sched is not None else None, _stream_ptr(stream))
     N.check(st)
     return (info.triangles, info) if sync else None
+
+
+def shard_ranges(prefix, nshards: int):
+    """The static count's multi-GPU split rule (tc_shard_ranges, host side): given the exclusive
+    prefix of the centres' predicted work (int64[n+1]), the first centre of each of nshards
+    shards; shard r counts the centres [lo[r], lo[r+1])."""
+    prefix = np.ascontiguousarray(prefix, dtype=np.int64)
+    n = prefix.size - 1
+    lo = np.zeros(nshards + 1, np.int32)
+    N.check(N.lib().tc_shard_ranges(prefix.ctypes.data, n, nshards, lo.ctypes.data))
+    return lo

@@ -124,7 +124,26 @@ tc_status Workspace::ensure(int64_t n, int64_t m, int64_t extent) {
   return TC_OK;
 }
 
+tc_status Workspace::ensure_shards(int64_t n) {
+  if (n + 1 <= shard_cap) return TC_OK;
+  cudaFree(shard_cost);
+  cudaFree(shard_prefix);
+  cudaFree(shard_tiles);
+  shard_cost = nullptr;
+  shard_prefix = nullptr;
+  shard_tiles = nullptr;
+  shard_cap = 0;
+  TC_CUDA_TRY(cudaMalloc(&shard_cost, sizeof(int32_t) * (size_t)(n + 1)));
+  TC_CUDA_TRY(cudaMalloc(&shard_prefix, sizeof(int64_t) * (size_t)(n + 2)));
+  TC_CUDA_TRY(cudaMalloc(&shard_tiles, sizeof(int64_t) * (size_t)(scan_tiles(n + 1) + 1)));
+  shard_cap = n + 1;
+  return TC_OK;
+}
+
 void Workspace::release() {
+  cudaFree(shard_cost);
+  cudaFree(shard_prefix);
+  cudaFree(shard_tiles);
   cudaFree(dplus);
   cudaFree(offp);
   cudaFree(indp);
@@ -247,6 +266,12 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
                          int64_t* triangles_dev, tc_count_info* info, const tc_sched* sched, void* stream) {
   tc::TraceRange trace_range("tc_count_csr64");
   return count_csr<Csr64View>(nv, d_off, d_ind, pv_mode, per_vertex, triangles_dev, info, sched, stream);
+}
+
+tc_status tc_shard_ranges(const int64_t* prefix_host, int32_t n, int32_t nshards, int32_t* lo_host) {
+  if (!prefix_host || !lo_host || n < 0 || nshards < 1) return fail(TC_ERR_INVALID_ARG, "invalid shard arguments");
+  for (int32_t r = 0; r <= nshards; ++r) lo_host[r] = shard_start(prefix_host, n, r, nshards);
+  return TC_OK;
 }
 
 tc_status tc_profile_enable(int on) {

@@ -99,7 +99,30 @@ struct DevStatus {
   unsigned int q_orient_vtx;             // vertex ids
   unsigned int cls_cnt[32];              // CTA-queue items per work class
   unsigned int cls_pos[32];              // and their fill cursors
+  unsigned int sharded;                  // 1: count only centres in [shard_lo, shard_hi)
+  unsigned int shard_lo, shard_hi;
+  unsigned int pad0;
+  unsigned long long shard_work;         // predicted work of this shard's centres (units of 16)
+  unsigned long long total_work;         // and of all centres
 };
+
+// Multi-GPU split of the static count: shard r of N counts the edge centres c in
+// [shard_start(r), shard_start(r + 1)), where prefix[c] is the exclusive prefix over the centres
+// of their predicted work; shard r starts at the first centre whose prefix reaches r/N of the
+// total. Host and device use this one function, so every rank derives the same ranges.
+__host__ __device__ inline int32_t shard_start(const int64_t* prefix, int32_t n, int32_t r, int32_t nshards) {
+  if (r <= 0) return 0;
+  if (r >= nshards) return n;
+  const int64_t total = prefix[n];
+  const int64_t target = (total / nshards) * r + ((total % nshards) * r) / nshards;
+  int32_t lo = 0, hi = n;  // first c in [0, n] with prefix[c] >= target
+  while (lo < hi) {
+    const int32_t mid = lo + (hi - lo) / 2;
+    if (prefix[mid] < target) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
 
 // ---- scheduler parameters as the kernels see them --------------------------------------
 
@@ -109,8 +132,8 @@ struct SchedParams {
   int32_t use_table;
   int32_t chunk;
   int32_t blocks_per_sm;   // 0 = occupancy limit
-  int32_t shard;           // count the edges whose centre c has c % nshards == shard
-  int32_t nshards;
+  int32_t shard;           // static: count the centres of range `shard` of `nshards` (shard_start);
+  int32_t nshards;         // streaming: the changed edges e with e % nshards == shard
   int32_t cell_filter;     // -1 all edges, -2 none, >= 0 only that degree cell
   int32_t lane_max;        // static: lists of at most this many entries are walked by one lane
   int32_t packed_max;      // static: longer lists up to this many entries are walked packed
@@ -140,8 +163,15 @@ struct Workspace {
   int64_t hub_cap = 0;
   int64_t chunk_cap = 0;
   DevStatus* st = nullptr;       // [1]
+  // multi-GPU split (allocated on the first sharded count): predicted work per centre (units of
+  // 16 probes), its exclusive prefix and the scan's tile sums
+  int32_t* shard_cost = nullptr;   // [shard_cap]
+  int64_t* shard_prefix = nullptr; // [shard_cap + 1]
+  int64_t* shard_tiles = nullptr;
+  int64_t shard_cap = 0;
   // n vertices, m directed edges, lists inside [0, extent) of the input's index space.
   tc_status ensure(int64_t n, int64_t m_directed, int64_t extent = -1);
+  tc_status ensure_shards(int64_t n);
   void release();
   // Hub arrays needed for a graph of m directed edges.
   static int64_t hubs_for(int64_t m) { return m / kHubMin + 1; }

@@ -2,17 +2,21 @@
 // (tc_count_csr32) with its working memory in a fixed array of this library's own device
 // memory instead of cudaMalloc'd buffers.
 //
-// Who needs it: code that runs where it cannot call cudaMalloc -- inside a captured CUDA
-// graph region, under an allocator that forbids device allocation after start-up, or from a
-// host that pre-plans every byte of device memory (a serving process with a fixed budget).
-// They still pass their own input CSR and output buffers.
+// Who needs it: callers that must not allocate device memory when they count. A process whose
+// memory is owned by another allocator (a framework's caching pool that has taken the free
+// device memory, so a cudaMalloc of its own would fail) or a service that reserves every byte of
+// device memory at start-up; and latency-sensitive loops, where cudaMalloc and cudaFree can
+// synchronise the device and stall the work of other streams. They still pass their own input
+// CSR and output buffers.
 //
 // The array is sized for graphs of up to TC_NOALLOC_MAX_NV vertices and TC_NOALLOC_MAX_EDGES
-// directed edges (about 32 MB); every GPU that loads the library holds it until the process
-// exits. All calls share it: two calls that overlap on the GPU race and corrupt each other, so
-// serialise them (one stream, or events). The first call on a device looks up the array's
-// device address (cudaGetSymbolAddress) with that device current; make that first call before
-// any stream capture.
+// directed edges: about 48.6 MiB (51 MB, checked below), which every GPU that loads the library
+// holds until the process exits. Larger graphs are rejected with TC_ERR_CAPACITY. All calls
+// share the array and each starts by clearing the part that must start at zero (the status
+// block); two calls that overlap on the GPU race and corrupt each other, so serialise them (one
+// stream, or events). The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current and keeps it for later calls. The edge count
+// d_off[nv] is read back to the host, so every call synchronises `stream` once.
 #include <cstring>
 #include <mutex>
 
@@ -45,6 +49,8 @@ constexpr size_t kOffHubCnt = align256(kOffHubDone + sizeof(int32_t) * kMaxHubs)
 constexpr size_t kOffChunkHub = align256(kOffHubCnt + sizeof(int32_t) * kMaxChunks);
 constexpr size_t kOffIndp = align256(kOffChunkHub + sizeof(int32_t) * kMaxChunks);
 constexpr size_t kScratchBytes = align256(kOffIndp + sizeof(int32_t) * kMaxEdges);
+static_assert(kScratchBytes > (size_t(48) << 20) && kScratchBytes < (size_t(49) << 20),
+              "the documented size of the no-alloc scratch (about 48.6 MiB) no longer holds");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -83,7 +89,10 @@ using namespace tc;
 extern "C" tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode,
                                             int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
                                             const tc_sched* sched, void* stream) {
+  tc::TraceRange trace_range("tc_count_csr32_noalloc");
   if (nv < 0 || (nv > 0 && (!d_off || !d_ind))) return fail(TC_ERR_INVALID_ARG, "invalid CSR (nv=%d)", nv);
+  if (sched && sched->nshards > 1)
+    return fail(TC_ERR_INVALID_ARG, "no-alloc count: a sharded count needs working memory this entry point does not hold");
   if (pv_mode < TC_PV_NONE || pv_mode > TC_PV_HANDLE64) return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
   if (pv_mode != TC_PV_NONE && nv > 0 && !per_vertex)
     return fail(TC_ERR_INVALID_ARG, "per_vertex output required for mode %d", pv_mode);

@@ -490,6 +490,8 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
   uint32_t tri = 0;
   const unsigned n_large = st->n_large;
   const unsigned n_medium = st->n_medium;
+  const bool sharded = st->sharded != 0;
+  const int32_t s_lo = (int32_t)st->shard_lo, s_hi = (int32_t)st->shard_hi;
 
   // CTA tier: one CTA per item (centre with a > warp_max, kCtaRange of its neighbours), over
   // chunks of kChunk staged entries of N+(c).
@@ -590,8 +592,8 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
       const bool in = uu < cend;
       const int aa = in ? __ldg(dplus + uu) : 0;
       const int dd = in ? __ldg(degv + uu) : 0;
-      unsigned elig =
-          __ballot_sync(kFull, aa >= 1 && aa <= sp.warp_max && dd <= kWarpRange && (uu % sp.nshards) == sp.shard);
+      unsigned elig = __ballot_sync(
+          kFull, aa >= 1 && aa <= sp.warp_max && dd <= kWarpRange && (!sharded || (uu >= s_lo && uu < s_hi)));
       while (elig) {
         const int sl = __ffs(elig) - 1;
         elig &= elig - 1;
@@ -671,17 +673,15 @@ struct OrientAcc {
 
 __device__ __forceinline__ void finish_vertex(const int32_t u, const int32_t d, const int64_t s, const int32_t a,
                                               int32_t* __restrict__ dplus, int64_t* __restrict__ offp,
-                                              int32_t* __restrict__ degv, const int shard, const int nshards,
-                                              OrientAcc& acc) {
+                                              int32_t* __restrict__ degv, OrientAcc& acc) {
   const int lane = threadIdx.x & (kWarp - 1);
-  const bool mine = (u % nshards) == shard;
   if (lane == 0) {
     dplus[u] = a;
     offp[u] = s;
     degv[u] = d;
     if (d >= 2) acc.ei += (unsigned long long)a;
     // sum over u -> v of d+(u) + d+(v) = sum over v of d+(v) deg(v)
-    if (mine) acc.work += (unsigned long long)a * (unsigned long long)d;
+    acc.work += (unsigned long long)a * (unsigned long long)d;
     acc.mx = max(acc.mx, (unsigned)a);
   }
 }
@@ -731,8 +731,7 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
                                                 const int32_t* __restrict__ hub_u,
                                                 const int32_t* __restrict__ hub_base, int32_t* __restrict__ hub_cnt,
                                                 int32_t* __restrict__ hub_done, const int32_t* __restrict__ chunk_hub,
-                                                const int64_t hub_cap, const int64_t chunk_cap, DevStatus* __restrict__ st,
-                                                const int shard, const int nshards) {
+                                                const int64_t hub_cap, const int64_t chunk_cap, DevStatus* __restrict__ st) {
   const int lane = threadIdx.x & (kWarp - 1);
   const unsigned nchunks = (unsigned)min((long long)st->n_hub_chunks, (long long)chunk_cap);
   const unsigned nhubs = (unsigned)min((long long)st->n_hubs, (long long)hub_cap);
@@ -789,7 +788,7 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
       }
       a += cn;
     }
-    finish_vertex(u, d, s, a, dplus, offp, degv, shard, nshards, acc);
+    finish_vertex(u, d, s, a, dplus, offp, degv, acc);
   }
 
   // Vertex tiles (hubs skipped: done above). The warp walks the concatenated lists of a tile's
@@ -879,7 +878,7 @@ __global__ void __launch_bounds__(256) k_orient(const View g, const int32_t n, i
       degv[u_l] = cap_bad ? 0 : d_l;
       const int32_t dd = cap_bad ? 0 : d_l;
       if (dd >= 2) acc.ei += (unsigned long long)a_l;
-      if ((u_l % nshards) == shard) acc.work += (unsigned long long)a_l * (unsigned long long)dd;
+      acc.work += (unsigned long long)a_l * (unsigned long long)dd;
       acc.mx = max(acc.mx, (unsigned)a_l);
     }
   }
@@ -915,16 +914,20 @@ __device__ __forceinline__ int work_class(const int32_t a, const int32_t d) {
   return min(kWorkClasses - 1, 63 - __clzll(max(w, 1ull)));
 }
 
-__device__ __forceinline__ bool cta_centre(const int32_t u, const int32_t a, const int warp_max, const int shard,
-                                           const int nshards) {
-  return a > warp_max && (u % nshards) == shard;
+// Is u a centre of this count's shard (every centre when the count is not sharded)?
+__device__ __forceinline__ bool in_shard(const DevStatus* __restrict__ st, const int32_t u) {
+  return !st->sharded || (u >= (int32_t)st->shard_lo && u < (int32_t)st->shard_hi);
+}
+
+__device__ __forceinline__ bool cta_centre(const DevStatus* __restrict__ st, const int32_t u, const int32_t a,
+                                           const int warp_max) {
+  return a > warp_max && in_shard(st, u);
 }
 
 __global__ void __launch_bounds__(256) k_push_items(const int32_t n, const int32_t* __restrict__ dplus,
                                                     const int32_t* __restrict__ degv,
                                                     unsigned long long* __restrict__ medium, const int64_t item_cap,
-                                                    DevStatus* __restrict__ st, const int warp_max, const int shard,
-                                                    const int nshards) {
+                                                    DevStatus* __restrict__ st, const int warp_max) {
   const int lane = threadIdx.x & (kWarp - 1);
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) / kWarp;
   unsigned bad = 0;
@@ -934,9 +937,9 @@ __global__ void __launch_bounds__(256) k_push_items(const int32_t n, const int32
     const int32_t u = (int32_t)uu;
     const int32_t a = in ? dplus[u] : 0;
     const int32_t d = in ? degv[u] : 0;
-    if (in && cta_centre(u, a, warp_max, shard, nshards))
+    if (in && cta_centre(st, u, a, warp_max))
       atomicAdd(&st->cls_cnt[work_class(a, d)], (unsigned)((d + kCtaRange - 1) / kCtaRange));
-    const bool wrp = in && a > 0 && a <= warp_max && d > kWarpRange && (u % nshards) == shard;
+    const bool wrp = in && a > 0 && a <= warp_max && d > kWarpRange && in_shard(st, u);
     const int x = wrp ? (d + kWarpRange - 1) / kWarpRange : 0;
     int incl = x;
 #pragma unroll
@@ -963,8 +966,7 @@ __global__ void __launch_bounds__(256) k_push_items(const int32_t n, const int32
 __global__ void __launch_bounds__(256) k_fill_items(const int32_t n, const int32_t* __restrict__ dplus,
                                                     const int32_t* __restrict__ degv,
                                                     unsigned long long* __restrict__ large, const int64_t item_cap,
-                                                    DevStatus* __restrict__ st, const int warp_max, const int shard,
-                                                    const int nshards) {
+                                                    DevStatus* __restrict__ st, const int warp_max) {
   __shared__ unsigned cls_base[kWorkClasses];
   __shared__ unsigned total;
   if (threadIdx.x < kWarp) {
@@ -989,7 +991,7 @@ __global__ void __launch_bounds__(256) k_fill_items(const int32_t n, const int32
   for (int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; uu < n; uu += (int64_t)gridDim.x * blockDim.x) {
     const int32_t u = (int32_t)uu;
     const int32_t a = dplus[u];
-    if (!cta_centre(u, a, warp_max, shard, nshards)) continue;
+    if (!cta_centre(st, u, a, warp_max)) continue;
     const int32_t d = degv[u];
     const int cls = work_class(a, d);
     const int nit = (d + kCtaRange - 1) / kCtaRange;
@@ -997,6 +999,45 @@ __global__ void __launch_bounds__(256) k_fill_items(const int32_t n, const int32
     if ((int64_t)at + nit > (int64_t)n_items) continue;  // only past a capacity error
     for (int j = 0; j < nit; ++j) large[at + j] = make_item(u, j * kCtaRange);
   }
+}
+
+// ---- multi-GPU split of the static count -------------------------------------------------
+
+// Predicted intersection work of each centre c (needs the orientation): one probe per entry of
+// the other endpoint's list for every edge {c, o} that c is the centre of, plus 2 per such edge
+// and 1 per neighbour scanned, in units of 16 (int32, clamped). One warp per vertex.
+template <class View>
+__global__ void __launch_bounds__(256) k_shard_cost(const View g, const int32_t n, const int32_t* __restrict__ dplus,
+                                                    int32_t* __restrict__ cost) {
+  const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) / kWarp;
+  for (int64_t uu = gw; uu < n; uu += nw) {
+    const int32_t u = (int32_t)uu;
+    const int32_t d = g.len(u), a = dplus[u];
+    const int64_t s = g.start(u);
+    unsigned long long w = 0;
+    for (int32_t k = lane; k < d; k += kWarp) {
+      const int32_t o = g.ind[s + k];
+      if (o < 0 || o >= n) continue;
+      const int32_t b = dplus[o];
+      if (b > 0 && centre_of(u, a, o, b)) w += (unsigned long long)b + 2ull;
+    }
+    w = warp_sum(w);
+    if (lane == 0) cost[u] = (int32_t)min((w + (unsigned long long)d + 15ull) / 16ull, (unsigned long long)INT32_MAX);
+  }
+}
+
+// This count's range of centres (shard_start over the exclusive prefix of the costs).
+__global__ void k_shard_bounds(const int64_t* __restrict__ prefix, const int32_t n, const int32_t shard,
+                               const int32_t nshards, DevStatus* __restrict__ st) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int32_t lo = shard_start(prefix, n, shard, nshards), hi = shard_start(prefix, n, shard + 1, nshards);
+  st->shard_lo = (unsigned)lo;
+  st->shard_hi = (unsigned)hi;
+  st->shard_work = (unsigned long long)(prefix[hi] - prefix[lo]);
+  st->total_work = (unsigned long long)prefix[n];
+  st->sharded = 1;
 }
 
 // ---- exclusive scan of int32 counts into int64 offsets ------------------------------------
@@ -1163,19 +1204,27 @@ tc_status orient(const View& view, int32_t n, Workspace& ws, const SchedParams& 
   if (write)
     k_orient<View, true><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap,
                                                    ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
-                                                   ws.hub_cap, ws.chunk_cap, ws.st, sp.shard, sp.nshards);
+                                                   ws.hub_cap, ws.chunk_cap, ws.st);
   else
     k_orient<View, false><<<grid, 256, 0, stream>>>(view, n, ws.dplus, ws.offp, ws.degv, ws.indp, ws.e_cap,
                                                     ws.hub_u, ws.hub_base, ws.hub_cnt, ws.hub_done, ws.chunk_hub,
-                                                    ws.hub_cap, ws.chunk_cap, ws.st, sp.shard, sp.nshards);
+                                                    ws.hub_cap, ws.chunk_cap, ws.st);
   TC_CUDA_TRY(cudaGetLastError());
   if (write) {
+    if (sp.nshards > 1) {
+      // this count's range of centres: predicted work per centre, its prefix, the range
+      if (!ws.shard_cost || ws.shard_cap < (int64_t)n + 1)
+        return fail(TC_ERR_STATE, "sharded count without its shard workspace");
+      k_shard_cost<View><<<orient_grid(n), 256, 0, stream>>>(view, n, ws.dplus, ws.shard_cost);
+      TC_CUDA_TRY(cudaGetLastError());
+      TC_TRY(scan_counts(ws.shard_cost, n, ws.shard_prefix, ws.shard_tiles, stream));
+      k_shard_bounds<<<1, 32, 0, stream>>>(ws.shard_prefix, n, sp.shard, sp.nshards, ws.st);
+      TC_CUDA_TRY(cudaGetLastError());
+    }
     // the count's work queues (only a count reads them)
-    k_push_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.medium, ws.item_cap, ws.st, sp.warp_max,
-                                                   sp.shard, sp.nshards);
+    k_push_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.medium, ws.item_cap, ws.st, sp.warp_max);
     TC_CUDA_TRY(cudaGetLastError());
-    k_fill_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.large, ws.item_cap, ws.st, sp.warp_max,
-                                                   sp.shard, sp.nshards);
+    k_fill_items<<<hubs_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.degv, ws.large, ws.item_cap, ws.st, sp.warp_max);
     TC_CUDA_TRY(cudaGetLastError());
   }
   return TC_OK;
@@ -1222,6 +1271,7 @@ SchedParams to_params(const tc_sched* s) {
 template <class View>
 tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, int pv_mode, int32_t* per_vertex,
                        int64_t* triangles_dev, const SchedParams& sp, cudaStream_t stream) {
+  if (sp.nshards > 1 && n > 0) TC_TRY(ws.ensure_shards(n));
   TC_CUDA_TRY(cudaMemsetAsync(ws.st, 0, sizeof(DevStatus), stream));
   if (pv_mode != TC_PV_NONE && n > 0)
     TC_CUDA_TRY(cudaMemsetAsync(per_vertex, 0, (pv_mode == TC_PV_HANDLE64 ? 8 : 4) * (size_t)n, stream));
@@ -1238,7 +1288,9 @@ tc_status static_count(const View& view, int32_t n, int64_t m, Workspace& ws, in
       default: return fail(TC_ERR_INVALID_ARG, "unknown per-vertex mode %d", pv_mode);
     }
     prof_mark(2, stream);
-    prof_launches(5);  // k_find_hubs, k_orient, k_push_items, k_fill_items, k_count
+    // k_find_hubs, k_orient, k_push_items, k_fill_items, k_count (+ k_shard_cost, three scan
+    // kernels and k_shard_bounds when sharded)
+    prof_launches(sp.nshards > 1 ? 10 : 5);
   }
   (void)m;
   if (triangles_dev)
@@ -1261,6 +1313,10 @@ tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* inf
   info->edges_intersected = (int64_t)h.edges_intersected;
   info->oriented_work = (int64_t)h.oriented_work;
   info->max_out_degree = (int32_t)h.max_dplus;
+  info->shard_lo = h.sharded ? (int32_t)h.shard_lo : 0;
+  info->shard_hi = h.sharded ? (int32_t)h.shard_hi : -1;
+  info->shard_work = (int64_t)h.shard_work;
+  info->total_work = (int64_t)h.total_work;
   if (h.bad_flags & (kBadRange | kBadOrder | kBadSelfLoop)) {
     info->status = TC_ERR_BAD_GRAPH;
     return fail(TC_ERR_BAD_GRAPH, "graph check failed:%s%s%s", (h.bad_flags & kBadRange) ? " id out of range" : "",

@@ -31,12 +31,17 @@ constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
 constexpr int kRunStage = 4096;  // new entries of one long list staged in shared memory
+// Tile shape of the delta count (defaults; the pipeline's autotuner picks per batch-size bin):
 constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
 constexpr int64_t kDeltaItems = 1 << 20;  // capacity of the split-item queue
 constexpr unsigned long long kNoItem = ~0ull;
+// Bounded wait of the persistent delta kernel's grid barrier (a wait that runs out reports
+// kErrTimeout and the kernel skips the work after the barrier).
+constexpr unsigned long long kSpinNs = 2000000000ull;  // 2 s
+constexpr unsigned kSpinMaxIters = 1u << 24;
 
-enum : unsigned { kErrRange = 1u, kErrPool = 2u };
+enum : unsigned { kErrRange = 1u, kErrPool = 2u, kErrTimeout = 4u };
 
 struct BatchStatus {
   unsigned long long n_uniq;      // unique undirected edges
@@ -53,6 +58,8 @@ struct BatchStatus {
   unsigned long long not_fitting;
   unsigned long long n_long;      // insertion runs whose list is long (CTA kernel)
   unsigned long long n_split[2];  // split-intersection items queued (deletions, insertions)
+  unsigned long long delta_bytes; // algorithmic bytes of the batch's intersections (4(deg x + deg y) + 8 each)
+  unsigned int bar[2];            // grid-barrier arrivals of the persistent delta kernels
   unsigned int err;
   unsigned int pad;
 };
@@ -584,6 +591,18 @@ struct DeltaArgs {
   // split queue: (entry << 24 | chunk) items of long intersections (NULL = no splitting)
   unsigned long long* split_items;
   unsigned long long* split_cnt;  // zero before the first pass
+  int split_min;     // intersections whose shorter list is longer than this are split ...
+  int chunk;         // ... into items of this many entries of the shorter list
+  int shard;         // this rank counts the entries e with e % nshards == shard
+  int nshards;
+  unsigned long long* bytes_out;  // algorithmic bytes of the intersections run (NULL = not kept)
+  // persistent kernel (k_delta_fused): grid-barrier arrivals (zero at launch), where a wait
+  // that runs out reports kErrTimeout, the arrivals it waits for beyond the grid (0; a test sets
+  // 1 to make the wait run out) and its bound
+  unsigned* bar;
+  unsigned* err;
+  unsigned bar_extra;
+  unsigned long long spin_ns;
   uint8_t table[256];
 };
 
@@ -714,21 +733,43 @@ __device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaP
   return warp_sum(c);
 }
 
-// The triangle delta of the changed edges, one warp per edge. An edge whose shorter list is
-// longer than kDeltaSplit (two hubs) would be one warp's serial tail of the whole launch: when
-// A.split_items is set it is queued instead as items of kDeltaChunk entries of its shorter list,
-// which k_delta_split spreads over all warps (a full queue leaves the edge to this warp).
+// Per-CTA flush of the kept-triangle total and the algorithmic bytes: one atomic each per CTA.
+__device__ __forceinline__ void delta_flush(unsigned long long tri_acc, unsigned long long bytes_acc,
+                                            unsigned long long* __restrict__ tri_out,
+                                            unsigned long long* __restrict__ bytes_out) {
+  __shared__ unsigned long long s_tri[kThreads / 32], s_bytes[kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    s_tri[wid] = tri_acc;
+    s_bytes[wid] = bytes_acc;
+  }
+  __syncwarp();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0, b = 0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      t += s_tri[w];
+      b += s_bytes[w];
+    }
+    if (t) atomicAdd(tri_out, t);
+    if (b && bytes_out) atomicAdd(bytes_out, b);
+  }
+}
+
+// The triangle delta of the changed edges, one warp per edge (entries e = this rank's shard,
+// warp-strided). An edge whose shorter list is longer than A.split_min (two hubs) would be one
+// warp's serial tail of the whole launch: when A.split_items is set it is queued instead as
+// items of A.chunk entries of its shorter list, which the item pass spreads over all warps (a
+// full queue leaves the edge to this warp). Lane 0 of each warp accumulates the kept triangles
+// and the edge's algorithmic bytes.
 template <int PRED>
-__global__ void __launch_bounds__(kThreads, 6) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
-                                                    unsigned long long* __restrict__ tri_out) {
-  __shared__ unsigned long long s_tri[kThreads / 32];
+__device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __restrict__ pv, const int64_t gw,
+                                              const int64_t nw, unsigned long long& tri_acc,
+                                              unsigned long long& bytes_acc) {
   const int lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
-  unsigned long long tri_acc = 0;
-  for (int64_t e = gw; e < cnt; e += nw) {
+  const int64_t ns = A.nshards > 1 ? A.nshards : 1;
+  for (int64_t e = gw * ns + (ns > 1 ? A.shard : 0); e < cnt; e += nw * ns) {
     int32_t x, y;
     bool count_total;
     if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
@@ -747,8 +788,9 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta(const DeltaArgs A, uint32
     }
     const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
     if (A.cell_filter == -2 || (A.cell_filter >= 0 && P.cell != A.cell_filter)) continue;
-    if (A.split_items && P.la > kDeltaSplit) {
-      const int nch = (P.la + kDeltaChunk - 1) / kDeltaChunk;
+    if (lane == 0 && count_total) bytes_acc += 4ull * (unsigned long long)(lx + ly) + 8ull;
+    if (A.split_items && P.la > A.split_min) {
+      const int nch = (P.la + A.chunk - 1) / A.chunk;
       unsigned long long at = 0;
       if (lane == 0) at = atomicAdd(A.split_cnt, (unsigned long long)nch);
       at = __shfl_sync(kFull, at, 0);
@@ -765,56 +807,113 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta(const DeltaArgs A, uint32
       if (count_total) tri_acc += c;
     }
   }
-  if (lane == 0) s_tri[wid] = tri_acc;
-  __syncwarp();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned long long s = 0;
-    for (int w = 0; w < kThreads / 32; ++w) s += s_tri[w];
-    if (s) atomicAdd(tri_out, s);
-  }
 }
 
 // The queued chunks of the split intersections, one warp per item. An item's edge passed every
-// check of k_delta already; its endpoints' per-vertex updates and the total add up per chunk.
-template <int PRED>
-__global__ void __launch_bounds__(kThreads, 6) k_delta_split(const DeltaArgs A, uint32_t* __restrict__ pv,
-                                                          unsigned long long* __restrict__ tri_out) {
-  __shared__ unsigned long long s_tri[kThreads / 32];
+// check of the entry pass already; its endpoints' per-vertex updates and the total add up per
+// chunk. kCoherent: the items were written by other CTAs of the same launch, so they are read
+// past the (non-coherent) L1.
+template <int PRED, bool kCoherent>
+__device__ __forceinline__ void delta_items(const DeltaArgs& A, uint32_t* __restrict__ pv, const int64_t gw,
+                                            const int64_t nw, unsigned long long& tri_acc) {
   const int lane = threadIdx.x & 31;
-  const int wid = threadIdx.x >> 5;
-  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const int64_t cnt = (int64_t)min(*A.split_cnt, (unsigned long long)kDeltaItems);
-  unsigned long long tri_acc = 0;
-  for (int64_t q = gw; q < cnt; q += nw) {
-    const unsigned long long item = A.split_items[q];
+  const unsigned long long queued = kCoherent ? __ldcg(A.split_cnt) : *A.split_cnt;
+  const int64_t n_items = (int64_t)min(queued, (unsigned long long)kDeltaItems);
+  const int64_t cnt = A.count_dev ? (int64_t)(kCoherent ? __ldcg(A.count_dev) : *A.count_dev) : A.count_host;
+  for (int64_t q = gw; q < n_items; q += nw) {
+    const unsigned long long item = kCoherent ? __ldcg(A.split_items + q) : A.split_items[q];
     if (item == kNoItem) continue;
     const int64_t e = (int64_t)(item >> 24);
     const int32_t k = (int32_t)(item & 0xffffffu);
+    if (e >= cnt) continue;  // only an item of an abandoned pass could hold one
     int32_t x, y;
     bool count_total;
     if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
     const int32_t lx = A.g.len(x), ly = A.g.len(y);
     const int64_t sx = A.g.start(x), sy = A.g.start(y);
     const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
-    const int32_t i0 = k * kDeltaChunk;
+    const int32_t i0 = k * A.chunk;
     if (i0 >= P.la) continue;
-    const uint32_t c = delta_range<PRED>(A, P, i0, min(P.la, i0 + kDeltaChunk), pv);
+    const uint32_t c = delta_range<PRED>(A, P, i0, min(P.la, i0 + A.chunk), pv);
     if (lane == 0 && c) {
       atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
       atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
       if (count_total) tri_acc += c;
     }
   }
-  if (lane == 0) s_tri[wid] = tri_acc;
+}
+
+// Grid-wide barrier of a resident grid, with a bounded wait: each CTA arrives once, then waits
+// until `expected` CTAs have arrived or the bound (spin_ns of device time, at most kSpinMaxIters
+// polls) runs out, in which case it reports kErrTimeout and the call returns false. The acquire
+// load makes the other CTAs' writes before their arrival visible to this CTA.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, const unsigned expected, const unsigned long long spin_ns,
+                                             unsigned* err) {
+  __shared__ int s_ok;
   __syncwarp();
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned long long s = 0;
-    for (int w = 0; w < kThreads / 32; ++w) s += s_tri[w];
-    if (s) atomicAdd(tri_out, s);
+    __threadfence();
+    atomicAdd(bar, 1u);
+    unsigned long long t0;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    int ok = 1;
+    for (unsigned it = 0;; ++it) {
+      unsigned v;
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
+      if (v >= expected) break;
+      unsigned long long t;
+      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+      if (it >= kSpinMaxIters || t - t0 > spin_ns) {
+        atomicOr(err, kErrTimeout);
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    s_ok = ok;
   }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Two launches: the entry pass, then the item pass (the cuStinger-style count, tc_count_batch).
+template <int PRED>
+__global__ void __launch_bounds__(kThreads, 6) k_delta(const DeltaArgs A, uint32_t* __restrict__ pv,
+                                                    unsigned long long* __restrict__ tri_out) {
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long tri_acc = 0, bytes_acc = 0;
+  delta_entries<PRED>(A, pv, gw, nw, tri_acc, bytes_acc);
+  delta_flush(tri_acc, bytes_acc, tri_out, A.bytes_out);
+}
+
+template <int PRED>
+__global__ void __launch_bounds__(kThreads, 6) k_delta_split(const DeltaArgs A, uint32_t* __restrict__ pv,
+                                                          unsigned long long* __restrict__ tri_out) {
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long tri_acc = 0;
+  delta_items<PRED, false>(A, pv, gw, nw, tri_acc);
+  delta_flush(tri_acc, 0ull, tri_out, nullptr);
+}
+
+// One persistent launch (a resident grid, at most the occupancy limit of CTAs per SM): the
+// entry pass, a grid-wide barrier, then the item pass over the chunks every CTA queued. The
+// batch size is read from device memory, so one captured launch serves every batch of a bin. A
+// barrier wait that runs out (the grid was not resident, or a test forces it) sets kErrTimeout
+// and the CTA skips the item pass: the batch's count is then incomplete and the host reports
+// TC_ERR_TIMEOUT.
+template <int PRED>
+__global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, uint32_t* __restrict__ pv,
+                                                          unsigned long long* __restrict__ tri_out) {
+  const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long tri_acc = 0, bytes_acc = 0;
+  delta_entries<PRED>(A, pv, gw, nw, tri_acc, bytes_acc);
+  if (grid_barrier(A.bar, gridDim.x + A.bar_extra, A.spin_ns, A.err))
+    delta_items<PRED, true>(A, pv, gw, nw, tri_acc);
+  delta_flush(tri_acc, bytes_acc, tri_out, A.bytes_out);
 }
 
 // ---- cuStinger-style batch helpers ------------------------------------------------------------
@@ -1069,12 +1168,50 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
   A.search_ratio_x16 = sp.search_ratio_x16;
   A.use_table = sp.use_table;
   A.cell_filter = sp.cell_filter;
+  A.split_min = kDeltaSplit;
+  A.chunk = kDeltaChunk;
+  A.shard = sp.shard;
+  A.nshards = sp.nshards;
+  A.spin_ns = kSpinNs;
   memcpy(A.table, sp.table, sizeof(A.table));
   return A;
 }
 
 int delta_grid() { return device_info().sms * 8; }
 int long_grid() { return device_info().sms * 8; }
+
+// Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
+// more than can be resident at once (its grid barrier needs every CTA running).
+tc_status fused_grid(int ctas_per_sm, int* grid) {
+  constexpr int kMaxDev = 64;
+  static int occ[kMaxDev] = {};
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  if (occ[dev] == 0) {
+    int b = 0;
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_delta_fused<kPredMark>, kThreads, 0));
+    occ[dev] = std::max(1, b);
+  }
+  const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ[dev]) : occ[dev];
+  *grid = device_info().sms * per_sm;
+  return TC_OK;
+}
+
+// The persistent delta kernel of one phase of a batch (deletions: phase 0, insertions: 1) on
+// the batch workspace's counters.
+tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, unsigned long long* tri_out,
+                             int ctas_per_sm, cudaStream_t s) {
+  A.split_items = w.split_items;
+  A.split_cnt = &w.st->n_split[phase];
+  A.bar = &w.st->bar[phase];
+  A.err = &w.st->err;
+  A.bytes_out = &w.st->delta_bytes;
+  int grid = 0;
+  TC_TRY(fused_grid(ctas_per_sm, &grid));
+  k_delta_fused<kPredMark><<<grid, kThreads, 0, s>>>(A, pv, tri_out);
+  return TC_OK;
+}
 
 }  // namespace
 }  // namespace tc
@@ -1152,10 +1289,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.count_dev = &w.st->n_del;
     A.sign = -1;
     A.weight = 2;
-    A.split_items = w.split_items;
-    A.split_cnt = &w.st->n_split[0];
-    k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
-    k_delta_split<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_removed);
+    TC_TRY(launch_delta_fused(A, w, 0, pv_use, &w.st->tri_removed, 0, s));
     k_endpoints<<<gd, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
@@ -1177,10 +1311,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     A.count_dev = &w.st->n_ins;
     A.sign = 1;
     A.weight = 2;
-    A.split_items = w.split_items;
-    A.split_cnt = &w.st->n_split[1];
-    k_delta<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
-    k_delta_split<kPredMark><<<delta_grid(), kThreads, 0, s>>>(A, pv_use, &w.st->tri_added);
+    TC_TRY(launch_delta_fused(A, w, 1, pv_use, &w.st->tri_added, 0, s));
     k_clear_slots<<<grid_for(2 * (int64_t)h.n_ins, kThreads), kThreads, 0, s>>>(w.ins_slot, 2 * (int64_t)h.n_ins,
                                                                                   nullptr, g->mark);
     TC_CUDA_TRY(cudaGetLastError());
@@ -1194,6 +1325,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     TC_CUDA_TRY(cudaStreamSynchronize(s));
     const BatchStatus& f = *w.st_host;
     if (f.err & kErrPool) return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+    if (f.err & kErrTimeout) return fail(TC_ERR_TIMEOUT, "the delta kernel's grid barrier gave up waiting");
     info->updates = b;
     info->inserted = (int64_t)f.n_ins;
     info->deleted = (int64_t)f.n_del;
@@ -1363,19 +1495,37 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
 // one CUDA graph per batch-size bin instead: every launch is sized for the bin's capacity and
 // reads the batch's real counts from device memory (grid-stride loops over device counts, the
 // batch padded with sentinel keys), so a batch is a few copies and one graph launch with no
-// host synchronisation inside. The pool headroom the relocations of one batch can take is
+// host synchronisation inside. The delta count of each phase (deletions, insertions) is one
+// persistent kernel (k_delta_fused). The pool headroom the relocations of one batch can take is
 // bounded ahead (every touched list moving: (m + 2b)(1 + slack) slots) and reserved before the
 // launch, so the device bump allocator cannot run out. The graphs capture the graph's pool and
 // workspace pointers and the caller's per-vertex and delta arrays; they are captured again when
-// any of these change. The autotuner times the candidate grids of the delta kernel per bin on
-// the caller's own batches (tc_pipeline_autotune) and keeps the fastest.
+// any of these change.
+//
+// Autotuner (tc_pipeline_autotune): the bins start as a fine ladder of capacities (2^10, 2^11,
+// ... up to max_batch). Over the next k batches each batch runs under one "arm" of its natural
+// bin (the smallest that holds it): one of the candidate tile shapes of the delta kernel (CTAs
+// per SM, split threshold and split-item size) in that bin's graph, or the default shape in the
+// next bin's graph. Each arm's time per update is measured with events. At the end every bin
+// keeps its fastest shape, and a bin whose batches ran no more than 3 % slower in the next bin's
+// graph is merged into it: its threshold is dropped and its batches use that graph (fewer
+// graphs where padding costs nothing, the fine ladder where it does).
 
 namespace tc {
 namespace {
-constexpr int kPipeBins = 8;
-constexpr int kPipeCands = 4;
-constexpr int kPipeCandBlocks[kPipeCands] = {2, 4, 8, 16};  // delta-kernel CTAs per SM
+constexpr int kPipeBins = 16;
 constexpr int64_t kPipeMinBin = 1 << 10;
+struct PipeCand {
+  int ctas;       // persistent delta kernel CTAs per SM (0 = the occupancy limit)
+  int chunk;      // split-item size: entries of the shorter list
+  int split_min;  // intersections whose shorter list is longer than this are split
+};
+constexpr int kPipeCands = 5;
+constexpr PipeCand kPipeCand[kPipeCands] = {
+    {0, kDeltaChunk, kDeltaSplit}, {4, kDeltaChunk, kDeltaSplit}, {2, kDeltaChunk, kDeltaSplit},
+    {0, kDeltaChunk / 2, kDeltaSplit / 2}, {0, kDeltaChunk * 2, kDeltaSplit * 2}};
+constexpr int kPipeArms = kPipeCands + 1;  // + the default shape in the next bin's graph
+constexpr double kMergeSlack = 1.03;
 }  // namespace
 }  // namespace tc
 
@@ -1385,13 +1535,13 @@ struct tc_pipeline {
   int64_t b_max = 0;
   int nbins = 0;
   int64_t bin_cap[tc::kPipeBins] = {};
-  int cand[tc::kPipeBins] = {};                      // chosen delta-grid candidate per bin
+  int cand[tc::kPipeBins] = {};                      // chosen tile-shape candidate per bin
+  int serve[tc::kPipeBins] = {};                     // bin whose graph runs this bin's batches
   cudaGraphExec_t exec[tc::kPipeBins][tc::kPipeCands] = {};
-  // autotuning: per bin and candidate, accumulated ms per update and samples
-  double tune_ms_per_update[tc::kPipeBins][tc::kPipeCands] = {};
-  int tune_n[tc::kPipeBins][tc::kPipeCands] = {};
+  // autotuning: per natural bin and arm, accumulated ms per update and samples
+  double tune_ms_per_update[tc::kPipeBins][tc::kPipeArms] = {};
+  int tune_n[tc::kPipeBins][tc::kPipeArms] = {};
   int tune_left = 0;                                 // batches still spent exploring
-  int tune_reps = 0;
   // what the captured graphs hold
   const void* key_pool = nullptr;
   const void* key_mark = nullptr;
@@ -1400,6 +1550,8 @@ struct tc_pipeline {
   uint64_t key_ws = 0;
   int64_t key_pool_cap = 0;
   tc::SchedParams sp;
+  unsigned long long spin_ns = tc::kSpinNs;          // bound of the delta kernel's barrier wait
+  unsigned bar_extra = 0;                            // (test hook: arrivals that never come)
   cudaStream_t cs = nullptr;     // capture stream
   int64_t* d_b = nullptr;
   int64_t* h_b = nullptr;        // pinned
@@ -1408,8 +1560,13 @@ struct tc_pipeline {
   uint32_t* pv_scratch = nullptr;
   int64_t* delta_scratch = nullptr;
   cudaEvent_t done = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t pev[4] = {};       // profiling: around the two delta kernels, inside the graphs
+  bool profile = false;
+  int64_t prof_batches = 0;
+  double prof_delta_ms = 0.0;
+  int64_t prof_delta_bytes = 0;
   bool pending = false;
-  int pending_bin = -1, pending_cand = -1;
+  int pending_bin = -1, pending_cand = -1, pending_arm = -1, pending_nat = -1;
   int64_t pending_b = 0;
   bool timing = false;
   tc_batch_info last{};
@@ -1447,10 +1604,18 @@ tc_status pipe_settle(tc_pipeline* p) {
   if (p->timing) {
     float ms = 0.f;
     TC_CUDA_TRY(cudaEventElapsedTime(&ms, p->t0, p->t1));
-    const int bi = p->pending_bin, cj = p->pending_cand;
-    p->tune_ms_per_update[bi][cj] += (double)ms / (double)std::max<int64_t>(p->pending_b, 1);
-    p->tune_n[bi][cj] += 1;
+    const int bi = p->pending_nat, a = p->pending_arm;
+    p->tune_ms_per_update[bi][a] += (double)ms / (double)std::max<int64_t>(p->pending_b, 1);
+    p->tune_n[bi][a] += 1;
     p->timing = false;
+  }
+  if (p->profile) {
+    float d0 = 0.f, d1 = 0.f;
+    TC_CUDA_TRY(cudaEventElapsedTime(&d0, p->pev[0], p->pev[1]));
+    TC_CUDA_TRY(cudaEventElapsedTime(&d1, p->pev[2], p->pev[3]));
+    p->prof_batches += 1;
+    p->prof_delta_ms += (double)d0 + (double)d1;
+    p->prof_delta_bytes += (int64_t)f.delta_bytes;
   }
   if (f.err & kErrRange) {
     p->last.status = TC_ERR_INVALID_ARG;
@@ -1459,6 +1624,10 @@ tc_status pipe_settle(tc_pipeline* p) {
   if (f.err & kErrPool) {
     p->last.status = TC_ERR_CAPACITY;
     return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+  }
+  if (f.err & kErrTimeout) {
+    p->last.status = TC_ERR_TIMEOUT;
+    return fail(TC_ERR_TIMEOUT, "the delta kernel's grid barrier gave up waiting; the batch's count is incomplete");
   }
   return TC_OK;
 }
@@ -1484,11 +1653,13 @@ void pipe_check_keys(tc_pipeline* p, const void* pv, const void* delta) {
   }
 }
 
-// Record the whole batch pipeline for a bin of capacity cap on the capture stream.
+// Record the whole batch pipeline for a bin of capacity cap, with tile shape `cand`, on the
+// capture stream.
 tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t* delta) {
   tc_graph* g = p->g;
   StreamWs& w = *g->sw;
   const int64_t cap = p->bin_cap[bin];
+  const PipeCand& pc = kPipeCand[cand];
   cudaStream_t s = p->cs;
   const int L = bits_for(std::max(g->n, 2));
   const uint64_t sent = (1ull << (2 * L + 1)) - 1;
@@ -1496,7 +1667,8 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
   const int gb = grid_for(cap, kThreads);
   const int g2 = grid_for(2 * cap, kThreads);
   const int gw = grid_for(2 * cap * 32, kThreads);
-  const int gdelta = device_info().sms * kPipeCandBlocks[cand];
+  int gdelta = 0;
+  TC_TRY(fused_grid(pc.ctas, &gdelta));
   cudaGraph_t graph = nullptr;
   TC_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
@@ -1520,10 +1692,18 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.count_dev = &w.st->n_del;
     A.sign = -1;
     A.weight = 2;
+    A.chunk = pc.chunk;
+    A.split_min = pc.split_min;
+    A.spin_ns = p->spin_ns;
+    A.bar_extra = p->bar_extra;
     A.split_items = w.split_items;
     A.split_cnt = &w.st->n_split[0];
-    k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
-    k_delta_split<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
+    A.bar = &w.st->bar[0];
+    A.err = &w.st->err;
+    A.bytes_out = &w.st->delta_bytes;
+    if (p->profile) cudaEventRecordWithFlags(p->pev[0], s, cudaEventRecordExternal);
+    k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
+    if (p->profile) cudaEventRecordWithFlags(p->pev[1], s, cudaEventRecordExternal);
     k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
@@ -1536,15 +1716,16 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, 2 * cap, w.long_runs, g->start, g->used, g->cap, g->pool,
                                                     g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
                                                     w.st);
-    DeltaArgs B = delta_args(g, p->sp);
+    DeltaArgs B = A;
+    B.dlist = nullptr;
     B.ilist = w.ilist;
     B.count_dev = &w.st->n_ins;
     B.sign = 1;
-    B.weight = 2;
-    B.split_items = w.split_items;
     B.split_cnt = &w.st->n_split[1];
-    k_delta<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
-    k_delta_split<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
+    B.bar = &w.st->bar[1];
+    if (p->profile) cudaEventRecordWithFlags(p->pev[2], s, cudaEventRecordExternal);
+    k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
+    if (p->profile) cudaEventRecordWithFlags(p->pev[3], s, cudaEventRecordExternal);
     k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);
     k_add_delta<<<1, 32, 0, s>>>(delta, &w.st->tri_added, &w.st->tri_removed);
     cudaMemcpyAsync(p->h_st, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s);
@@ -1562,6 +1743,40 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
   return TC_OK;
 }
 
+// End of the exploration: the fastest shape per bin, then the merges (top bin down, so a chain
+// of merged bins resolves to the graph that serves the highest of them).
+void pipe_finish_tuning(tc_pipeline* p) {
+  for (int i = 0; i < p->nbins; ++i) {
+    int best = p->cand[i];
+    double best_v = 0.0;
+    for (int j = 0; j < kPipeCands; ++j) {
+      if (p->tune_n[i][j] < 1) continue;
+      const double v = p->tune_ms_per_update[i][j] / p->tune_n[i][j];
+      if (best_v == 0.0 || v < best_v) {
+        best_v = v;
+        best = j;
+      }
+    }
+    p->cand[i] = best;
+  }
+  p->serve[p->nbins - 1] = p->nbins - 1;
+  for (int i = p->nbins - 2; i >= 0; --i) {
+    p->serve[i] = i;
+    const int own = 0, up = kPipeCands;
+    if (p->tune_n[i][own] > 0 && p->tune_n[i][up] > 0) {
+      const double v_own = p->tune_ms_per_update[i][own] / p->tune_n[i][own];
+      const double v_up = p->tune_ms_per_update[i][up] / p->tune_n[i][up];
+      if (v_up <= kMergeSlack * v_own) p->serve[i] = p->serve[i + 1];
+    }
+  }
+}
+
+int pipe_natural_bin(const tc_pipeline* p, int64_t b) {
+  int bin = 0;
+  while (bin + 1 < p->nbins && p->bin_cap[bin] < b) ++bin;
+  return bin;
+}
+
 }  // namespace
 }  // namespace tc
 
@@ -1575,12 +1790,26 @@ tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sch
   p->g = g;
   p->sp = to_params(sched);
   TC_CUDA_TRY(cudaGetDevice(&p->device));
-  for (int64_t c = kPipeMinBin; p->nbins < kPipeBins; c *= 4) {
+  // fine ladder: 2^10, 2^11, ... (the last bin holds max_batch; past kPipeBins bins the ladder
+  // doubles its step)
+  int64_t step = 2;
+  {
+    int64_t levels = 1;
+    for (int64_t c = kPipeMinBin; c < max_batch; c *= 2) ++levels;
+    while (levels > kPipeBins) {
+      step *= 2;
+      levels = (levels + 1) / 2;
+    }
+  }
+  for (int64_t c = kPipeMinBin; p->nbins < kPipeBins; c *= step) {
     p->bin_cap[p->nbins++] = std::min(c, std::max(max_batch, kPipeMinBin));
     if (c >= max_batch) break;
   }
   p->b_max = p->bin_cap[p->nbins - 1];
-  for (int i = 0; i < kPipeBins; ++i) p->cand[i] = 2;  // 8 CTAs per SM until tuned
+  for (int i = 0; i < kPipeBins; ++i) {
+    p->cand[i] = 0;
+    p->serve[i] = i;
+  }
   tc_status rc = TC_OK;
   do {
     if ((rc = ensure_stream_ws(g, p->b_max)) != TC_OK) break;
@@ -1592,7 +1821,9 @@ tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sch
         cudaMalloc(&p->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
         cudaMalloc(&p->delta_scratch, sizeof(int64_t)) != cudaSuccess ||
         cudaEventCreate(&p->done) != cudaSuccess || cudaEventCreate(&p->t0) != cudaSuccess ||
-        cudaEventCreate(&p->t1) != cudaSuccess) {
+        cudaEventCreate(&p->t1) != cudaSuccess || cudaEventCreate(&p->pev[0]) != cudaSuccess ||
+        cudaEventCreate(&p->pev[1]) != cudaSuccess || cudaEventCreate(&p->pev[2]) != cudaSuccess ||
+        cudaEventCreate(&p->pev[3]) != cudaSuccess) {
       rc = fail(TC_ERR_OOM, "pipeline: allocation failed");
       break;
     }
@@ -1622,6 +1853,8 @@ tc_status tc_pipeline_destroy(tc_pipeline* p) {
   if (p->done) cudaEventDestroy(p->done);
   if (p->t0) cudaEventDestroy(p->t0);
   if (p->t1) cudaEventDestroy(p->t1);
+  for (int i = 0; i < 4; ++i)
+    if (p->pev[i]) cudaEventDestroy(p->pev[i]);
   delete p;
   return TC_OK;
 }
@@ -1648,14 +1881,18 @@ tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t*
   int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
   StreamWs& w = *g->sw;
   pipe_check_keys(p, pv, delta);
-  int bin = 0;
-  while (p->bin_cap[bin] < b) ++bin;
+  const int nat = pipe_natural_bin(p, b);
+  int bin = p->serve[nat];
   int cand = p->cand[bin];
+  int arm = -1;
   if (p->tune_left > 0) {
-    // explore: the candidate with the fewest samples in this bin
-    cand = 0;
-    for (int j = 1; j < kPipeCands; ++j)
-      if (p->tune_n[bin][j] < p->tune_n[bin][cand]) cand = j;
+    // explore: the arm of this natural bin with the fewest samples
+    arm = 0;
+    const int narms = nat + 1 < p->nbins ? kPipeArms : kPipeCands;
+    for (int j = 1; j < narms; ++j)
+      if (p->tune_n[nat][j] < p->tune_n[nat][arm]) arm = j;
+    bin = arm < kPipeCands ? nat : nat + 1;
+    cand = arm < kPipeCands ? arm : 0;
   }
   if (!p->exec[bin][cand]) TC_TRY(pipe_capture(p, bin, cand, pv, delta));
   // the batch into the capacity-sized buffers the graph reads
@@ -1665,7 +1902,7 @@ tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t*
   else TC_CUDA_TRY(cudaMemsetAsync(w.isdel, 0, b, s));
   *p->h_b = b;
   TC_CUDA_TRY(cudaMemcpyAsync(p->d_b, p->h_b, sizeof(int64_t), cudaMemcpyHostToDevice, s));
-  p->timing = p->tune_left > 0;
+  p->timing = arm >= 0;
   if (p->timing) TC_CUDA_TRY(cudaEventRecord(p->t0, s));
   TC_CUDA_TRY(cudaGraphLaunch(p->exec[bin][cand], s));
   if (p->timing) TC_CUDA_TRY(cudaEventRecord(p->t1, s));
@@ -1673,23 +1910,13 @@ tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t*
   p->pending = true;
   p->pending_bin = bin;
   p->pending_cand = cand;
+  p->pending_arm = arm;
+  p->pending_nat = nat;
   p->pending_b = b;
   if (p->tune_left > 0 && --p->tune_left == 0) {
-    // exploration over: settle the last sample, keep the fastest candidate per bin
+    // exploration over: settle the last sample, keep the fastest shape per bin, merge bins
     TC_TRY(pipe_settle(p));
-    for (int i = 0; i < p->nbins; ++i) {
-      int best = p->cand[i];
-      double best_v = 0.0;
-      for (int j = 0; j < kPipeCands; ++j) {
-        if (p->tune_n[i][j] < 1) continue;
-        const double v = p->tune_ms_per_update[i][j] / p->tune_n[i][j];
-        if (best_v == 0.0 || v < best_v) {
-          best_v = v;
-          best = j;
-        }
-      }
-      p->cand[i] = best;
-    }
+    pipe_finish_tuning(p);
   }
   return TC_OK;
 }
@@ -1704,8 +1931,10 @@ tc_status tc_pipeline_prepare(tc_pipeline* p, int32_t* per_vertex, int64_t* delt
   uint32_t* pv = per_vertex ? reinterpret_cast<uint32_t*>(per_vertex) : p->pv_scratch;
   int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
   pipe_check_keys(p, pv, delta);
-  for (int i = 0; i < p->nbins; ++i)
-    if (!p->exec[i][p->cand[i]]) TC_TRY(pipe_capture(p, i, p->cand[i], pv, delta));
+  for (int i = 0; i < p->nbins; ++i) {
+    const int bin = p->serve[i];
+    if (!p->exec[bin][p->cand[bin]]) TC_TRY(pipe_capture(p, bin, p->cand[bin], pv, delta));
+  }
   return TC_OK;
 }
 
@@ -1718,8 +1947,10 @@ tc_status tc_pipeline_sync(tc_pipeline* p, tc_batch_info* last) {
 
 tc_status tc_pipeline_autotune(tc_pipeline* p, int32_t batches) {
   if (!p || batches < 0) return fail(TC_ERR_INVALID_ARG, "invalid autotune arguments");
+  TC_TRY(pipe_settle(p));
   memset(p->tune_ms_per_update, 0, sizeof(p->tune_ms_per_update));
   memset(p->tune_n, 0, sizeof(p->tune_n));
+  for (int i = 0; i < kPipeBins; ++i) p->serve[i] = i;
   p->tune_left = batches;
   return TC_OK;
 }
@@ -1728,9 +1959,83 @@ tc_status tc_pipeline_info(const tc_pipeline* p, int32_t* nbins, int64_t* bin_ca
   if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
   if (nbins) *nbins = p->nbins;
   for (int i = 0; i < p->nbins; ++i) {
+    const int bin = p->serve[i];
     if (bin_cap) bin_cap[i] = p->bin_cap[i];
-    if (delta_blocks_per_sm) delta_blocks_per_sm[i] = kPipeCandBlocks[p->cand[i]];
+    if (delta_blocks_per_sm) {
+      int grid = 0;
+      if (fused_grid(kPipeCand[p->cand[bin]].ctas, &grid) != TC_OK) return TC_ERR_CUDA;
+      delta_blocks_per_sm[i] = grid / device_info().sms;
+    }
   }
+  return TC_OK;
+}
+
+tc_status tc_pipeline_plan_get(const tc_pipeline* p, tc_pipeline_plan* plan) {
+  if (!p || !plan) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  memset(plan, 0, sizeof(*plan));
+  plan->nbins = p->nbins;
+  for (int i = 0; i < p->nbins; ++i) {
+    const PipeCand& c = kPipeCand[p->cand[p->serve[i]]];
+    plan->bin_cap[i] = p->bin_cap[i];
+    plan->serve[i] = p->serve[i];
+    plan->ctas_per_sm[i] = c.ctas;
+    plan->chunk[i] = c.chunk;
+    plan->split_min[i] = c.split_min;
+  }
+  return TC_OK;
+}
+
+tc_status tc_pipeline_plan_set(tc_pipeline* p, const tc_pipeline_plan* plan) {
+  if (!p || !plan) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
+  if (plan->nbins != p->nbins) return fail(TC_ERR_INVALID_ARG, "plan has %d bins, the pipeline %d", plan->nbins, p->nbins);
+  int cand[kPipeBins], serve[kPipeBins];
+  for (int i = 0; i < p->nbins; ++i) {
+    if (plan->bin_cap[i] != p->bin_cap[i]) return fail(TC_ERR_INVALID_ARG, "plan bin %d capacity differs", i);
+    if (plan->serve[i] < i || plan->serve[i] >= p->nbins || (i > 0 && plan->serve[i] < plan->serve[i - 1]))
+      return fail(TC_ERR_INVALID_ARG, "plan bin %d is served by bin %d", i, plan->serve[i]);
+    cand[i] = -1;
+    for (int j = 0; j < kPipeCands; ++j)
+      if (kPipeCand[j].ctas == plan->ctas_per_sm[i] && kPipeCand[j].chunk == plan->chunk[i] &&
+          kPipeCand[j].split_min == plan->split_min[i])
+        cand[i] = j;
+    if (cand[i] < 0) return fail(TC_ERR_INVALID_ARG, "plan bin %d: tile shape is not one of the candidates", i);
+    serve[i] = plan->serve[i];
+  }
+  TC_TRY(pipe_settle(p));
+  for (int i = 0; i < p->nbins; ++i) {
+    p->serve[i] = serve[i];
+    p->cand[serve[i]] = cand[i];
+  }
+  p->tune_left = 0;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_profile(tc_pipeline* p, int on) {
+  if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
+  TC_TRY(pipe_settle(p));
+  if ((on != 0) != p->profile) drop_graphs(p);  // the event records live inside the graphs
+  p->profile = on != 0;
+  p->prof_batches = 0;
+  p->prof_delta_ms = 0.0;
+  p->prof_delta_bytes = 0;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_stats(tc_pipeline* p, int64_t* batches, double* delta_ms, int64_t* delta_bytes) {
+  if (!p) return fail(TC_ERR_INVALID_ARG, "pipeline is NULL");
+  TC_TRY(pipe_settle(p));
+  if (batches) *batches = p->prof_batches;
+  if (delta_ms) *delta_ms = p->prof_delta_ms;
+  if (delta_bytes) *delta_bytes = p->prof_delta_bytes;
+  return TC_OK;
+}
+
+tc_status tc_pipeline_set_wait_bound(tc_pipeline* p, uint64_t wait_ns, int32_t extra_arrivals) {
+  if (!p || wait_ns == 0 || extra_arrivals < 0) return fail(TC_ERR_INVALID_ARG, "invalid wait bound");
+  TC_TRY(pipe_settle(p));
+  p->spin_ns = wait_ns;
+  p->bar_extra = (unsigned)extra_arrivals;
+  drop_graphs(p);  // the bound is an argument of the captured launches
   return TC_OK;
 }
 

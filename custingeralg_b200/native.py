@@ -51,7 +51,8 @@ class Sched(ctypes.Structure):
 
 class CountInfo(ctypes.Structure):
     _fields_ = [("triangles", _i64), ("edges_intersected", _i64), ("oriented_work", _i64),
-                ("max_out_degree", _i32), ("status", _i32)]
+                ("max_out_degree", _i32), ("status", _i32), ("shard_lo", _i32), ("shard_hi", _i32),
+                ("shard_work", _i64), ("total_work", _i64)]
 
 
 class PhaseTimes(ctypes.Structure):
@@ -61,6 +62,11 @@ class PhaseTimes(ctypes.Structure):
 class BatchInfo(ctypes.Structure):
     _fields_ = [("updates", _i64), ("inserted", _i64), ("deleted", _i64), ("ignored", _i64),
                 ("triangles_added", _i64), ("triangles_removed", _i64), ("status", _i32)]
+
+
+class PipelinePlan(ctypes.Structure):
+    _fields_ = [("nbins", _i32), ("bin_cap", _i64 * 16), ("serve", _i32 * 16), ("ctas_per_sm", _i32 * 16),
+                ("chunk", _i32 * 16), ("split_min", _i32 * 16)]
 
 
 class TcError(RuntimeError):
@@ -89,6 +95,7 @@ SIGNATURES = {
     "tc_count_csr64": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
                                       ctypes.POINTER(Sched), _P]),
     "tc_workspace_status": (ctypes.c_int, [_P, ctypes.POINTER(CountInfo)]),
+    "tc_shard_ranges": (ctypes.c_int, [_P, _i32, _i32, _P]),
     "tc_count_csr32_noalloc": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
                                               ctypes.POINTER(Sched), _P]),
     "tc_apply_batch": (ctypes.c_int, [_P, _P, _P, _P, _i64, ctypes.c_int, _P, _P, ctypes.POINTER(BatchInfo),
@@ -116,6 +123,12 @@ SIGNATURES = {
     "tc_pipeline_sync": (ctypes.c_int, [_P, ctypes.POINTER(BatchInfo)]),
     "tc_pipeline_autotune": (ctypes.c_int, [_P, _i32]),
     "tc_pipeline_info": (ctypes.c_int, [_P, _P, _P, _P]),
+    "tc_pipeline_plan_get": (ctypes.c_int, [_P, _P]),
+    "tc_pipeline_plan_set": (ctypes.c_int, [_P, _P]),
+    "tc_pipeline_profile": (ctypes.c_int, [_P, ctypes.c_int]),
+    "tc_pipeline_stats": (ctypes.c_int, [_P, ctypes.POINTER(_i64), ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(_i64)]),
+    "tc_pipeline_set_wait_bound": (ctypes.c_int, [_P, ctypes.c_uint64, _i32]),
     "tc_pipeline_destroy": (ctypes.c_int, [_P]),
     "tc_profile_enable": (ctypes.c_int, [ctypes.c_int]),
     "tc_profile_last": (ctypes.c_int, [ctypes.POINTER(PhaseTimes)]),

@@ -72,8 +72,12 @@ typedef struct tc_sched {
                              out-degree, b = the other endpoint's): 0 = the warp streams N+(b)
                              through the hash set, 1 = one lane walks it, 2 = packed (see
                              packed_max_deg). Streaming: 0 = search, 1 = merge */
-  int32_t shard;          /* count only the edges whose centre c has c % nshards == shard */
-  int32_t nshards;        /* (multi-GPU work split; 1 = everything) */
+  int32_t shard;          /* multi-GPU work split (1 = everything): this call counts shard `shard` of */
+  int32_t nshards;        /* `nshards`. Static count: a contiguous range of edge centres, the ranges
+                             balanced by each centre's predicted intersection work (every rank
+                             computes the same ranges from the same graph). Streaming: the changed
+                             edges e with e % nshards == shard. Per-vertex outputs and totals are
+                             then partial sums that add up over the shards. */
   int32_t cell_filter;    /* timing mode for scheduler training: -1 = intersect every edge (normal),
                              -2 = none, c >= 0 = only edges of degree cell c (16*log2 d_a + log2 d_b);
                              counts are partial unless -1 */
@@ -118,6 +122,10 @@ typedef struct tc_count_info {
   int32_t max_out_degree;    /* max d+ in the degree orientation */
   int32_t status;            /* structural check made during the count: TC_OK,
                                 TC_ERR_BAD_GRAPH or TC_ERR_NOT_SYMMETRIC */
+  int32_t shard_lo;          /* sharded count (sched->nshards > 1): the centres [shard_lo, shard_hi) */
+  int32_t shard_hi;          /* it counted (0, -1 when not sharded); */
+  int64_t shard_work;        /* their predicted work and that of all centres (units of 16 probes) */
+  int64_t total_work;
 } tc_count_info;
 
 /* Static count over a graph handle.
@@ -146,21 +154,27 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
 
 /* Allocation-free variant of tc_count_csr32 (no counterpart in the reference): same inputs,
  * outputs and conventions, but it never calls cudaMalloc or cudaFree. It is for callers that
- * cannot allocate device memory at count time: code running inside a captured CUDA graph
- * region, processes whose allocator forbids device allocation after start-up, or services
- * that budget every byte of device memory up front. Its working memory is a fixed array inside
- * this library's device image, sized for at most TC_NOALLOC_MAX_NV vertices and
- * TC_NOALLOC_MAX_EDGES directed edges (about 49 MB, held by every GPU that loads the library
- * until the process exits); larger graphs are rejected with TC_ERR_CAPACITY. All calls share
- * that array, so calls that overlap on the GPU race: issue them on one stream or order them
- * with events. The first call on a device looks up the array's device address with that
- * device current; make it before any stream capture. The edge count d_off[nv] is read back to
- * the host, so the call synchronises `stream` once. */
+ * must not allocate device memory when they count: processes whose device memory is owned by
+ * another allocator (a framework's caching pool) or reserved in full at start-up, and
+ * latency-sensitive loops, where cudaMalloc and cudaFree can synchronise the device. Its working
+ * memory is a fixed array inside this library's device image, sized for at most
+ * TC_NOALLOC_MAX_NV vertices and TC_NOALLOC_MAX_EDGES directed edges (about 48.6 MiB, held by
+ * every GPU that loads the library until the process exits); larger graphs are rejected with
+ * TC_ERR_CAPACITY, and a sharded count (sched->nshards > 1) with TC_ERR_INVALID_ARG. All calls
+ * share that array and keep the last call's contents (each call clears what must start at zero),
+ * so calls that overlap on the GPU race: issue them on one stream or order them with events. The
+ * first call on a device looks up the array's device address with that device current. The edge
+ * count d_off[nv] is read back to the host, so the call synchronises `stream` once. */
 #define TC_NOALLOC_MAX_NV (1 << 20)
 #define TC_NOALLOC_MAX_EDGES (1 << 22)
 tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode,
                                  int32_t* per_vertex, int64_t* triangles_dev, tc_count_info* info,
                                  const tc_sched* sched, void* stream);
+
+/* The multi-GPU split rule of the static count on the host: lo[r] = first centre of shard r of
+ * nshards (lo[0] = 0, lo[nshards] = n) given prefix[0..n], the exclusive prefix of the centres'
+ * predicted work. The device applies the same rule to its own prefix. */
+tc_status tc_shard_ranges(const int64_t* prefix_host, int32_t n, int32_t nshards, int32_t* lo_host);
 
 /* Read back the info of the last stateless count on the current device. Syncs `stream`. */
 tc_status tc_workspace_status(void* stream, tc_count_info* info);
@@ -216,10 +230,13 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  * three streaming kernels one by one per batch, cct_upd.cu:412-440) ------------------------------
  *
  * The same semantics as tc_apply_batch for device batches, as one CUDA graph launch per batch
- * with no host synchronisation inside it. Batches are binned by size (capacities 2^10, 2^12, ...
- * up to max_batch); each bin's graph is captured on first use with launches sized for the bin
- * and reads the batch's counts on the device. Pool headroom for the worst case of a batch (every
- * list it touches relocating) is reserved before each launch.
+ * with no host synchronisation inside it. Batches are binned by size (capacities 2^10, 2^11, ...
+ * up to max_batch, until the autotuner merges bins); each bin's graph is captured on first use
+ * with launches sized for the bin and reads the batch's counts on the device. The triangle
+ * delta of each phase of a batch (deletions, insertions) is one persistent kernel over a
+ * resident grid: the per-edge pass, a grid-wide barrier with a bounded wait, then the queued
+ * chunks of hub-hub intersections. Pool headroom for the worst case of a batch (every list it
+ * touches relocating) is reserved before each launch.
  *
  * tc_pipeline_create: for batches of at most max_batch updates on graph g (the graph must not be
  *                     updated through other calls while the pipeline has a batch in flight).
@@ -230,11 +247,35 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  *                     previous batch is settled first (its status folded into the graph).
  * tc_pipeline_prepare: reserve pool headroom for max_batch and capture every bin's graph for these
  *                     outputs now (optional; otherwise both happen on first use).
- * tc_pipeline_sync:   wait for the last batch and report it (errors of that batch surface here).
- * tc_pipeline_autotune: time the next `batches` batches under the candidate grids of the delta
- *                     kernel per bin (2, 4, 8, 16 CTAs per SM) and keep the fastest per bin.
- * tc_pipeline_info:   bins, their capacities and the delta-kernel CTAs per SM each uses. */
+ * tc_pipeline_sync:   wait for the last batch and report it (errors of that batch surface here;
+ *                     TC_ERR_TIMEOUT when a delta kernel's barrier wait ran out).
+ * tc_pipeline_autotune: explore over the next `batches` batches: each runs under one arm of its
+ *                     natural bin, a candidate tile shape of the delta kernel (CTAs per SM: the
+ *                     occupancy limit, 4 or 2; split threshold / split-item size 2048/1024,
+ *                     1024/512 or 4096/2048 entries) or the default shape in the next bin's graph,
+ *                     timed with events. Afterwards each bin keeps its fastest shape, and a bin
+ *                     whose batches ran at most 3 % slower in the next bin's graph is merged into
+ *                     it (its threshold dropped).
+ * tc_pipeline_info:   bins, their capacities and the delta-kernel CTAs per SM each uses.
+ * tc_pipeline_plan_get / _set: the tuned bins and shapes, to carry a tuning over to another
+ *                     pipeline with the same max_batch (e.g. tuned on a copy of the graph).
+ * tc_pipeline_profile: record events around the two delta kernels inside the captured graphs
+ *                     (drops the graphs when it changes; call before tc_pipeline_prepare) and
+ *                     count their algorithmic bytes, sum over changed edges {x,y} of
+ *                     4 (deg x + deg y) + 8; tc_pipeline_stats returns the totals since.
+ * tc_pipeline_set_wait_bound: the bound of the delta kernels' barrier wait (default 2 s) and a
+ *                     number of arrivals it waits for beyond the grid (0 normally; a test gives 1
+ *                     to make every wait run out and checks that the batch reports
+ *                     TC_ERR_TIMEOUT with the device still usable). Drops the captured graphs. */
 typedef struct tc_pipeline tc_pipeline;
+typedef struct tc_pipeline_plan {
+  int32_t nbins;
+  int64_t bin_cap[16];     /* bin capacities (the fine ladder) */
+  int32_t serve[16];       /* bin whose graph runs the batches of bin i (>= i; > i where merged) */
+  int32_t ctas_per_sm[16]; /* delta kernel shape of that graph: CTAs per SM (0 = occupancy limit), */
+  int32_t chunk[16];       /* split-item size and */
+  int32_t split_min[16];   /* split threshold (entries of the shorter list) */
+} tc_pipeline_plan;
 tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sched, tc_pipeline** out);
 tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t* d_dst, const uint8_t* d_is_delete,
                             int64_t b, int32_t* per_vertex, int64_t* delta_dev, void* stream);
@@ -242,6 +283,11 @@ tc_status tc_pipeline_prepare(tc_pipeline* p, int32_t* per_vertex, int64_t* delt
 tc_status tc_pipeline_sync(tc_pipeline* p, tc_batch_info* last);
 tc_status tc_pipeline_autotune(tc_pipeline* p, int32_t batches);
 tc_status tc_pipeline_info(const tc_pipeline* p, int32_t* nbins, int64_t* bin_cap, int32_t* delta_blocks_per_sm);
+tc_status tc_pipeline_plan_get(const tc_pipeline* p, tc_pipeline_plan* plan);
+tc_status tc_pipeline_plan_set(tc_pipeline* p, const tc_pipeline_plan* plan);
+tc_status tc_pipeline_profile(tc_pipeline* p, int on);
+tc_status tc_pipeline_stats(tc_pipeline* p, int64_t* batches, double* delta_ms, int64_t* delta_bytes);
+tc_status tc_pipeline_set_wait_bound(tc_pipeline* p, uint64_t wait_ns, int32_t extra_arrivals);
 tc_status tc_pipeline_destroy(tc_pipeline* p);
 
 /* Per degree-cell statistics of the oriented edges of the last static count, filed as the count

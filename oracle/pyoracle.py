@@ -45,6 +45,10 @@ def lib():
         L.oracle_fast_count.argtypes = [i32, _P, _P, ctypes.c_int, _P, _P]
         L.oracle_fast_count_shard.argtypes = [i32, _P, _P, ctypes.c_int, i32, i32, _P, _P]
         L.oracle_fast_count_shard.restype = None
+        L.oracle_fast_count_range.argtypes = [i32, _P, _P, ctypes.c_int, i32, i32, _P, _P]
+        L.oracle_fast_count_range.restype = None
+        L.oracle_centre_cost.argtypes = [i32, _P, _P, ctypes.c_int, _P]
+        L.oracle_centre_cost.restype = None
         L.oracle_host_count_sample.argtypes = [i32, _P, _P, _P, i32, ctypes.c_int]
         L.oracle_host_count_sample.restype = i64
         for f in ("oracle_host_count_triangles", "oracle_static_per_vertex", "oracle_csr_per_vertex",
@@ -74,6 +78,8 @@ def ref():
         L.ref_host_count_triangles_omp.restype = ctypes.c_int64
         L.ref_host_count_triangles_omp_sample.argtypes = [i32, _P, _P, _P, i32, ctypes.c_int]
         L.ref_host_count_triangles_omp_sample.restype = ctypes.c_int64
+        L.ref_host_count_triangles_omp_pervertex.argtypes = [i32, _P, _P, _P, _P, ctypes.c_int]
+        L.ref_host_count_triangles_omp_pervertex.restype = ctypes.c_int64
         _ref = L
     return _ref
 
@@ -193,6 +199,22 @@ def ref_host_count_triangles_omp(n, off, ind, nthreads=0):
     return int(ref().ref_host_count_triangles_omp(n, _ptr(off32), _ptr(ind), nthreads))
 
 
+def ref_host_count_triangles_pervertex(n, off, ind, nthreads=0):
+    """The reference's hostSingleIntersection over every directed edge, each edge's count (its
+    triNE entry, tests/cct.cpp:71-89) summed into its source vertex. Returns (6T, int64 2t(v) per
+    vertex, int64 forward count per vertex: the sum over edges with dest > src only, the raw-CSR
+    GPU counter's convention, tests/cct_csr.cu:246-249)."""
+    off32 = np.ascontiguousarray(off, dtype=np.int32)
+    ind = np.ascontiguousarray(ind, dtype=np.int32)
+    if ind.size == 0:
+        ind = np.zeros(1, np.int32)
+    pv = np.zeros(max(n, 1), np.int64)
+    fw = np.zeros(max(n, 1), np.int64)
+    tot = int(ref().ref_host_count_triangles_omp_pervertex(n, _ptr(off32), _ptr(ind), _ptr(pv), _ptr(fw),
+                                                           nthreads))
+    return tot, pv[:n], fw[:n]
+
+
 def ref_host_count_triangles_omp_sample(n, off32, ind, verts, nthreads=0):
     """The reference's per-edge intersections for the source vertices in `verts` only."""
     off32 = np.ascontiguousarray(off32, dtype=np.int32)
@@ -220,3 +242,20 @@ def fast_count_shard(n, off, ind, shard, nshards, nthreads=0):
     pv = np.zeros(max(n, 1), np.int32)
     lib().oracle_fast_count_shard(n, _ptr(off), _ptr(ind), nthreads, shard, nshards, _ptr(tot), _ptr(pv))
     return int(tot[0]), pv[:n]
+
+
+def fast_count_range(n, off, ind, lo, hi, nthreads=0):
+    """Total (6T share) and per-vertex counts of the centres in [lo, hi) (a contiguous shard)."""
+    off, ind = _g(off, ind)
+    tot = np.zeros(1, np.int64)
+    pv = np.zeros(max(n, 1), np.int32)
+    lib().oracle_fast_count_range(n, _ptr(off), _ptr(ind), nthreads, lo, hi, _ptr(tot), _ptr(pv))
+    return int(tot[0]), pv[:n]
+
+
+def centre_cost(n, off, ind, nthreads=0):
+    """Predicted work per centre (int32, units of 16) as the multi-GPU split balances it."""
+    off, ind = _g(off, ind)
+    cost = np.zeros(max(n, 1), np.int32)
+    lib().oracle_centre_cost(n, _ptr(off), _ptr(ind), nthreads, _ptr(cost))
+    return cost[:n]

@@ -7,6 +7,9 @@
 //                                    called once per directed edge from an OpenMP loop over
 //                                    source vertices: the same arithmetic on all host cores.
 //   ref_host_count_triangles_omp_sample -> the same over a list of source vertices.
+//   ref_host_count_triangles_omp_pervertex -> the same over all directed edges, each edge's count
+//                                    summed into its source vertex (2 t(v), and the forward
+//                                    counts of the raw-CSR convention): the per-vertex pin.
 #include <cstdint>
 #include <omp.h>
 #include "cuStinger.hpp"
@@ -70,6 +73,67 @@ int64_t ref_host_count_triangles_omp_sample(int32_t nv, const int32_t* off, cons
       vertexId_t dest = ind[it];
       length_t destLen = off[dest + 1] - off[dest];
       sum += hostSingleIntersection(src, srcLen, ind + off[src], dest, destLen, ind + off[dest]);
+    }
+  }
+  return sum;
+}
+
+// Per-vertex form of hostCountTriangles (tests/cct.cpp:71-89): the same unmodified
+// hostSingleIntersection per directed edge, with each edge's count (the reference's triNE[edge])
+// added to its source vertex, so pv[src] = sum of triNE over src's edges = 2 t(src), exact in
+// int64. pv_fwd (nullable) gets the same sum over the edges with dest > src only: the raw-CSR
+// GPU counter's forward convention (tests/cct_csr.cu:246-249). The loop runs over edges, not
+// sources, so a hub's edges spread over all threads. Returns the sum over all edges (the
+// reference's allTriangles, 6T).
+int64_t ref_host_count_triangles_omp_pervertex(int32_t nv, const int32_t* off, const int32_t* ind,
+                                               int64_t* pv, int64_t* pv_fwd, int nthreads) {
+  int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+  const int64_t m = off[nv];
+  for (int32_t v = 0; v < nv; ++v) pv[v] = 0;
+  if (pv_fwd)
+    for (int32_t v = 0; v < nv; ++v) pv_fwd[v] = 0;
+  int64_t sum = 0;
+#pragma omp parallel num_threads(nt) reduction(+ : sum)
+  {
+    int32_t cur = -1;  // source of the last edge this thread took, and its running counts
+    int64_t acc = 0, acc_fwd = 0;
+#pragma omp for schedule(dynamic, 4096)
+    for (int64_t e = 0; e < m; ++e) {
+      if (cur < 0 || e < off[cur] || e >= off[cur + 1]) {
+        if (cur >= 0 && acc) {
+#pragma omp atomic
+          pv[cur] += acc;
+        }
+        if (cur >= 0 && acc_fwd) {
+#pragma omp atomic
+          pv_fwd[cur] += acc_fwd;
+        }
+        acc = 0;
+        acc_fwd = 0;
+        int32_t lo = 0, hi = nv - 1;  // last vertex whose list starts at or before e
+        while (lo < hi) {
+          int32_t mid = lo + (hi - lo + 1) / 2;
+          if (off[mid] <= e) lo = mid; else hi = mid - 1;
+        }
+        while (off[lo + 1] <= e) ++lo;  // skip empty lists that start at e
+        cur = lo;
+      }
+      const vertexId_t src = cur;
+      const length_t srcLen = off[src + 1] - off[src];
+      const vertexId_t dest = ind[e];
+      const length_t destLen = off[dest + 1] - off[dest];
+      const int c = hostSingleIntersection(src, srcLen, ind + off[src], dest, destLen, ind + off[dest]);
+      acc += c;
+      if (pv_fwd && dest > src) acc_fwd += c;
+      sum += c;
+    }
+    if (cur >= 0 && acc) {
+#pragma omp atomic
+      pv[cur] += acc;
+    }
+    if (cur >= 0 && acc_fwd) {
+#pragma omp atomic
+      pv_fwd[cur] += acc_fwd;
     }
   }
   return sum;

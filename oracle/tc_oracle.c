@@ -214,11 +214,57 @@ static inline int precedes(const int64_t* off, int32_t u, int32_t v) {
 
 void oracle_fast_count(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads,
                        int64_t* total, int32_t* per_vertex) {
-  oracle_fast_count_shard(nv, off, ind, nthreads, 0, 1, total, per_vertex);
+  oracle_fast_count_range(nv, off, ind, nthreads, 0, nv, total, per_vertex);
+}
+
+/* Out-degrees of the degree orientation. */
+static int32_t* out_degrees(int32_t nv, const int64_t* off, const int32_t* ind, int nt) {
+  int32_t* dp = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nv > 0 ? nv : 1));
+  (void)nt;
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 4096)
+  for (int32_t u = 0; u < nv; ++u) {
+    int32_t c = 0;
+    for (int64_t k = off[u]; k < off[u + 1]; ++k) c += precedes(off, u, ind[k]);
+    dp[u] = c;
+  }
+  return dp;
+}
+
+void oracle_centre_cost(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t* cost) {
+#ifdef _OPENMP
+  int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#else
+  int nt = 1;
+  (void)nthreads;
+#endif
+  int32_t* dp = out_degrees(nv, off, ind, nt);
+#pragma omp parallel for num_threads(nt) schedule(dynamic, 1024)
+  for (int32_t c = 0; c < nv; ++c) {
+    const int32_t a = dp[c];
+    uint64_t w = (uint64_t)(off[c + 1] - off[c]);
+    for (int64_t k = off[c]; k < off[c + 1]; ++k) {
+      const int32_t o = ind[k];
+      const int32_t b = dp[o];
+      if (b > 0 && (b < a || (b == a && c < o))) w += (uint64_t)b + 2u;
+    }
+    const uint64_t q = (w + 15u) / 16u;
+    cost[c] = q > (uint64_t)INT32_MAX ? INT32_MAX : (int32_t)q;
+  }
+  free(dp);
 }
 
 void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
                              int32_t nshards, int64_t* total, int32_t* per_vertex) {
+  oracle_fast_count_split(nv, off, ind, nthreads, shard, nshards, 0, nv, total, per_vertex);
+}
+
+void oracle_fast_count_range(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t lo,
+                             int32_t hi, int64_t* total, int32_t* per_vertex) {
+  oracle_fast_count_split(nv, off, ind, nthreads, 0, 1, lo, hi, total, per_vertex);
+}
+
+void oracle_fast_count_split(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
+                             int32_t nshards, int32_t lo, int32_t hi, int64_t* total, int32_t* per_vertex) {
 #ifdef _OPENMP
   int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
 #else
@@ -254,11 +300,11 @@ void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind,
       int32_t v = a[i];
       const int32_t* bb = pind + poff[v];
       int64_t bl = poff[v + 1] - poff[v];
-      if (nshards > 1) {
+      if (nshards > 1 || lo > 0 || hi < nv) {
         /* A shard owns the edges whose centre (the endpoint with the larger out-degree, ties to
          * the smaller id: the GPU count's hash side) is one of its vertices. */
         const int32_t centre = (bl < al || (bl == al && u < v)) ? u : v;
-        if (centre % nshards != shard) continue;
+        if (centre % nshards != shard || centre < lo || centre >= hi) continue;
       }
       int64_t x = 0, y = 0;
       uint32_t c = 0;

@@ -79,6 +79,20 @@ void oracle_fast_count(int32_t nv, const int64_t* off, const int32_t* ind, int n
 void oracle_fast_count_shard(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
                              int32_t nshards, int64_t* total, int32_t* per_vertex);
 
+/* The same restricted to the triangles whose edge {x, y} has its centre in [lo, hi): a shard of
+ * the multi-GPU count as it splits the centres into contiguous ranges. */
+void oracle_fast_count_range(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t lo,
+                             int32_t hi, int64_t* total, int32_t* per_vertex);
+
+/* Both restrictions at once (modulo shard and centre range). */
+void oracle_fast_count_split(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t shard,
+                             int32_t nshards, int32_t lo, int32_t hi, int64_t* total, int32_t* per_vertex);
+
+/* Predicted work of each centre c, the quantity the multi-GPU split balances: over the edges
+ * {c, o} that c is the centre of (o with out-degree b >= 1 and b < d+(c), or b == d+(c) and
+ * c < o), b + 2 each, plus deg(c); in units of 16, rounded up, clamped to int32. */
+void oracle_centre_cost(int32_t nv, const int64_t* off, const int32_t* ind, int nthreads, int32_t* cost);
+
 /* The per-edge loop of hostCountTriangles over a list of source vertices (bounded sample). */
 int64_t oracle_host_count_sample(int32_t nv, const int64_t* off, const int32_t* ind, const int32_t* verts,
                                  int32_t nverts, int nthreads);

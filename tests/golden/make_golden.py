@@ -3,7 +3,7 @@
 Run in a container that holds the reference sources (the reference's own CPU counter is built
 into oracle/_ref/ from tests/cct.cpp by oracle/Makefile):
 
-    make -f oracle/Makefile && python tests/golden/make_golden.py
+    make -f oracle/Makefile REF=<reference tree> && python tests/golden/make_golden.py
 
 For each graph it records a digest of the generated CSR (so generator drift is caught), the
 total of the reference's hostCountTriangles (tests/cct.cpp:71-89, = 6T) and digests of the
@@ -52,12 +52,15 @@ def graph_specs():
         ("rmat12_ef16_noise_s7", lambda: G.rmat(12, 16, seed=7, noise=True)),
         ("ba4096_m8_s1", lambda: G.barabasi_albert(4096, 8, seed=1)),
         ("grid64_r05_s1", lambda: G.grid_rewired(64, 0.05, seed=1)),
+        # rewired grids whose random edges close triangles (the 5 % grid above has none)
+        ("grid128_r05_s1", lambda: G.grid_rewired(128, 0.05, seed=1)),
+        ("grid64_r50_s1", lambda: G.grid_rewired(64, 0.5, seed=1)),
     ]
 
 
 def record(g, keep_arrays: bool):
     if not O.ref_available():
-        raise SystemExit("oracle/_ref/libref_cct.so missing: build it with make -f oracle/Makefile")
+        raise SystemExit("oracle/_ref/libref_cct.so missing: build it with make -f oracle/Makefile REF=<reference tree>")
     ref_total, ref_tri = O.ref_host_count_triangles(g.n, g.off, g.ind, per_edge=True)
     tot, tri = O.host_count_triangles(g.n, g.off, g.ind, per_edge=True)
     assert tot == ref_total and np.array_equal(tri, ref_tri), g.name

@@ -70,7 +70,8 @@ def test_every_reference_algorithm_compiles_on_these_headers():
     """The reference's BFS, connected components, PageRank, betweenness centrality and static and
     streaming Katz sources (its src/ tree) compile unmodified against include/ (oracle/Makefile
     target algs_check; skipped where the reference tree is absent)."""
-    r = subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "algs_check"],
+    from oracle import make_args
+    r = subprocess.run(["make", "-s", "-f", os.path.join(ROOT, "oracle", "Makefile"), "algs_check"] + make_args(),
                        capture_output=True, text=True, timeout=900)
     if "reference not present" in r.stdout:
         pytest.skip("reference tree absent")

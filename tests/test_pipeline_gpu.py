@@ -80,9 +80,162 @@ def test_pipeline_autotune_keeps_counts_and_picks_a_grid():
     T, _ = _recount(graph, n)
     assert T == T0 + int(delta.item())
     bins = pipe.info()
-    assert [c for c, _ in bins] == [1 << 10, 1 << 12]
-    assert all(b in (2, 4, 8, 16) for _, b in bins)
+    assert [c for c, _ in bins] == [1 << 10, 1 << 11, 1 << 12]
+    assert all(1 <= b <= 16 for _, b in bins)
+    plan = pipe.plan()
+    assert plan.nbins == 3
+    for i in range(3):
+        assert i <= plan.serve[i] < 3 and (i == 0 or plan.serve[i] >= plan.serve[i - 1])
+        assert plan.split_min[i] == 2 * plan.chunk[i]
     pipe.close()
+
+
+def _apply_both(torch, pipe, g_ref, batches, n):
+    """Run the batches through the pipeline and through tc_apply_batch on a twin; compare."""
+    pv_p = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    pv_r = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    dp = torch.zeros(1, dtype=torch.int64, device="cuda")
+    dr = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for s, d, x in batches:
+        ts, td, tx = _dev(torch, s, d, x)
+        pipe.apply(ts, td, tx, per_vertex=pv_p, delta_dev=dp)
+        pipe.sync()
+        g_ref.apply_batch(ts, td, tx, per_vertex=pv_r, delta_dev=dr)
+    assert int(dp.item()) == int(dr.item())
+    assert torch.equal(pv_p, pv_r)
+    return int(dp.item())
+
+
+@pytest.mark.parametrize("shape", [(0, 1024, 2048), (4, 1024, 2048), (2, 1024, 2048), (0, 512, 1024),
+                                   (0, 2048, 4096)])
+def test_every_tile_shape_counts_the_same(shape):
+    """Each candidate tile shape of the persistent delta kernel (CTAs per SM, split-item size,
+    split threshold), set through a plan, gives tc_apply_batch's results on hub-heavy batches
+    (hub lists of 3000-6000 entries, so hub-hub intersections are split at every threshold)."""
+    torch = _torch()
+    rng = np.random.default_rng(40)
+    n = 9000
+    hubs = np.arange(6, dtype=np.int32)
+    src, dst = [], []
+    for h in hubs:
+        nb = rng.choice(np.arange(6, n), int(rng.integers(3000, 6000)), replace=False).astype(np.int32)
+        src.append(np.full(nb.size, h, np.int32))
+        dst.append(nb)
+    src.append(rng.integers(0, n, 30000).astype(np.int32))
+    dst.append(rng.integers(0, n, 30000).astype(np.int32))
+    base = G.from_pairs(n, np.concatenate(src), np.concatenate(dst))
+    g_pipe = api.Graph.from_csr(base, slack=0.25)
+    g_ref = api.Graph.from_csr(base, slack=0.25)
+    pipe = api.Pipeline(g_pipe, 1 << 13)
+    plan = pipe.plan()
+    for i in range(plan.nbins):
+        plan.serve[i] = i
+        plan.ctas_per_sm[i], plan.chunk[i], plan.split_min[i] = shape
+    pipe.set_plan(plan)
+    batches = []
+    for k in [40, 900, 5000]:
+        # hub-hub edges (both endpoints hubs) and edges into the hubs' neighbourhoods
+        s = np.concatenate([rng.choice(hubs, k // 4), rng.integers(0, n, k - k // 4)]).astype(np.int32)
+        d = np.concatenate([rng.choice(hubs, k // 4), rng.integers(0, n, k - k // 4)]).astype(np.int32)
+        x = (rng.random(k) < 0.3).astype(np.uint8)
+        batches.append((s, d, x))
+    T0, _ = _recount(g_pipe, n)
+    delta = _apply_both(torch, pipe, g_ref, batches, n)
+    T, _ = _recount(g_pipe, n)
+    assert T == T0 + delta
+    pipe.close()
+
+
+def test_plan_carries_over_to_a_second_pipeline():
+    """Tune on one graph, carry the plan to a pipeline on a twin graph: same shapes, same counts."""
+    torch = _torch()
+    rng = np.random.default_rng(9)
+    base = G.rmat(12, 16, seed=8)
+    n = base.n
+    g_tune = api.Graph.from_csr(base, slack=0.25)
+    tuner = api.Pipeline(g_tune, 1 << 13)
+    tuner.autotune(30)
+    for i in range(30):
+        s, d, x = random_batch(rng, base, int(np.exp(rng.uniform(0, np.log(8000)))))
+        tuner.apply(*_dev(torch, s, d, x))
+    tuner.sync()
+    plan = tuner.plan()
+    tuner.close()
+    g_pipe = api.Graph.from_csr(base, slack=0.25)
+    g_ref = api.Graph.from_csr(base, slack=0.25)
+    pipe = api.Pipeline(g_pipe, 1 << 13)
+    pipe.set_plan(plan)
+    got = pipe.plan()
+    for i in range(plan.nbins):
+        assert (got.serve[i], got.ctas_per_sm[i], got.chunk[i], got.split_min[i]) == \
+            (plan.serve[i], plan.ctas_per_sm[i], plan.chunk[i], plan.split_min[i])
+    T0, _ = _recount(g_pipe, n)
+    batches = [random_batch(rng, base, k) for k in (5, 300, 2500, 7000)]
+    delta = _apply_both(torch, pipe, g_ref, batches, n)
+    T, _ = _recount(g_pipe, n)
+    assert T == T0 + delta
+    pipe.close()
+
+
+def test_delta_kernel_wait_bound_reports_timeout_and_device_stays_usable():
+    """The persistent delta kernel's grid barrier has a bounded wait. Made to wait for an arrival
+    that never comes (one beyond the grid), every CTA gives up after the bound (1 ms here), the
+    batch reports TC_ERR_TIMEOUT, and the device keeps working: the structure update completed,
+    a recount runs, and later batches count right again with the normal bound."""
+    torch = _torch()
+    rng = np.random.default_rng(12)
+    base = G.rmat(11, 16, seed=3)
+    n = base.n
+    graph = api.Graph.from_csr(base, slack=0.25)
+    pipe = api.Pipeline(graph, 1 << 12)
+    pipe.set_wait_bound(1_000_000, 1)
+    s, d, x = random_batch(rng, base, 800)
+    pipe.apply(*_dev(torch, s, d, x))
+    with pytest.raises(N.TcError) as ei:
+        pipe.sync()
+    assert ei.value.status == N.TC_ERR_TIMEOUT
+    pipe.set_wait_bound(2_000_000_000, 0)
+    T1, _ = _recount(graph, n)
+    delta = torch.zeros(1, dtype=torch.int64, device="cuda")
+    off, ind = graph.export()
+    cur = G.Csr(n, off, ind)
+    for k in (3, 500, 3000):
+        s, d, x = random_batch(rng, cur, k)
+        pipe.apply(*_dev(torch, s, d, x), delta_dev=delta)
+        pipe.sync()
+    T2, _ = _recount(graph, n)
+    assert T2 == T1 + int(delta.item())
+    pipe.close()
+
+
+def test_streaming_shards_add_up():
+    """Two ranks' shares of the delta count (changed edges e % 2 == 0 and == 1), run one after the
+    other on twin graphs, add up to the unsharded count, totals and per-vertex."""
+    torch = _torch()
+    rng = np.random.default_rng(14)
+    base = G.rmat(12, 16, seed=6)
+    n = base.n
+    batches = [random_batch(rng, base, k) for k in (7, 700, 4000)]
+    parts = []
+    for shard in range(2):
+        g = api.Graph.from_csr(base, slack=0.25)
+        sch = N.default_sched()
+        sch.shard, sch.nshards = shard, 2
+        pipe = api.Pipeline(g, 1 << 12, sched=sch)
+        pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+        dl = torch.zeros(1, dtype=torch.int64, device="cuda")
+        for s, d, x in batches:
+            pipe.apply(*_dev(torch, s, d, x), per_vertex=pv, delta_dev=dl)
+            pipe.sync()
+        parts.append((int(dl.item()), pv.clone()))
+        pipe.close()
+    g_full = api.Graph.from_csr(base, slack=0.25)
+    pv_f = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    d_f = torch.zeros(1, dtype=torch.int64, device="cuda")
+    for s, d, x in batches:
+        g_full.apply_batch(*_dev(torch, s, d, x), per_vertex=pv_f, delta_dev=d_f)
+    assert parts[0][0] + parts[1][0] == int(d_f.item())
+    assert torch.equal(parts[0][1] + parts[1][1], pv_f)
 
 
 def test_pipeline_rejects_oversize_batch_and_recaptures_on_new_outputs():

@@ -174,23 +174,39 @@ def test_export_roundtrip():
     assert n == g.n and used == g.m and alloc >= used
 
 
-@pytest.mark.parametrize("nshards", [2, 3])
-def test_shards_sum_to_full(nshards):
+@pytest.mark.parametrize("name,nshards", [("rmat12_ef16_s2", 2), ("rmat12_ef16_s2", 3), ("ba4096_m8_s1", 4),
+                                          ("rmat14_ef16_s2", 8)])
+def test_shards_sum_to_full(name, nshards):
+    """Each shard counts the contiguous range of centres the split rule gives it: the device's
+    predicted work per centre equals the oracle's, its range equals the host rule's
+    (tc_shard_ranges) on that work, its count equals the oracle's count of the range, and the
+    shards add up to the full count (total and per-vertex digest)."""
     torch = _torch()
-    g = golden_graph("rmat12_ef16_s2")
-    rec = GOLD["rmat12_ef16_s2"]
+    g = golden_graph(name)
+    rec = GOLD[name]
     graph = api.Graph.from_csr(g)
+    cost = O.centre_cost(g.n, g.off, g.ind)
+    pre = np.concatenate([[0], np.cumsum(cost, dtype=np.int64)])
+    lo = api.shard_ranges(pre, nshards)
     total = 0
     acc = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
     for sh in range(nshards):
         out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
-        T, _ = graph.count(N.TC_PV_HANDLE, out, sched=sched(shard=sh, nshards=nshards))
-        tot_o, pv_o = O.fast_count_shard(g.n, g.off, g.ind, sh, nshards)
+        T, info = graph.count(N.TC_PV_HANDLE, out, sched=sched(shard=sh, nshards=nshards))
+        assert (info.shard_lo, info.shard_hi) == (lo[sh], lo[sh + 1])
+        assert info.total_work == pre[-1] and info.shard_work == pre[lo[sh + 1]] - pre[lo[sh]]
+        tot_o, pv_o = O.fast_count_range(g.n, g.off, g.ind, int(lo[sh]), int(lo[sh + 1]))
         assert 6 * T == tot_o and np.array_equal(out[: g.n].cpu().numpy(), pv_o)
         total += T
         acc += out
     assert total == rec["triangles"]
     assert digest(acc[: g.n].cpu().numpy()) == rec["per_vertex_handle_digest"]
+
+
+def test_unsharded_count_reports_no_range():
+    g = golden_graph("rmat12_ef16_s2")
+    _, _, info = run_handle(g, N.TC_PV_HANDLE)
+    assert (info.shard_lo, info.shard_hi) == (0, -1)
 
 
 @pytest.mark.parametrize("name", ["rmat12_ef16_s2", "K70", "ba4096_m8_s1"])

@@ -41,6 +41,8 @@ GRAPH_SPECS = {
     "rmat12_ef16_noise_s7": lambda: G.rmat(12, 16, seed=7, noise=True),
     "ba4096_m8_s1": lambda: G.barabasi_albert(4096, 8, seed=1),
     "grid64_r05_s1": lambda: G.grid_rewired(64, 0.05, seed=1),
+    "grid128_r05_s1": lambda: G.grid_rewired(128, 0.05, seed=1),
+    "grid64_r50_s1": lambda: G.grid_rewired(64, 0.5, seed=1),
 }
 
 
