@@ -1,5 +1,6 @@
 // C ABI (include/custinger_tc.h): graph handle, workspaces and static counts.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -22,6 +23,19 @@ struct Prof {
 };
 thread_local Prof g_prof;
 }  // namespace
+
+namespace {
+std::atomic<long long> g_alloc_cap{0};  // 0 = no cap
+}  // namespace
+
+cudaError_t dev_malloc_bytes(void** p, size_t bytes) {
+  const long long cap = g_alloc_cap.load(std::memory_order_relaxed);
+  if (cap > 0 && (long long)bytes > cap) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
 
 void prof_mark(int point, cudaStream_t stream) {
   if (!g_prof.on || point < 0 || point > 2) return;
@@ -78,18 +92,27 @@ tc_status grow(T*& p, int64_t& cap, int64_t want) {
   p = nullptr;
   cap = 0;
   const int64_t n = std::max<int64_t>(want, 1);
-  TC_CUDA_TRY(cudaMalloc(&p, sizeof(T) * (size_t)n));
+  const cudaError_t e = ::tc::dev_malloc(&p, sizeof(T) * (size_t)n);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    return fail(e == cudaErrorMemoryAllocation ? TC_ERR_OOM : TC_ERR_CUDA, "device allocation of %lld bytes: %s",
+                (long long)(sizeof(T) * (size_t)n), cudaGetErrorString(e));
+  }
   cap = n;
   return TC_OK;
 }
 }  // namespace
 
+// Each group of arrays is (re)allocated together; a failed allocation leaves the group's
+// capacity at 0 (every array of it freed or null), so the next call allocates it again and no
+// kernel ever sees a freed or missing array.
 tc_status Workspace::ensure(int64_t n, int64_t m, int64_t extent) {
   int dev = 0;
   TC_CUDA_TRY(cudaGetDevice(&dev));
   if (device >= 0 && device != dev) return fail(TC_ERR_INVALID_ARG, "workspace used on device %d, created on %d", dev, device);
   device = dev;
   if (n + 1 > n_cap) {
+    n_cap = 0;
     int64_t c1 = 0, c2 = 0, c3 = 0;
     if (dplus) { cudaFree(dplus); dplus = nullptr; }
     if (offp) { cudaFree(offp); offp = nullptr; }
@@ -100,27 +123,39 @@ tc_status Workspace::ensure(int64_t n, int64_t m, int64_t extent) {
     n_cap = n + 1;
   }
   if (items_for(n, m) > item_cap) {
-    int64_t c1 = 0;
-    if (medium) { cudaFree(medium); medium = nullptr; }
-    TC_TRY(grow(medium, c1, items_for(n, m)));
-    TC_TRY(grow(large, item_cap, items_for(n, m)));
-  }
-  TC_TRY(grow(indp, e_cap, std::max(m, extent)));
-  if (hubs_for(m) > hub_cap) {
+    item_cap = 0;
     int64_t c1 = 0, c2 = 0;
+    if (medium) { cudaFree(medium); medium = nullptr; }
+    if (large) { cudaFree(large); large = nullptr; }
+    TC_TRY(grow(medium, c1, items_for(n, m)));
+    TC_TRY(grow(large, c2, items_for(n, m)));
+    item_cap = items_for(n, m);
+  }
+  TC_TRY(grow(indp, e_cap, std::max(m, extent) + kIndpPad));
+  if (hubs_for(m) > hub_cap) {
+    hub_cap = 0;
+    int64_t c1 = 0, c2 = 0, c3 = 0;
     if (hub_base) { cudaFree(hub_base); hub_base = nullptr; }
     if (hub_done) { cudaFree(hub_done); hub_done = nullptr; }
+    if (hub_u) { cudaFree(hub_u); hub_u = nullptr; }
     TC_TRY(grow(hub_base, c1, hubs_for(m)));
     TC_TRY(grow(hub_done, c2, hubs_for(m)));
-    TC_TRY(grow(hub_u, hub_cap, hubs_for(m)));
+    TC_TRY(grow(hub_u, c3, hubs_for(m)));
+    hub_cap = hubs_for(m);
   }
   if (chunks_for(m) > chunk_cap) {
-    int64_t c1 = 0;
+    chunk_cap = 0;
+    int64_t c1 = 0, c2 = 0;
     if (chunk_hub) { cudaFree(chunk_hub); chunk_hub = nullptr; }
-    TC_TRY(grow(hub_cnt, chunk_cap, chunks_for(m)));
-    TC_TRY(grow(chunk_hub, c1, chunks_for(m)));
+    if (hub_cnt) { cudaFree(hub_cnt); hub_cnt = nullptr; }
+    TC_TRY(grow(hub_cnt, c1, chunks_for(m)));
+    TC_TRY(grow(chunk_hub, c2, chunks_for(m)));
+    chunk_cap = chunks_for(m);
   }
-  if (!st) TC_CUDA_TRY(cudaMalloc(&st, sizeof(DevStatus)));
+  if (!st && ::tc::dev_malloc(&st, sizeof(DevStatus)) != cudaSuccess) {
+    st = nullptr;
+    return fail(TC_ERR_OOM, "workspace status: device allocation failed");
+  }
   return TC_OK;
 }
 
@@ -133,9 +168,17 @@ tc_status Workspace::ensure_shards(int64_t n) {
   shard_prefix = nullptr;
   shard_tiles = nullptr;
   shard_cap = 0;
-  TC_CUDA_TRY(cudaMalloc(&shard_cost, sizeof(int32_t) * (size_t)(n + 1)));
-  TC_CUDA_TRY(cudaMalloc(&shard_prefix, sizeof(int64_t) * (size_t)(n + 2)));
-  TC_CUDA_TRY(cudaMalloc(&shard_tiles, sizeof(int64_t) * (size_t)(scan_tiles(n + 1) + 1)));
+  if (::tc::dev_malloc(&shard_cost, sizeof(int32_t) * (size_t)(n + 1)) != cudaSuccess ||
+      ::tc::dev_malloc(&shard_prefix, sizeof(int64_t) * (size_t)(n + 2)) != cudaSuccess ||
+      ::tc::dev_malloc(&shard_tiles, sizeof(int64_t) * (size_t)(scan_tiles(n + 1) + 1)) != cudaSuccess) {
+    cudaFree(shard_cost);
+    cudaFree(shard_prefix);
+    cudaFree(shard_tiles);
+    shard_cost = nullptr;
+    shard_prefix = nullptr;
+    shard_tiles = nullptr;
+    return fail(TC_ERR_OOM, "shard workspace: device allocation failed");
+  }
   shard_cap = n + 1;
   return TC_OK;
 }
@@ -266,6 +309,12 @@ tc_status tc_count_csr64(int32_t nv, const int64_t* d_off, const int32_t* d_ind,
                          int64_t* triangles_dev, tc_count_info* info, const tc_sched* sched, void* stream) {
   tc::TraceRange trace_range("tc_count_csr64");
   return count_csr<Csr64View>(nv, d_off, d_ind, pv_mode, per_vertex, triangles_dev, info, sched, stream);
+}
+
+tc_status tc_debug_alloc_cap(int64_t bytes) {
+  if (bytes < 0) return fail(TC_ERR_INVALID_ARG, "negative allocation cap");
+  g_alloc_cap.store((long long)bytes, std::memory_order_relaxed);
+  return TC_OK;
 }
 
 tc_status tc_shard_ranges(const int64_t* prefix_host, int32_t n, int32_t nshards, int32_t* lo_host) {

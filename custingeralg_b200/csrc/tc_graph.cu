@@ -99,7 +99,22 @@ tc_status tc_graph_create(int32_t nv, const int64_t* off, const int32_t* ind, in
   if (m < 0 || (m > 0 && !ind)) return fail(TC_ERR_INVALID_ARG, "invalid edge array");
 
   tc_graph* g = new tc_graph();
+  int64_t* t_off = nullptr;
+  int32_t* t_ind = nullptr;
+  unsigned* d_bad = nullptr;
+  int64_t* tiles = nullptr;
+  auto free_tmp = [&]() {
+    cudaFree(t_off);
+    cudaFree(t_ind);
+    cudaFree(d_bad);
+    cudaFree(tiles);
+    t_off = nullptr;
+    t_ind = nullptr;
+    d_bad = nullptr;
+    tiles = nullptr;
+  };
   auto bail = [&](tc_status st) {
+    free_tmp();
     free_graph(g);
     delete g;
     return st;
@@ -119,29 +134,19 @@ tc_status tc_graph_create(int32_t nv, const int64_t* off, const int32_t* ind, in
 
   const int64_t* d_off = off;
   const int32_t* d_ind = ind;
-  int64_t* t_off = nullptr;
-  int32_t* t_ind = nullptr;
-  unsigned* d_bad = nullptr;
-  int64_t* tiles = nullptr;
-  auto free_tmp = [&]() {
-    cudaFree(t_off);
-    cudaFree(t_ind);
-    cudaFree(d_bad);
-    cudaFree(tiles);
-  };
   if (mem == TC_MEM_HOST) {
-    G_TRY(cudaMalloc(&t_off, sizeof(int64_t) * ((size_t)nv + 1)));
-    G_TRY(cudaMalloc(&t_ind, sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)));
+    G_TRY(::tc::dev_malloc(&t_off, sizeof(int64_t) * ((size_t)nv + 1)));
+    G_TRY(::tc::dev_malloc(&t_ind, sizeof(int32_t) * (size_t)std::max<int64_t>(m, 1)));
     G_TRY(cudaMemcpyAsync(t_off, off, sizeof(int64_t) * ((size_t)nv + 1), cudaMemcpyHostToDevice, s));
     if (m) G_TRY(cudaMemcpyAsync(t_ind, ind, sizeof(int32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
     d_off = t_off;
     d_ind = t_ind;
   }
-  G_TRY(cudaMalloc(&g->start, sizeof(int64_t) * ((size_t)nv + 1)));
-  G_TRY(cudaMalloc(&g->used, sizeof(int32_t) * (size_t)std::max(nv, 1)));
-  G_TRY(cudaMalloc(&g->cap, sizeof(int32_t) * (size_t)std::max(nv, 1)));
-  G_TRY(cudaMalloc(&d_bad, sizeof(unsigned)));
-  G_TRY(cudaMalloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(nv) + 1)));
+  G_TRY(::tc::dev_malloc(&g->start, sizeof(int64_t) * ((size_t)nv + 1)));
+  G_TRY(::tc::dev_malloc(&g->used, sizeof(int32_t) * (size_t)std::max(nv, 1)));
+  G_TRY(::tc::dev_malloc(&g->cap, sizeof(int32_t) * (size_t)std::max(nv, 1)));
+  G_TRY(::tc::dev_malloc(&d_bad, sizeof(unsigned)));
+  G_TRY(::tc::dev_malloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(nv) + 1)));
   G_TRY(cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s));
   if (nv > 0) {
     k_init_caps<<<warp_grid(nv), 256, 0, s>>>(nv, d_off, g->used, g->cap, g->slack_q10, d_bad);
@@ -167,8 +172,8 @@ tc_status tc_graph_create(int32_t nv, const int64_t* off, const int32_t* ind, in
   g->pool_top = top;
   // Headroom for lists that move when they outgrow their slack.
   g->pool_cap = top + (g->slack_q10 > 0 ? std::max<int64_t>(top / 4, 1 << 16) : 0);
-  G_TRY(cudaMalloc(&g->pool, sizeof(int32_t) * (size_t)std::max<int64_t>(g->pool_cap, 1)));
-  G_TRY(cudaMalloc(&g->d_pool_top, sizeof(unsigned long long)));
+  G_TRY(::tc::dev_malloc(&g->pool, sizeof(int32_t) * (size_t)std::max<int64_t>(g->pool_cap, 1)));
+  G_TRY(::tc::dev_malloc(&g->d_pool_top, sizeof(unsigned long long)));
   G_TRY(cudaMemcpyAsync(g->d_pool_top, &g->pool_top, sizeof(unsigned long long), cudaMemcpyHostToDevice, s));
   if (nv > 0) {
     k_copy_lists<<<warp_grid(nv), 256, 0, s>>>(nv, d_off, d_ind, g->start, g->used, g->pool);
@@ -226,9 +231,9 @@ tc_status tc_graph_export(tc_graph* g, int64_t* off_host, int32_t* ind_host) {
   int64_t* tiles = nullptr;
   tc_status rc = TC_OK;
   do {
-    if (cudaMalloc(&coff, sizeof(int64_t) * ((size_t)n + 1)) != cudaSuccess ||
-        cudaMalloc(&cind, sizeof(int32_t) * (size_t)std::max<int64_t>(g->m, 1)) != cudaSuccess ||
-        cudaMalloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(n) + 1)) != cudaSuccess) {
+    if (::tc::dev_malloc(&coff, sizeof(int64_t) * ((size_t)n + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&cind, sizeof(int32_t) * (size_t)std::max<int64_t>(g->m, 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(n) + 1)) != cudaSuccess) {
       rc = fail(TC_ERR_OOM, "export: allocation failed");
       break;
     }

@@ -28,6 +28,9 @@ constexpr int kHubMin = 256;        // orientation: lists longer than this are o
 static_assert(kHubMin <= kHubChunk, "a hub has at least one chunk");
 constexpr int kWarpTierMax = 128;   // largest out-degree a single warp counts on its own
 constexpr int kItemRangeMin = 256;  // fewest neighbours of a count work item (queue sizing)
+// The count reads oriented lists in aligned 16-byte units, up to 3 entries past a list's end:
+// every oriented-list array holds this many entries past its capacity.
+constexpr int kIndpPad = 4;
 
 // ---- error reporting -------------------------------------------------------------------
 
@@ -43,6 +46,16 @@ tc_status fail(tc_status s, const char* fmt, ...);
                         __LINE__);                                                         \
     }                                                                                      \
   } while (0)
+
+// Every device allocation of the library goes through dev_malloc. A test hook
+// (tc_debug_alloc_cap) makes allocations above a size fail the way cudaMalloc fails when device
+// memory runs out (cudaErrorMemoryAllocation, nothing allocated), so the out-of-memory paths can
+// be tested without exhausting a GPU.
+cudaError_t dev_malloc_bytes(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
 
 #define TC_TRY(expr)                  \
   do {                                \
@@ -79,7 +92,7 @@ struct SlackView {
 
 // ---- device-side status of one count ---------------------------------------------------
 
-enum : unsigned { kBadRange = 1u, kBadOrder = 2u, kBadSelfLoop = 4u, kBadCapacity = 8u };
+enum : unsigned { kBadRange = 1u, kBadOrder = 2u, kBadSelfLoop = 4u, kBadCapacity = 8u, kBadTimeout = 16u };
 
 struct DevStatus {
   unsigned long long triangles;          // T

@@ -327,8 +327,8 @@ tc_status tc_sched_learned(const float* d_params, int kind, const float* cell_fe
   cell_feature_rows(cell_features, feat.data());
   cudaStream_t s = (cudaStream_t)stream;
   float *dx = nullptr, *dy = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&dx, sizeof(float) * feat.size()));
-  TC_CUDA_TRY(cudaMalloc(&dy, sizeof(float) * 256 * kOut));
+  TC_CUDA_TRY(::tc::dev_malloc(&dx, sizeof(float) * feat.size()));
+  TC_CUDA_TRY(::tc::dev_malloc(&dy, sizeof(float) * 256 * kOut));
   std::vector<float> y(256 * kOut);
   tc_status rc = TC_OK;
   if (cudaMemcpyAsync(dx, feat.data(), sizeof(float) * feat.size(), cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -348,10 +348,10 @@ tc_status tc_mlp_train(float* d_params, const float* d_x, const int32_t* d_strat
   if (!d_params || n <= 0 || epochs < 1) return fail(TC_ERR_INVALID_ARG, "invalid training arguments");
   cudaStream_t s = (cudaStream_t)stream;
   float *g = nullptr, *m = nullptr, *v = nullptr, *l = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&g, sizeof(float) * kParams));
-  TC_CUDA_TRY(cudaMalloc(&m, sizeof(float) * kParams));
-  TC_CUDA_TRY(cudaMalloc(&v, sizeof(float) * kParams));
-  TC_CUDA_TRY(cudaMalloc(&l, sizeof(float)));
+  TC_CUDA_TRY(::tc::dev_malloc(&g, sizeof(float) * kParams));
+  TC_CUDA_TRY(::tc::dev_malloc(&m, sizeof(float) * kParams));
+  TC_CUDA_TRY(::tc::dev_malloc(&v, sizeof(float) * kParams));
+  TC_CUDA_TRY(::tc::dev_malloc(&l, sizeof(float)));
   cudaMemsetAsync(m, 0, sizeof(float) * kParams, s);
   cudaMemsetAsync(v, 0, sizeof(float) * kParams, s);
   tc_status rc = TC_OK;

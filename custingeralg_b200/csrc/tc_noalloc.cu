@@ -33,7 +33,7 @@ constexpr int64_t kMaxChunks = kMaxEdges / kHubMin + kMaxEdges / kHubChunk + 2;
 
 // Layout (bytes, each part 256-aligned): DevStatus | offp int64[maxnv+1] | dplus, degv
 // int32[maxnv+1] | large, medium uint64[items] | hub_u, hub_base, hub_done int32[hubs]
-// | hub_cnt, chunk_hub int32[chunks] | indp int32[max_edges]
+// | hub_cnt, chunk_hub int32[chunks] | indp int32[max_edges + kIndpPad]
 constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 constexpr size_t kOffStatus = 0;
 constexpr size_t kOffOffp = align256(kOffStatus + sizeof(DevStatus));
@@ -48,7 +48,7 @@ constexpr size_t kOffHubDone = align256(kOffHubBase + sizeof(int32_t) * kMaxHubs
 constexpr size_t kOffHubCnt = align256(kOffHubDone + sizeof(int32_t) * kMaxHubs);
 constexpr size_t kOffChunkHub = align256(kOffHubCnt + sizeof(int32_t) * kMaxChunks);
 constexpr size_t kOffIndp = align256(kOffChunkHub + sizeof(int32_t) * kMaxChunks);
-constexpr size_t kScratchBytes = align256(kOffIndp + sizeof(int32_t) * kMaxEdges);
+constexpr size_t kScratchBytes = align256(kOffIndp + sizeof(int32_t) * (kMaxEdges + kIndpPad));
 static_assert(kScratchBytes > (size_t(48) << 20) && kScratchBytes < (size_t(49) << 20),
               "the documented size of the no-alloc scratch (about 48.6 MiB) no longer holds");
 

@@ -56,7 +56,6 @@ constexpr int kThreads = 128;     // 4 warps: small CTAs keep more warps residen
 constexpr int kWarps = kThreads / kWarp;
 constexpr int kChunk = 1024;      // A entries staged per pass for an L-tier vertex
 constexpr int kHashMax = 2048;    // hash slots for such a chunk (load <= 0.5)
-constexpr int kUnroll = 4;        // list elements a lane loads before probing (independent loads)
 constexpr int kWarpRange = 256;   // neighbours of a warp-tier centre per work item
 constexpr int kCtaRange = 4096;   // neighbours of a CTA-tier centre per work item
 static_assert(kWarpRange >= kItemRangeMin && kCtaRange >= kItemRangeMin, "queue sizing");
@@ -117,8 +116,52 @@ struct CountSmem {
   } t;
   unsigned long long tri[kWarps];
   unsigned long long item;
+  uint64_t mbar;  // completion of the bulk copy that stages a CTA-tier chunk
   int gctr;
 };
+
+// ---- bulk copies into shared memory (cp.async.bulk, completion on an mbarrier) ----------------
+
+// Bound of the wait for a staged chunk: it lands within microseconds; a wait that runs out sets
+// kBadTimeout and the CTA stops (after a second bounded wait for its copy in flight).
+constexpr unsigned long long kStageWaitNs = 1000000000ull;  // 1 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Issue one 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory; the mbarrier's phase completes when the bytes have landed.
+__device__ __forceinline__ void stage_bulk(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Wait (bounded by kStageWaitNs of device time) for the mbarrier phase `parity` to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (unsigned it = 0; it < (1u << 26); ++it) {
+    uint32_t done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > kStageWaitNs) break;
+  }
+  return false;
+}
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned r;
@@ -254,43 +297,46 @@ __device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c
   return 1;
 }
 
-// The warp streams the list lst[0 .. len) through the hash set with coalesced loads, kUnroll
-// per lane in flight; returns this lane's hits.
+// The warp streams the list indp[base .. base + len) through the hash set: each lane loads one
+// aligned 16-byte unit (four entries) per step, so a warp step is one coalesced 512-byte read
+// and four probes per lane; entries of the first and last units outside the list are masked.
+// Returns this lane's hits.
 template <int PV>
-__device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
-                                               const int32_t o, const int32_t* hkeys, const int bits,
+__device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ indp, const int64_t base, const int len,
+                                               const int32_t c, const int32_t o, const int32_t* hkeys, const int bits,
                                                uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
   const int lane = threadIdx.x & (kWarp - 1);
+  const int64_t a0 = base & ~int64_t(3);
+  const int skip = (int)(base - a0);
+  const int nvec = (skip + len + 3) >> 2;
+  const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
   uint32_t hits = 0;
-  for (int k0 = lane; k0 < len; k0 += kUnroll * kWarp) {
-    int32_t w[kUnroll];
+  for (int i = lane; i < nvec; i += kWarp) {
+    const int4 q = __ldg(vec + i);
+    const int e0 = 4 * i - skip;  // list index of q.x
+    const int32_t w[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-    for (int j = 0; j < kUnroll; ++j) {
-      const int k = k0 + j * kWarp;
-      w[j] = k < len ? __ldg(lst + k) : -1;
-    }
-#pragma unroll
-    for (int j = 0; j < kUnroll; ++j) {
+    for (int j = 0; j < 4; ++j) {
+      if (e0 + j < 0 || e0 + j >= len) continue;
       const int32_t key = w[j];
-      if (key < 0) continue;
       // First bucket in one 128-bit load; the common case (a miss in a bucket with a free
       // slot) ends here without computing a slot.
       const uint32_t bk = hash_bucket(key, bits);
-      const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
-      const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
-      if (hit | (q.w != -1)) {
-        const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
-                          : hash_find_after(hkeys, bits, key, bk);
-        if (s >= 0) {
+      const int4 h = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
+      const bool hit = (h.x == key) | (h.y == key) | (h.z == key) | (h.w == key);
+      if (hit | (h.w != -1)) {
+        const int sl = hit ? (int)(4 * bk) + (h.x == key ? 0 : h.y == key ? 1 : h.z == key ? 2 : 3)
+                           : hash_find_after(hkeys, bits, key, bk);
+        if (sl >= 0) {
           ++hits;
           if (handle_like<PV>()) {
-            atomicAdd(&cnt[s], 1u);
+            atomicAdd(&cnt[sl], 1u);
           } else if (PV == TC_PV_CSR) {
             uint32_t wc, wo, ww;
             tri_weights<PV>(c, o, key, wc, wo, ww);
             c_acc += wc;
             vacc += wo;
-            if (ww) atomicAdd(&cnt[s], ww);
+            if (ww) atomicAdd(&cnt[sl], ww);
           }
         }
       }
@@ -299,21 +345,26 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, 
   return hits;
 }
 
-// One lane walks a whole (short) list lst[0 .. len), kUnroll entries in flight; returns the
-// hits. The lanes of a warp walk different lists at once, so short lists do not leave most of
-// the warp idle.
+// One lane walks a whole (short) list indp[base .. base + len) in aligned 16-byte units, two
+// in flight; returns the hits. The lanes of a warp walk different lists at once, so short lists
+// do not leave most of the warp idle.
 template <int PV>
-__device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
-                                              const int32_t o, const int32_t* hkeys, const int bits,
+__device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ indp, const int64_t base, const int len,
+                                              const int32_t c, const int32_t o, const int32_t* hkeys, const int bits,
                                               uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
+  const int64_t a0 = base & ~int64_t(3);
+  const int skip = (int)(base - a0);
+  const int nvec = (skip + len + 3) >> 2;
+  const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
   uint32_t hits = 0;
-  for (int k0 = 0; k0 < len; k0 += kUnroll) {
-    int32_t w[kUnroll];
+  for (int i = 0; i < nvec; i += 2) {
+    const int4 q0 = __ldg(vec + i);
+    const int4 q1 = i + 1 < nvec ? __ldg(vec + i + 1) : make_int4(-1, -1, -1, -1);
+    const int32_t w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    const int e0 = 4 * i - skip;
 #pragma unroll
-    for (int j = 0; j < kUnroll; ++j) w[j] = k0 + j < len ? __ldg(lst + k0 + j) : -1;
-#pragma unroll
-    for (int j = 0; j < kUnroll; ++j)
-      if (w[j] >= 0) hits += probe_one<PV>(w[j], c, o, hkeys, bits, cnt, c_acc, vacc);
+    for (int j = 0; j < 8; ++j)
+      if (e0 + j >= 0 && e0 + j < len) hits += probe_one<PV>(w[j], c, o, hkeys, bits, cnt, c_acc, vacc);
   }
   return hits;
 }
@@ -353,7 +404,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
   if (__any_sync(kFull, by_lane)) {
     if (by_lane) {
       uint32_t vacc = 0;
-      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
+      const uint32_t hits = walk_list<PV>(indp, base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
       tri += hits;
       if (handle_like<PV>()) {
         c_acc += hits;
@@ -417,7 +468,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     const int sb = __shfl_sync(kFull, b, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
     uint32_t vacc = 0;
-    const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
+    const uint32_t hits = probe_list<PV>(indp, sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
     tri += hits;
     if (handle_like<PV>()) {
       c_acc += hits;
@@ -440,7 +491,6 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
                                             const int64_t* __restrict__ offp, const int32_t* __restrict__ indp,
                                             uint32_t* __restrict__ out, const SchedParams& sp, uint32_t& tri) {
   const int lane = threadIdx.x & (kWarp - 1);
-  const int32_t* Ag = indp + start;
   int bits = 4;  // buckets: 4 * 2^bits slots >= 4a (load <= 0.25) while they fit in kMedSlots
   while ((1 << bits) < a && (8 << bits) <= kMedSlots) ++bits;
   const int S = 4 << bits;
@@ -449,7 +499,21 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
     t.cnt[s] = 0;
   }
   __syncwarp();
-  for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, bits, __ldg(Ag + j));
+  {
+    // N+(c) in aligned 16-byte units (a <= kWarpTierMax: at most 33 units, about one per lane)
+    const int64_t a0 = start & ~int64_t(3);
+    const int skip = (int)(start - a0);
+    const int nvec = (skip + a + 3) >> 2;
+    const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
+    for (int i = lane; i < nvec; i += kWarp) {
+      const int4 q = __ldg(vec + i);
+      const int32_t w[4] = {q.x, q.y, q.z, q.w};
+      const int e0 = 4 * i - skip;
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (e0 + j >= 0 && e0 + j < a) hash_insert(t.hkeys, bits, w[j]);
+    }
+  }
   __syncwarp();
   uint32_t c_acc = 0;
   for (int g = k0; g < k1; g += kWarp)
@@ -494,8 +558,11 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
   const int32_t s_lo = (int32_t)st->shard_lo, s_hi = (int32_t)st->shard_hi;
 
   // CTA tier: one CTA per item (centre with a > warp_max, kCtaRange of its neighbours), over
-  // chunks of kChunk staged entries of N+(c).
+  // chunks of kChunk entries of N+(c), each staged into shared memory by one bulk copy.
   BlockTable& L = sm.t.L;
+  if (threadIdx.x == 0) mbar_init(&sm.mbar);
+  __syncthreads();
+  uint32_t stage_phase = 0;
   while (true) {
     if (threadIdx.x == 0) {
       const unsigned q = atomicAdd(&st->q_large, 1u);
@@ -511,7 +578,6 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
     const int32_t a = dplus[c];
     const int64_t start = offp[c];
     const int32_t k1 = min(degv[c], k0 + kCtaRange);
-    const int32_t* Ag = indp + start;
     uint32_t c_acc = 0;
     for (int cb = 0; cb < a; cb += kChunk) {
       const int clen = min(kChunk, a - cb);
@@ -519,14 +585,30 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
       constexpr int bits = 9;
       static_assert((4 << bits) == kHashMax, "CTA table size");
       const int S = 4 << bits;
-      for (int s = threadIdx.x; s < S; s += kThreads) {
-        L.hkeys[s] = -1;
-        L.cnt[s] = 0;
+      // Stage N+(c)[cb, cb + clen) in the counter half of the table (cleared after the build):
+      // one bulk copy of the 16-byte units that cover it (at most clen + 3 entries, inside the
+      // list or the array's padding), issued while the threads clear the keys.
+      const int64_t gs = start + cb, ga = gs & ~int64_t(3);
+      const int skip = (int)(gs - ga);
+      static_assert(sizeof(L.cnt) >= sizeof(int32_t) * (kChunk + 4), "staging area");
+      int32_t* stage = reinterpret_cast<int32_t*>(L.cnt);
+      if (threadIdx.x == 0) {
+        sm.gctr = 0;
+        stage_bulk(stage, indp + ga, (uint32_t)(((skip + clen + 3) & ~3) * sizeof(int32_t)), &sm.mbar);
       }
-      if (threadIdx.x == 0) sm.gctr = 0;
+      for (int s = threadIdx.x; s < S; s += kThreads) L.hkeys[s] = -1;
+      const bool landed = mbar_wait(&sm.mbar, stage_phase);
+      stage_phase ^= 1u;
+      if (__syncthreads_or(!landed)) {
+        // the copy did not land in time: report it, wait once more for it, stop this CTA
+        if (threadIdx.x == 0) atomicOr(&st->bad_flags, kBadTimeout);
+        mbar_wait(&sm.mbar, stage_phase ^ 1u);
+        return;
+      }
+      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, bits, stage[skip + j]);
       __syncwarp();
       __syncthreads();
-      for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, bits, __ldg(Ag + cb + j));
+      for (int s = threadIdx.x; s < S; s += kThreads) L.cnt[s] = 0;
       __syncwarp();
       __syncthreads();
       const int ngroups = (k1 - k0 + kWarp - 1) / kWarp;
@@ -1327,6 +1409,10 @@ tc_status read_info(const Workspace& ws, cudaStream_t stream, tc_count_info* inf
     info->status = TC_ERR_CAPACITY;
     return fail(TC_ERR_CAPACITY, "oriented graph exceeded its workspace");
   }
+  if (h.bad_flags & kBadTimeout) {
+    info->status = TC_ERR_TIMEOUT;
+    return fail(TC_ERR_TIMEOUT, "a staged copy of the count kernel did not land in time; the count is incomplete");
+  }
   if (h.sym_checksum != 0) {
     info->status = TC_ERR_NOT_SYMMETRIC;
     return fail(TC_ERR_NOT_SYMMETRIC, "adjacency is not symmetric");
@@ -1370,7 +1456,7 @@ __global__ void __launch_bounds__(256) k_cell_stats(const int32_t n, const int32
 
 tc_status cell_stats(int32_t n, Workspace& ws, double* out_host, cudaStream_t stream) {
   double* d = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&d, sizeof(double) * 1024));
+  TC_CUDA_TRY(::tc::dev_malloc(&d, sizeof(double) * 1024));
   cudaMemsetAsync(d, 0, sizeof(double) * 1024, stream);
   if (n > 0) k_cell_stats<<<orient_grid(n), 256, 0, stream>>>(n, ws.dplus, ws.offp, ws.indp, d);
   cudaError_t e = cudaMemcpyAsync(out_host, d, sizeof(double) * 1024, cudaMemcpyDeviceToHost, stream);

@@ -1077,58 +1077,93 @@ void release_stream_ws(StreamWs* w) {
 
 namespace {
 
+// Allocate (or grow) the batch workspace. Each group of arrays is replaced as a whole: a failed
+// allocation frees the group and leaves its capacity at 0, so a later call allocates it again and
+// no kernel sees a freed or missing array (the graph itself is untouched).
 tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   if (!g->sw) g->sw = new StreamWs();
   StreamWs& w = *g->sw;
   if (!g->mark) {
-    TC_CUDA_TRY(cudaMalloc(&g->mark, (size_t)std::max<int64_t>(g->pool_cap, 1)));
-    TC_CUDA_TRY(cudaMemset(g->mark, 0, (size_t)std::max<int64_t>(g->pool_cap, 1)));
+    uint8_t* mk = nullptr;
+    if (::tc::dev_malloc(&mk, (size_t)std::max<int64_t>(g->pool_cap, 1)) != cudaSuccess)
+      return fail(TC_ERR_OOM, "edge marks: device allocation failed");
+    const cudaError_t e = cudaMemset(mk, 0, (size_t)std::max<int64_t>(g->pool_cap, 1));
+    if (e != cudaSuccess) {
+      cudaFree(mk);
+      return fail(TC_ERR_CUDA, "edge marks: %s", cudaGetErrorString(e));
+    }
+    g->mark = mk;
   }
   if (w.n_cap < (int64_t)g->n + 1) {
     cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
-    TC_CUDA_TRY(cudaMalloc(&w.claim, sizeof(unsigned) * ((size_t)g->n + 1)));
-    TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * ((size_t)g->n + 1)));
-    TC_CUDA_TRY(cudaMalloc(&w.d_epoch, sizeof(unsigned)));
-    TC_CUDA_TRY(cudaMemset(w.d_epoch, 0, sizeof(unsigned)));
-    TC_CUDA_TRY(cudaMalloc(&w.cnt, sizeof(int32_t) * ((size_t)g->n + 1)));
-    TC_CUDA_TRY(cudaMalloc(&w.scan64, sizeof(int64_t) * ((size_t)g->n + 2)));
-    TC_CUDA_TRY(cudaMalloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)));
-    w.n_cap = g->n + 1;
+    w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
+    w.n_cap = 0;
     ++w.version;
+    const size_t n1 = (size_t)g->n + 1;
+    if (::tc::dev_malloc(&w.claim, sizeof(unsigned) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.d_epoch, sizeof(unsigned)) != cudaSuccess ||
+        ::tc::dev_malloc(&w.cnt, sizeof(int32_t) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.scan64, sizeof(int64_t) * (n1 + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)) != cudaSuccess) {
+      cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
+      w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
+      return fail(TC_ERR_OOM, "batch workspace (per vertex): device allocation failed");
+    }
+    TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * n1));
+    TC_CUDA_TRY(cudaMemset(w.d_epoch, 0, sizeof(unsigned)));
+    w.n_cap = g->n + 1;
   }
-  if (!w.st) {
-    TC_CUDA_TRY(cudaMalloc(&w.st, sizeof(BatchStatus)));
-    TC_CUDA_TRY(cudaMallocHost(&w.st_host, sizeof(BatchStatus)));
-    TC_CUDA_TRY(cudaMalloc(&w.counter, sizeof(unsigned long long)));
-    TC_CUDA_TRY(cudaMalloc(&w.split_items, sizeof(unsigned long long) * kDeltaItems));
+  if (!w.st || !w.st_host || !w.counter || !w.split_items) {
+    cudaFree(w.st); cudaFreeHost(w.st_host); cudaFree(w.counter); cudaFree(w.split_items);
+    w.st = nullptr; w.st_host = nullptr; w.counter = nullptr; w.split_items = nullptr;
+    if (::tc::dev_malloc(&w.st, sizeof(BatchStatus)) != cudaSuccess ||
+        cudaMallocHost(&w.st_host, sizeof(BatchStatus)) != cudaSuccess ||
+        ::tc::dev_malloc(&w.counter, sizeof(unsigned long long)) != cudaSuccess ||
+        ::tc::dev_malloc(&w.split_items, sizeof(unsigned long long) * kDeltaItems) != cudaSuccess) {
+      cudaFree(w.st); cudaFreeHost(w.st_host); cudaFree(w.counter); cudaFree(w.split_items);
+      w.st = nullptr; w.st_host = nullptr; w.counter = nullptr; w.split_items = nullptr;
+      return fail(TC_ERR_OOM, "batch status: allocation failed");
+    }
+    ++w.version;
   }
   if (b <= w.b_cap) return TC_OK;
   const int64_t nb = std::max<int64_t>(b, 1024);
-  cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
-  cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start); cudaFree(w.long_runs);
-  cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
-  w.cub_tmp = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&w.src, sizeof(int32_t) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.dst, sizeof(int32_t) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.isdel, nb));
-  TC_CUDA_TRY(cudaMalloc(&w.keys, sizeof(uint64_t) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.keys2, sizeof(uint64_t) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.head, sizeof(int32_t) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.dlist, sizeof(int4) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.ilist, sizeof(int2) * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.dk, sizeof(uint64_t) * 2 * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.dk2, sizeof(uint64_t) * 2 * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.run_start, sizeof(int32_t) * 2 * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.long_runs, sizeof(int32_t) * 2 * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.ins_slot, sizeof(int64_t) * 2 * nb));
-  TC_CUDA_TRY(cudaMalloc(&w.vlist, sizeof(int32_t) * 2 * nb));
-  size_t t1 = 0, t2 = 0;
-  TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t1, w.keys, w.keys2, (int)(2 * nb)));
-  TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t2, w.dk, w.dk2, (int)(2 * nb)));
-  w.cub_bytes = std::max(t1, t2);
-  TC_CUDA_TRY(cudaMalloc(&w.cub_tmp, w.cub_bytes));
-  w.b_cap = nb;
+  auto free_batch = [&w]() {
+    cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
+    cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
+    cudaFree(w.long_runs); cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
+    w.src = nullptr; w.dst = nullptr; w.isdel = nullptr; w.keys = nullptr; w.keys2 = nullptr; w.head = nullptr;
+    w.dlist = nullptr; w.ilist = nullptr; w.dk = nullptr; w.dk2 = nullptr; w.run_start = nullptr;
+    w.long_runs = nullptr; w.ins_slot = nullptr; w.vlist = nullptr; w.cub_tmp = nullptr;
+    w.b_cap = 0;
+    w.cub_bytes = 0;
+  };
+  free_batch();
   ++w.version;
+  size_t t1 = 0, t2 = 0;
+  bool ok = ::tc::dev_malloc(&w.src, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.dst, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.isdel, nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.keys, sizeof(uint64_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.keys2, sizeof(uint64_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.head, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.dlist, sizeof(int4) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.ilist, sizeof(int2) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.dk, sizeof(uint64_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.dk2, sizeof(uint64_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.run_start, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.long_runs, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.ins_slot, sizeof(int64_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.vlist, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            cub::DeviceRadixSort::SortKeys(nullptr, t1, w.keys, w.keys2, (int)(2 * nb)) == cudaSuccess &&
+            cub::DeviceRadixSort::SortKeys(nullptr, t2, w.dk, w.dk2, (int)(2 * nb)) == cudaSuccess &&
+            ::tc::dev_malloc(&w.cub_tmp, std::max(t1, t2)) == cudaSuccess;
+  if (!ok) {
+    free_batch();
+    return fail(TC_ERR_OOM, "batch workspace for %lld updates: device allocation failed", (long long)nb);
+  }
+  w.cub_bytes = std::max(t1, t2);
+  w.b_cap = nb;
   return TC_OK;
 }
 
@@ -1139,8 +1174,12 @@ tc_status ensure_pool(tc_graph* g, int64_t extra, cudaStream_t s) {
   const int64_t ncap = std::max<int64_t>(need + need / 4, g->pool_cap * 3 / 2);
   int32_t* np = nullptr;
   uint8_t* nm = nullptr;
-  TC_CUDA_TRY(cudaMalloc(&np, sizeof(int32_t) * (size_t)ncap));
-  TC_CUDA_TRY(cudaMalloc(&nm, (size_t)ncap));
+  if (::tc::dev_malloc(&np, sizeof(int32_t) * (size_t)ncap) != cudaSuccess ||
+      ::tc::dev_malloc(&nm, (size_t)ncap) != cudaSuccess) {
+    cudaFree(np);
+    cudaFree(nm);
+    return fail(TC_ERR_OOM, "adjacency pool growth to %lld slots: device allocation failed", (long long)ncap);
+  }
   TC_CUDA_TRY(cudaMemcpyAsync(np, g->pool, sizeof(int32_t) * (size_t)g->pool_top, cudaMemcpyDeviceToDevice, s));
   TC_CUDA_TRY(cudaMemsetAsync(nm, 0, (size_t)ncap, s));
   if (g->mark) TC_CUDA_TRY(cudaMemcpyAsync(nm, g->mark, (size_t)g->pool_top, cudaMemcpyDeviceToDevice, s));
@@ -1275,7 +1314,10 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
   uint32_t* scratch_pv = nullptr;
   if (!pv_use) {
     // counts only: route per-vertex updates to a scratch array
-    if (!g->pv_scratch) TC_CUDA_TRY(cudaMalloc(&g->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)));
+    if (!g->pv_scratch && ::tc::dev_malloc(&g->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess) {
+      g->pv_scratch = nullptr;
+      return fail(TC_ERR_OOM, "per-vertex scratch: device allocation failed");
+    }
     scratch_pv = reinterpret_cast<uint32_t*>(g->pv_scratch);
     pv_use = scratch_pv;
   }
@@ -1352,12 +1394,12 @@ tc_status tc_batch_sort(int32_t nv, int32_t* d_src, int32_t* d_dst, int64_t b, i
   tc_status rc = TC_OK;
   unsigned herr = 0;
   do {
-    if (cudaMalloc(&k1, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
-        cudaMalloc(&k2, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
-        cudaMalloc(&cnt, sizeof(int32_t) * ((size_t)nv + 1)) != cudaSuccess ||
-        cudaMalloc(&off64, sizeof(int64_t) * ((size_t)nv + 2)) != cudaSuccess ||
-        cudaMalloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(nv) + 1)) != cudaSuccess ||
-        cudaMalloc(&err, sizeof(unsigned)) != cudaSuccess) {
+    if (::tc::dev_malloc(&k1, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&k2, sizeof(uint64_t) * std::max<int64_t>(b, 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&cnt, sizeof(int32_t) * ((size_t)nv + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&off64, sizeof(int64_t) * ((size_t)nv + 2)) != cudaSuccess ||
+        ::tc::dev_malloc(&tiles, sizeof(int64_t) * (size_t)(scan_tiles(nv) + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&err, sizeof(unsigned)) != cudaSuccess) {
       rc = fail(TC_ERR_OOM, "batch sort: allocation failed");
       break;
     }
@@ -1366,7 +1408,7 @@ tc_status tc_batch_sort(int32_t nv, int32_t* d_src, int32_t* d_dst, int64_t b, i
     if (b > 0) {
       k_pack_dir<<<grid_for(b, kThreads), kThreads, 0, s>>>(d_src, d_dst, b, k1);
       cub::DeviceRadixSort::SortKeys(nullptr, tb, k1, k2, (int)b, 0, 64, s);
-      if (cudaMalloc(&tmp, std::max<size_t>(tb, 1)) != cudaSuccess) {
+      if (::tc::dev_malloc(&tmp, std::max<size_t>(tb, 1)) != cudaSuccess) {
         rc = fail(TC_ERR_OOM, "batch sort: allocation failed");
         break;
       }
@@ -1609,13 +1651,18 @@ tc_status pipe_settle(tc_pipeline* p) {
     p->tune_n[bi][a] += 1;
     p->timing = false;
   }
-  if (p->profile) {
+  if (p->profile && p->prof_delta_ms >= 0.0) {
+    // a failed read (no event recorded by the graph) turns the profile off, not the batch
     float d0 = 0.f, d1 = 0.f;
-    TC_CUDA_TRY(cudaEventElapsedTime(&d0, p->pev[0], p->pev[1]));
-    TC_CUDA_TRY(cudaEventElapsedTime(&d1, p->pev[2], p->pev[3]));
-    p->prof_batches += 1;
-    p->prof_delta_ms += (double)d0 + (double)d1;
-    p->prof_delta_bytes += (int64_t)f.delta_bytes;
+    if (cudaEventElapsedTime(&d0, p->pev[0], p->pev[1]) != cudaSuccess ||
+        cudaEventElapsedTime(&d1, p->pev[2], p->pev[3]) != cudaSuccess) {
+      cudaGetLastError();
+      p->prof_delta_ms = -1.0;
+    } else {
+      p->prof_batches += 1;
+      p->prof_delta_ms += (double)d0 + (double)d1;
+      p->prof_delta_bytes += (int64_t)f.delta_bytes;
+    }
   }
   if (f.err & kErrRange) {
     p->last.status = TC_ERR_INVALID_ARG;
@@ -1814,12 +1861,12 @@ tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sch
   do {
     if ((rc = ensure_stream_ws(g, p->b_max)) != TC_OK) break;
     if (cudaStreamCreateWithFlags(&p->cs, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&p->d_b, sizeof(int64_t)) != cudaSuccess ||
+        ::tc::dev_malloc(&p->d_b, sizeof(int64_t)) != cudaSuccess ||
         cudaMallocHost(&p->h_b, sizeof(int64_t)) != cudaSuccess ||
         cudaMallocHost(&p->h_st, sizeof(BatchStatus)) != cudaSuccess ||
         cudaMallocHost(&p->h_top, sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&p->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
-        cudaMalloc(&p->delta_scratch, sizeof(int64_t)) != cudaSuccess ||
+        ::tc::dev_malloc(&p->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&p->delta_scratch, sizeof(int64_t)) != cudaSuccess ||
         cudaEventCreate(&p->done) != cudaSuccess || cudaEventCreate(&p->t0) != cudaSuccess ||
         cudaEventCreate(&p->t1) != cudaSuccess || cudaEventCreate(&p->pev[0]) != cudaSuccess ||
         cudaEventCreate(&p->pev[1]) != cudaSuccess || cudaEventCreate(&p->pev[2]) != cudaSuccess ||

@@ -176,6 +176,11 @@ tc_status tc_count_csr32_noalloc(int32_t nv, const int32_t* d_off, const int32_t
  * predicted work. The device applies the same rule to its own prefix. */
 tc_status tc_shard_ranges(const int64_t* prefix_host, int32_t n, int32_t nshards, int32_t* lo_host);
 
+/* Fault injection for tests (host side, no GPU fault): while bytes > 0, every device allocation
+ * the library makes that is larger than `bytes` fails as cudaMalloc fails when memory runs out,
+ * so calls return TC_ERR_OOM and leave their objects usable. 0 removes the cap. */
+tc_status tc_debug_alloc_cap(int64_t bytes);
+
 /* Read back the info of the last stateless count on the current device. Syncs `stream`. */
 tc_status tc_workspace_status(void* stream, tc_count_info* info);
 
