@@ -339,6 +339,17 @@ tc_status tc_profile_last(tc_phase_times* t) {
   return TC_OK;
 }
 
+tc_status tc_workspace_release(void) {
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  GlobalWs& g = global_ws();
+  std::lock_guard<std::mutex> lk(g.mu);
+  TC_CUDA_TRY(cudaDeviceSynchronize());  // no count may still use it
+  g.ws[dev].release();
+  return TC_OK;
+}
+
 tc_status tc_workspace_status(void* stream, tc_count_info* info) {
   if (!info) return fail(TC_ERR_INVALID_ARG, "info is NULL");
   int dev = 0;

@@ -95,6 +95,7 @@ SIGNATURES = {
     "tc_count_csr64": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),
                                       ctypes.POINTER(Sched), _P]),
     "tc_workspace_status": (ctypes.c_int, [_P, ctypes.POINTER(CountInfo)]),
+    "tc_workspace_release": (ctypes.c_int, []),
     "tc_shard_ranges": (ctypes.c_int, [_P, _i32, _i32, _P]),
     "tc_debug_alloc_cap": (ctypes.c_int, [_i64]),
     "tc_count_csr32_noalloc": (ctypes.c_int, [_i32, _P, _P, ctypes.c_int, _P, _P, ctypes.POINTER(CountInfo),

@@ -183,6 +183,9 @@ tc_status tc_debug_alloc_cap(int64_t bytes);
 
 /* Read back the info of the last stateless count on the current device. Syncs `stream`. */
 tc_status tc_workspace_status(void* stream, tc_count_info* info);
+/* Free the working memory the stateless counts (tc_count_csr32/64) keep on the current device
+ * (it is allocated again by the next such count). Waits for the device first. */
+tc_status tc_workspace_release(void);
 
 /* ---- streaming updates ------------------------------------------------------------------ */
 

@@ -55,13 +55,18 @@ def test_stateless_count_reports_oom_then_works():
         out = torch.zeros(g.n + 1, dtype=torch.int32, device="cuda")
         return api.count_all_triangles_csr(g.n, d_off, d_ind, out, pv_mode=N.TC_PV_CSR), out[:g.n].cpu().numpy()
 
-    run(small)                        # the library's workspace now exists, sized for the small graph
+    N.check(N.lib().tc_workspace_release())   # the library's workspace: none on this device now
     N.check(N.lib().tc_debug_alloc_cap(CAP))
     with pytest.raises(N.TcError) as ei:
-        run(big)                      # growing it fails
+        run(big)                      # allocating it fails
     assert ei.value.status == N.TC_ERR_OOM
-    (T, _), pv = run(small)           # a smaller graph still counts (the workspace was left consistent)
+    (T, _), pv = run(small)           # a graph whose workspace fits under the cap counts right
     tot, _ = O.host_count_triangles(small.n, small.off, small.ind)
+    assert 6 * T == tot and np.array_equal(pv, O.csr_per_vertex(small.n, small.off, small.ind))
+    with pytest.raises(N.TcError) as ei:
+        run(big)                      # growing it fails, and leaves it usable
+    assert ei.value.status == N.TC_ERR_OOM
+    (T, _), pv = run(small)
     assert 6 * T == tot and np.array_equal(pv, O.csr_per_vertex(small.n, small.off, small.ind))
     N.check(N.lib().tc_debug_alloc_cap(0))
     (T, _), pv = run(big)
