@@ -146,7 +146,7 @@ struct SchedParams {
   int32_t chunk;
   int32_t blocks_per_sm;   // 0 = occupancy limit
   int32_t shard;           // static: count the centres of range `shard` of `nshards` (shard_start);
-  int32_t nshards;         // streaming: the changed edges e with e % nshards == shard
+  int32_t nshards;         // streaming: the changed edges whose key hashes to `shard` (edge_shard)
   int32_t cell_filter;     // -1 all edges, -2 none, >= 0 only that degree cell
   int32_t lane_max;        // static: lists of at most this many entries are walked by one lane
   int32_t packed_max;      // static: longer lists up to this many entries are walked packed

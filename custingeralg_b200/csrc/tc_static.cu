@@ -56,6 +56,7 @@ constexpr int kThreads = 128;     // 4 warps: small CTAs keep more warps residen
 constexpr int kWarps = kThreads / kWarp;
 constexpr int kChunk = 1024;      // A entries staged per pass for an L-tier vertex
 constexpr int kHashMax = 2048;    // hash slots for such a chunk (load <= 0.5)
+constexpr int kUnroll = 4;        // list elements a lane loads before probing (independent loads)
 constexpr int kWarpRange = 256;   // neighbours of a warp-tier centre per work item
 constexpr int kCtaRange = 4096;   // neighbours of a CTA-tier centre per work item
 static_assert(kWarpRange >= kItemRangeMin && kCtaRange >= kItemRangeMin, "queue sizing");
@@ -297,46 +298,43 @@ __device__ __forceinline__ uint32_t probe_one(const int32_t key, const int32_t c
   return 1;
 }
 
-// The warp streams the list indp[base .. base + len) through the hash set: each lane loads one
-// aligned 16-byte unit (four entries) per step, so a warp step is one coalesced 512-byte read
-// and four probes per lane; entries of the first and last units outside the list are masked.
-// Returns this lane's hits.
+// The warp streams the list lst[0 .. len) through the hash set with coalesced loads, kUnroll
+// per lane in flight; returns this lane's hits.
 template <int PV>
-__device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ indp, const int64_t base, const int len,
-                                               const int32_t c, const int32_t o, const int32_t* hkeys, const int bits,
+__device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
+                                               const int32_t o, const int32_t* hkeys, const int bits,
                                                uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
   const int lane = threadIdx.x & (kWarp - 1);
-  const int64_t a0 = base & ~int64_t(3);
-  const int skip = (int)(base - a0);
-  const int nvec = (skip + len + 3) >> 2;
-  const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
   uint32_t hits = 0;
-  for (int i = lane; i < nvec; i += kWarp) {
-    const int4 q = __ldg(vec + i);
-    const int e0 = 4 * i - skip;  // list index of q.x
-    const int32_t w[4] = {q.x, q.y, q.z, q.w};
+  for (int k0 = lane; k0 < len; k0 += kUnroll * kWarp) {
+    int32_t w[kUnroll];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      if (e0 + j < 0 || e0 + j >= len) continue;
+    for (int j = 0; j < kUnroll; ++j) {
+      const int k = k0 + j * kWarp;
+      w[j] = k < len ? __ldg(lst + k) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j) {
       const int32_t key = w[j];
+      if (key < 0) continue;
       // First bucket in one 128-bit load; the common case (a miss in a bucket with a free
       // slot) ends here without computing a slot.
       const uint32_t bk = hash_bucket(key, bits);
-      const int4 h = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
-      const bool hit = (h.x == key) | (h.y == key) | (h.z == key) | (h.w == key);
-      if (hit | (h.w != -1)) {
-        const int sl = hit ? (int)(4 * bk) + (h.x == key ? 0 : h.y == key ? 1 : h.z == key ? 2 : 3)
-                           : hash_find_after(hkeys, bits, key, bk);
-        if (sl >= 0) {
+      const int4 q = *reinterpret_cast<const int4*>(hkeys + 4 * bk);
+      const bool hit = (q.x == key) | (q.y == key) | (q.z == key) | (q.w == key);
+      if (hit | (q.w != -1)) {
+        const int s = hit ? (int)(4 * bk) + (q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : 3)
+                          : hash_find_after(hkeys, bits, key, bk);
+        if (s >= 0) {
           ++hits;
           if (handle_like<PV>()) {
-            atomicAdd(&cnt[sl], 1u);
+            atomicAdd(&cnt[s], 1u);
           } else if (PV == TC_PV_CSR) {
             uint32_t wc, wo, ww;
             tri_weights<PV>(c, o, key, wc, wo, ww);
             c_acc += wc;
             vacc += wo;
-            if (ww) atomicAdd(&cnt[sl], ww);
+            if (ww) atomicAdd(&cnt[s], ww);
           }
         }
       }
@@ -345,26 +343,21 @@ __device__ __forceinline__ uint32_t probe_list(const int32_t* __restrict__ indp,
   return hits;
 }
 
-// One lane walks a whole (short) list indp[base .. base + len) in aligned 16-byte units, two
-// in flight; returns the hits. The lanes of a warp walk different lists at once, so short lists
-// do not leave most of the warp idle.
+// One lane walks a whole (short) list lst[0 .. len), kUnroll entries in flight; returns the
+// hits. The lanes of a warp walk different lists at once, so short lists do not leave most of
+// the warp idle.
 template <int PV>
-__device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ indp, const int64_t base, const int len,
-                                              const int32_t c, const int32_t o, const int32_t* hkeys, const int bits,
+__device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, const int len, const int32_t c,
+                                              const int32_t o, const int32_t* hkeys, const int bits,
                                               uint32_t* cnt, uint32_t& c_acc, uint32_t& vacc) {
-  const int64_t a0 = base & ~int64_t(3);
-  const int skip = (int)(base - a0);
-  const int nvec = (skip + len + 3) >> 2;
-  const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
   uint32_t hits = 0;
-  for (int i = 0; i < nvec; i += 2) {
-    const int4 q0 = __ldg(vec + i);
-    const int4 q1 = i + 1 < nvec ? __ldg(vec + i + 1) : make_int4(-1, -1, -1, -1);
-    const int32_t w[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    const int e0 = 4 * i - skip;
+  for (int k0 = 0; k0 < len; k0 += kUnroll) {
+    int32_t w[kUnroll];
 #pragma unroll
-    for (int j = 0; j < 8; ++j)
-      if (e0 + j >= 0 && e0 + j < len) hits += probe_one<PV>(w[j], c, o, hkeys, bits, cnt, c_acc, vacc);
+    for (int j = 0; j < kUnroll; ++j) w[j] = k0 + j < len ? __ldg(lst + k0 + j) : -1;
+#pragma unroll
+    for (int j = 0; j < kUnroll; ++j)
+      if (w[j] >= 0) hits += probe_one<PV>(w[j], c, o, hkeys, bits, cnt, c_acc, vacc);
   }
   return hits;
 }
@@ -404,7 +397,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
   if (__any_sync(kFull, by_lane)) {
     if (by_lane) {
       uint32_t vacc = 0;
-      const uint32_t hits = walk_list<PV>(indp, base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
+      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
       tri += hits;
       if (handle_like<PV>()) {
         c_acc += hits;
@@ -468,7 +461,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     const int sb = __shfl_sync(kFull, b, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
     uint32_t vacc = 0;
-    const uint32_t hits = probe_list<PV>(indp, sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
+    const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
     tri += hits;
     if (handle_like<PV>()) {
       c_acc += hits;
@@ -499,21 +492,7 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
     t.cnt[s] = 0;
   }
   __syncwarp();
-  {
-    // N+(c) in aligned 16-byte units (a <= kWarpTierMax: at most 33 units, about one per lane)
-    const int64_t a0 = start & ~int64_t(3);
-    const int skip = (int)(start - a0);
-    const int nvec = (skip + a + 3) >> 2;
-    const int4* __restrict__ vec = reinterpret_cast<const int4*>(indp + a0);
-    for (int i = lane; i < nvec; i += kWarp) {
-      const int4 q = __ldg(vec + i);
-      const int32_t w[4] = {q.x, q.y, q.z, q.w};
-      const int e0 = 4 * i - skip;
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (e0 + j >= 0 && e0 + j < a) hash_insert(t.hkeys, bits, w[j]);
-    }
-  }
+  for (int j = lane; j < a; j += kWarp) hash_insert(t.hkeys, bits, __ldg(indp + start + j));
   __syncwarp();
   uint32_t c_acc = 0;
   for (int g = k0; g < k1; g += kWarp)

@@ -756,8 +756,17 @@ __device__ __forceinline__ void delta_flush(unsigned long long tri_acc, unsigned
   }
 }
 
-// The triangle delta of the changed edges, one warp per edge (entries e = this rank's shard,
-// warp-strided). An edge whose shorter list is longer than A.split_min (two hubs) would be one
+// Rank that counts the changed edge {x, y} of a sharded count: a hash of the edge's canonical
+// key, so every rank assigns each edge alike whatever the order of its own lists.
+__device__ __forceinline__ int edge_shard(int32_t x, int32_t y, int nshards) {
+  uint64_t z = ekey(x, y) + 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return (int)((z ^ (z >> 31)) % (uint64_t)nshards);
+}
+
+// The triangle delta of the changed edges, one warp per edge (warp-strided; with shards, only
+// this rank's edges). An edge whose shorter list is longer than A.split_min (two hubs) would be one
 // warp's serial tail of the whole launch: when A.split_items is set it is queued instead as
 // items of A.chunk entries of its shorter list, which the item pass spreads over all warps (a
 // full queue leaves the edge to this warp). Lane 0 of each warp accumulates the kept triangles
@@ -768,11 +777,11 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
                                               unsigned long long& bytes_acc) {
   const int lane = threadIdx.x & 31;
   const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
-  const int64_t ns = A.nshards > 1 ? A.nshards : 1;
-  for (int64_t e = gw * ns + (ns > 1 ? A.shard : 0); e < cnt; e += nw * ns) {
+  for (int64_t e = gw; e < cnt; e += nw) {
     int32_t x, y;
     bool count_total;
     if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
+    if (A.nshards > 1 && edge_shard(x, y, A.nshards) != A.shard) continue;
     const int32_t lx = A.g.len(x), ly = A.g.len(y);
     if (lx < 2 || ly < 2) continue;
     const int64_t sx = A.g.start(x), sy = A.g.start(y);

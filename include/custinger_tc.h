@@ -76,7 +76,7 @@ typedef struct tc_sched {
   int32_t nshards;        /* `nshards`. Static count: a contiguous range of edge centres, the ranges
                              balanced by each centre's predicted intersection work (every rank
                              computes the same ranges from the same graph). Streaming: the changed
-                             edges e with e % nshards == shard. Per-vertex outputs and totals are
+                             edges whose canonical key hashes to `shard` (mod nshards). Per-vertex outputs and totals are
                              then partial sums that add up over the shards. */
   int32_t cell_filter;    /* timing mode for scheduler training: -1 = intersect every edge (normal),
                              -2 = none, c >= 0 = only edges of degree cell c (16*log2 d_a + log2 d_b);

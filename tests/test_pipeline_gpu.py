@@ -209,8 +209,8 @@ def test_delta_kernel_wait_bound_reports_timeout_and_device_stays_usable():
 
 
 def test_streaming_shards_add_up():
-    """Two ranks' shares of the delta count (changed edges e % 2 == 0 and == 1), run one after the
-    other on twin graphs, add up to the unsharded count, totals and per-vertex."""
+    """Two ranks' shares of the delta count (the changed edges whose key hashes to 0 and to 1), run
+    one after the other on twin graphs, add up to the unsharded count, totals and per-vertex."""
     torch = _torch()
     rng = np.random.default_rng(14)
     base = G.rmat(12, 16, seed=6)
