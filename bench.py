@@ -531,6 +531,10 @@ def run_ours(a, rank, world, local_rank):
             result["streaming"]["fixed"] = {k: fx[k] for k in ("value", "ms_total", "updates", "recount_checks",
                                                                   "scheduler", "delta_kernel_ms")}
             result["streaming"]["fixed"]["learned_over_fixed"] = round(result["streaming"]["value"] / fx["value"], 4)
+            if fx.get("delta_kernel_ms") and result["streaming"].get("delta_kernel_ms"):
+                # the kernels the learned table schedules: the two delta kernels of every batch
+                result["streaming"]["fixed"]["delta_kernel_learned_over_fixed"] = round(
+                    fx["delta_kernel_ms"] / result["streaming"]["delta_kernel_ms"], 4)
         result["scheduler"]["streaming"] = result["streaming"]["scheduler"]
 
     clocks.stop()

@@ -533,8 +533,6 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
   uint32_t tri = 0;
   const unsigned n_large = st->n_large;
   const unsigned n_medium = st->n_medium;
-  const bool sharded = st->sharded != 0;
-  const int32_t s_lo = (int32_t)st->shard_lo, s_hi = (int32_t)st->shard_hi;
 
   // CTA tier: one CTA per item (centre with a > warp_max, kCtaRange of its neighbours), over
   // chunks of kChunk entries of N+(c), each staged into shared memory by one bulk copy.
@@ -648,6 +646,9 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
     c0 = __shfl_sync(kFull, c0, 0);
     if (c0 >= (unsigned long long)n) break;
     const int32_t cend = (int32_t)min((unsigned long long)n, c0 + (unsigned long long)sp.chunk);
+    // this count's centres (all of them unless sharded), read per claimed chunk
+    const bool sharded = st->sharded != 0;
+    const int32_t s_lo = (int32_t)st->shard_lo, s_hi = (int32_t)st->shard_hi;
     for (int32_t ub = (int32_t)c0; ub < cend; ub += kWarp) {
       const int32_t uu = ub + lane;
       const bool in = uu < cend;

@@ -87,8 +87,20 @@ def test_learned_table_is_exact_and_reports_gain(spec):
     assert r["counts_equal"]
     g = L.make_graph(spec)
     assert r["triangles"] == O.fast_count(g.n, g.off, g.ind, per_vertex=False)[0] // 6
-    # the fallback keeps the learned table from losing much where it departs from the rule
-    assert r["learned_ms"] <= 1.15 * r["fixed_ms"] + 0.05
+    # the fallback keeps the table from losing where it departs from the rule (timing noise aside)
+    assert r["learned_ms"] <= 1.03 * r["fixed_ms"] + 0.02
+
+
+@needs_weights
+def test_learned_static_table_gains_on_a_held_out_graph():
+    """Erdos-Renyi n = 2^20, average degree 32 (not a training graph): its lists are mostly 16-64
+    entries, where the network departs from the length thresholds; the learned table must beat
+    the fixed rule there, with the same counts."""
+    params = L.load()
+    r = L.evaluate_graph(params, ("er", dict(n_log=20, deg=32, seed=20)), reps=7)
+    print(json.dumps(r))
+    assert r["counts_equal"]
+    assert r["gain"] >= 1.02, r
 
 
 needs_stream_weights = pytest.mark.skipif(not os.path.exists(L.STREAM_WEIGHTS),
@@ -101,6 +113,18 @@ def test_learned_stream_table_is_exact_and_reports_gain():
     r = L.evaluate_stream_graph(params, ("ba", dict(n_log=16, m0=16, seed=1601)), k=50000, reps=3)
     print(json.dumps(r))
     assert r["counts_equal"]
+
+
+@needs_stream_weights
+def test_learned_stream_table_gains_on_the_held_out_rmat22():
+    """The streaming workload's base graph (R-MAT 22, seed 4; not a training graph): the delta
+    count of 400k of its edges with the learned search/merge table must be at least 10 % faster
+    than with the fixed ratio rule, with the same count."""
+    params = L.load(L.STREAM_WEIGHTS)
+    r = L.evaluate_stream_graph(params, ("rmat", dict(scale=22, a=0.57, seed=4)), k=400000, reps=5)
+    print(json.dumps(r))
+    assert r["counts_equal"]
+    assert r["gain"] >= 1.10, r
 
 
 def test_untrained_stream_network_keeps_the_pipeline_exact():
