@@ -75,6 +75,7 @@ def parse(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-rule comparison runs")
+    ap.add_argument("--no-split", action="store_true", help="skip the one-GPU measurement of the multi-GPU split")
     ap.add_argument("--no-streaming", action="store_true")
     ap.add_argument("--stream-scale", type=int, default=22)
     ap.add_argument("--stream-batches", type=int, default=200)
@@ -437,7 +438,41 @@ def static_workload(ctx, g, scale, ef, seed, steps, warmup, fixed_too, e2e):
                         "kernel_learned_over_fixed": round(statistics.mean(f_count) / statistics.mean(count_ms), 4)}
     if e2e:
         res["e2e"] = e2e_static(ctx, g, e_int, out, tri, sched, steps, warmup, T_full)
+    if ctx.world == 1 and not ctx.a.no_split:
+        res["multi_gpu_split"] = split_balance(graph, out, sched, T_full)
     return res, graph
+
+
+def split_balance(graph, out, sched, T_full, counts=(2, 4, 8), reps=3):
+    """The multi-GPU split measured on one GPU: for N ranks, each shard r counted alone (the count
+    rank r would run), its centre range, predicted work and best count-kernel time; the shards'
+    totals must add up to the whole count. Reports max/mean of work and of time per N."""
+    import copy
+    from custingeralg_b200 import native as N
+    N.lib().tc_profile_enable(1)
+    rows = {}
+    for n_sh in counts:
+        works, times, total = [], [], 0
+        for r in range(n_sh):
+            sc = copy.copy(sched)
+            sc.shard, sc.nshards = r, n_sh
+            best = float("inf")
+            for _ in range(reps):
+                T, info = graph.count(N.TC_PV_HANDLE, out, sched=sc)
+                pt = N.PhaseTimes()
+                N.check(N.lib().tc_profile_last(pt))
+                best = min(best, pt.count_ms)
+            total += T
+            works.append(info.shard_work)
+            times.append(best)
+        if total != T_full:
+            raise SystemExit(f"{n_sh} shards add up to {total}, not {T_full}")
+        rows[str(n_sh)] = {"work_max_over_mean": round(max(works) / (sum(works) / n_sh), 4),
+                           "kernel_ms_max_over_mean": round(max(times) / (sum(times) / n_sh), 4),
+                           "kernel_ms_per_shard": [round(t, 3) for t in times]}
+    N.lib().tc_profile_enable(0)
+    return {"note": "each shard of N counted alone on one GPU (the work rank r of N would do); shard totals add "
+                    "up to the whole count", "by_ranks": rows}
 
 
 def e2e_static(ctx, g, e_int, out, tri, sched, steps, warmup, T_full):
@@ -511,7 +546,7 @@ def run_ours(a, rank, world, local_rank):
     if world > 1:
         result["parallelism"] = (f"{world} ranks: contiguous edge-centre ranges balanced by predicted work, "
                                  "NCCL all-reduce of per-vertex counts and total inside the step")
-    for k in ("fixed", "e2e"):
+    for k in ("fixed", "e2e", "multi_gpu_split"):
         if k in main:
             result[k] = main[k]
     del g

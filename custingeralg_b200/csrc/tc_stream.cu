@@ -697,24 +697,44 @@ __device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaP
     // The first five search levels come from 32 evenly spaced samples of the longer list, one
     // per lane (a single coalesced load): a lane counts the samples below its key with
     // shuffles, then searches memory only inside that bucket.
+    // Each lane searches two entries at once (two independent chains of loads in flight).
     const int64_t step = ((int64_t)P.lb + 31) / 32;
     const int32_t smp = (int64_t)lane * step < P.lb ? L[sb + (int64_t)lane * step] : INT32_MAX;
     const int32_t s31 = __shfl_sync(kFull, smp, 31);
-    for (int32_t base = i_begin; base < i_end; base += 32) {
-      const int32_t i = base + lane;
-      const bool in = i < i_end;
-      const int32_t w = in ? L[P.sa + i] : INT32_MAX;
+    // [lo, hi): the part of the longer list between the samples around w
+    auto bucket = [&](const int32_t w, int64_t& lo, int64_t& hi) {
       int pos = 0;  // samples below w (they ascend with the lane)
 #pragma unroll
       for (int st = 16; st > 0; st >>= 1)
         if (__shfl_sync(kFull, smp, pos + st - 1) < w) pos += st;
       if (pos == 31 && s31 < w) pos = 32;
-      if (in) {
-        const int64_t lo = pos > 0 ? (int64_t)(pos - 1) * step + 1 : 0;
-        const int64_t hi = pos < 32 ? min((int64_t)pos * step, (int64_t)P.lb) : (int64_t)P.lb;
-        const int64_t p = lower_bound(L, sb + lo, sb + hi, w);
-        if (p < eb && L[p] == w) on_match(i, p - sb, w);
+      lo = sb + (pos > 0 ? (int64_t)(pos - 1) * step + 1 : 0);
+      hi = sb + (pos < 32 ? min((int64_t)pos * step, (int64_t)P.lb) : (int64_t)P.lb);
+    };
+    for (int32_t base = i_begin; base < i_end; base += 64) {
+      const int32_t i = base + lane, i2 = i + 32;
+      const bool in = i < i_end, in2 = i2 < i_end;
+      const int32_t w = in ? L[P.sa + i] : INT32_MAX;
+      const int32_t w2 = in2 ? L[P.sa + i2] : INT32_MAX;
+      int64_t lo, hi, lo2, hi2;
+      bucket(w, lo, hi);
+      bucket(w2, lo2, hi2);
+      if (!in) lo = hi;
+      if (!in2) lo2 = hi2;
+      while (lo < hi || lo2 < hi2) {  // two lower bounds, one step of each per round
+        if (lo < hi) {
+          const int64_t mid = lo + ((hi - lo) >> 1);
+          if (__ldg(L + mid) < w) lo = mid + 1;
+          else hi = mid;
+        }
+        if (lo2 < hi2) {
+          const int64_t mid = lo2 + ((hi2 - lo2) >> 1);
+          if (__ldg(L + mid) < w2) lo2 = mid + 1;
+          else hi2 = mid;
+        }
       }
+      if (in && lo < eb && L[lo] == w) on_match(i, lo - sb, w);
+      if (in2 && lo2 < eb && L[lo2] == w2) on_match(i2, lo2 - sb, w2);
     }
   } else {
     const int32_t len = i_end - i_begin;
