@@ -23,8 +23,10 @@
 //     work is the sum over edges of min(d+u, d+v). k_count is a persistent grid; a centre walks
 //     its original neighbour list N(c) in groups of 32 and takes the neighbours it is centre
 //     for. Tiers by a = d+(c):
-//       CTA   a > warp_max: one CTA per item of 4096 neighbours, N+(c) staged 1024 entries per
-//             pass in the full 2048-slot table (load <= 0.25 up to 512 entries);
+//       CTA   a > warp_max: one CTA per item of 4096 neighbours, N+(c) staged in the full
+//             2048-slot table (load <= 0.25 up to 512 entries) in passes of at most 1024
+//             entries split evenly; a pass holds a value range of N+(c), and each streamed list
+//             is cut to that range by binary search, so no list entry is probed twice;
 //       warp  1 <= a <= warp_max (at most 128): one warp per centre (items of 256 neighbours for
 //             centres with more), a warp-private set of up to 256 slots.
 //     CTAs of 4 warps, 12 resident per SM (40 registers, 16 KB of shared memory each).
@@ -110,6 +112,9 @@ struct BlockTable {
   uint32_t cnt[kHashMax];
 };
 
+// Dynamic shared memory of k_count, laid out as CountSmem.
+extern __shared__ __align__(16) unsigned char smem_raw[];
+
 struct CountSmem {
   union {
     BlockTable L;
@@ -119,6 +124,10 @@ struct CountSmem {
   unsigned long long item;
   uint64_t mbar;  // completion of the bulk copy that stages a CTA-tier chunk
   int gctr;
+  // Value range [vlo, vhi) of the CTA-tier pass in flight when its centre takes several passes
+  // (ranged = 1; 0 for a centre of one pass). Only the CTA tier reads them.
+  int ranged;
+  int32_t vlo, vhi;
 };
 
 // ---- bulk copies into shared memory (cp.async.bulk, completion on an mbarrier) ----------------
@@ -362,6 +371,25 @@ __device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, c
   return hits;
 }
 
+// First index of the ascending list lst[0 .. len) whose entry is >= key (one lane, binary search).
+__device__ __forceinline__ int lower_bound_list(const int32_t* __restrict__ lst, int len, const int32_t key) {
+  int lo = 0;
+  while (len > 0) {
+    const int half = len >> 1;
+    if (__ldg(lst + lo + half) < key) {
+      lo += half + 1;
+      len -= half + 1;
+    } else {
+      len = half;
+    }
+  }
+  return lo;
+}
+
+// Lists at most this long are walked whole in a value-range pass (entries outside the pass's
+// range just miss the hash set); longer ones are first cut to the range by two binary searches.
+constexpr int kRangeSearchMin = 32;
+
 // One warp takes the neighbours o = nbr[0 .. gcount) of centre c (out-degree a) and
 // intersects every edge {c, o} whose centre is c: N+(o), the shorter list (b <= a entries), goes
 // through the hash set of the staged chunk of N+(c) (2^bits buckets, cnt[slot] the counter of
@@ -373,7 +401,12 @@ __device__ __forceinline__ uint32_t walk_list(const int32_t* __restrict__ lst, c
 //           mid-size lists takes a few rounds of coalesced loads instead of one per list;
 //   warp:   the lists are taken one at a time and the warp streams each with coalesced loads,
 //           so o, its list and its count stay warp-uniform.
-template <int PV>
+// When the hash set holds only the entries of N+(c) in [vlo, vhi) (one pass of a centre whose
+// N+(c) is larger than a table), only the part of each N+(o) inside that range is walked: both
+// lists are ascending, so no entry outside it can hit. The range sits in shared memory
+// (CountSmem::ranged, vlo, vhi), so it holds no register across the group loop; kMayRange (the
+// CTA tier) compiles the cut in, the warp tiers (one pass always) leave it out.
+template <int PV, bool kMayRange>
 __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, const int a,
                                               const int32_t* __restrict__ nbr, const int gcount,
                                               const int32_t* hkeys, const int bits, uint32_t* cnt, const int32_t* __restrict__ dplus,
@@ -388,16 +421,30 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
   const bool mine = valid && b > 0 && centre_of(c, a, o, b) &&
                     (sp.cell_filter == -1 ||
                      (sp.cell_filter >= 0 && log2_cell(a) * 16 + log2_cell(b) == sp.cell_filter));
-  const int64_t base = mine ? __ldg(offp + o) : 0;
-  const int strat = !mine ? -1
-                    : sp.use_table ? sp.table[log2_cell(a)][log2_cell(b)]
-                                   : (b <= sp.lane_max ? 1 : b <= sp.packed_max ? 2 : 0);
+  int64_t base = mine ? __ldg(offp + o) : 0;
+  int strat = !mine ? -1
+              : sp.use_table ? sp.table[log2_cell(a)][log2_cell(b)]
+                             : (b <= sp.lane_max ? 1 : b <= sp.packed_max ? 2 : 0);
+  int len = b;  // entries of N+(o) walked, from indp[base]
+  const CountSmem& sm = *reinterpret_cast<const CountSmem*>(smem_raw);
+  if (kMayRange && sm.ranged) {  // uniform over the CTA
+    if (strat >= 0 && b > kRangeSearchMin) {
+      const int32_t vlo = sm.vlo, vhi = sm.vhi;
+      const int32_t* lst = indp + base;
+      const int p0 = vlo == INT_MIN ? 0 : lower_bound_list(lst, b, vlo);
+      const int p1 = vhi == INT_MAX ? b : p0 + lower_bound_list(lst + p0, b - p0, vhi);
+      base += p0;
+      len = p1 - p0;
+      if (len == 0) strat = -1;
+    }
+    __syncwarp();
+  }
   const bool by_lane = strat == 1;
   const bool by_pack = strat == 2;
   if (__any_sync(kFull, by_lane)) {
     if (by_lane) {
       uint32_t vacc = 0;
-      const uint32_t hits = walk_list<PV>(indp + base, b, c, o, hkeys, bits, cnt, c_acc, vacc);
+      const uint32_t hits = walk_list<PV>(indp + base, len, c, o, hkeys, bits, cnt, c_acc, vacc);
       tri += hits;
       if (handle_like<PV>()) {
         c_acc += hits;
@@ -408,7 +455,7 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     __syncwarp();
   }
   if (__any_sync(kFull, by_pack)) {
-    const int len_l = by_pack ? b : 0;
+    const int len_l = by_pack ? len : 0;
     int incl = len_l;
 #pragma unroll
     for (int d = 1; d < kWarp; d <<= 1) {
@@ -453,12 +500,12 @@ __device__ __forceinline__ void process_group(const int32_t n, const int32_t c, 
     }
     __syncwarp();
   }
-  unsigned todo = __ballot_sync(kFull, mine && !by_lane && !by_pack);
+  unsigned todo = __ballot_sync(kFull, strat == 0);
   while (todo) {
     const int sl = __ffs(todo) - 1;
     todo &= todo - 1;
     const int32_t so = __shfl_sync(kFull, o, sl);
-    const int sb = __shfl_sync(kFull, b, sl);
+    const int sb = __shfl_sync(kFull, len, sl);
     const int64_t sbase = __shfl_sync(kFull, base, sl);
     uint32_t vacc = 0;
     const uint32_t hits = probe_list<PV>(indp + sbase, sb, c, so, hkeys, bits, cnt, c_acc, vacc);
@@ -496,8 +543,8 @@ __device__ __forceinline__ void warp_centre(const int32_t n, const int32_t c, co
   __syncwarp();
   uint32_t c_acc = 0;
   for (int g = k0; g < k1; g += kWarp)
-    process_group<PV>(n, c, a, ind + start + g, min(kWarp, k1 - g), t.hkeys, bits, t.cnt, dplus, offp, indp, out,
-                      sp, tri, c_acc);
+    process_group<PV, false>(n, c, a, ind + start + g, min(kWarp, k1 - g), t.hkeys, bits, t.cnt, dplus, offp, indp,
+                             out, sp, tri, c_acc);
   if (PV != TC_PV_NONE) {
     for (int s = lane; s < S; s += kWarp) {
       const uint32_t x = t.cnt[s];
@@ -526,7 +573,6 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
                                                     uint32_t* __restrict__ out, DevStatus* __restrict__ st,
                                                     const SchedParams sp) {
   TC_DBG_ENTER(6);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   CountSmem& sm = *reinterpret_cast<CountSmem*>(smem_raw);
   const int lane = threadIdx.x & (kWarp - 1);
   const int wid = threadIdx.x / kWarp;
@@ -537,7 +583,10 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
   // CTA tier: one CTA per item (centre with a > warp_max, kCtaRange of its neighbours), over
   // chunks of kChunk entries of N+(c), each staged into shared memory by one bulk copy.
   BlockTable& L = sm.t.L;
-  if (threadIdx.x == 0) mbar_init(&sm.mbar);
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.mbar);
+    sm.ranged = 0;
+  }
   __syncthreads();
   uint32_t stage_phase = 0;
   while (true) {
@@ -556,8 +605,13 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
     const int64_t start = offp[c];
     const int32_t k1 = min(degv[c], k0 + kCtaRange);
     uint32_t c_acc = 0;
-    for (int cb = 0; cb < a; cb += kChunk) {
-      const int clen = min(kChunk, a - cb);
+    // N+(c) in passes of at most kChunk entries, split evenly; pass pk holds the entries of N+(c)
+    // in [vlo, vhi), and only that part of each streamed list is walked in it.
+    const int passes = (a + kChunk - 1) / kChunk;
+    for (int pk = 0; pk < passes; ++pk) {
+      const int cb = (int)(((int64_t)pk * a) / passes);
+      const int cb_next = (int)(((int64_t)(pk + 1) * a) / passes);
+      const int clen = cb_next - cb;
       // the whole table whatever clen: load clen / kHashMax (<= 0.25 up to 512 entries, <= 0.5)
       constexpr int bits = 9;
       static_assert((4 << bits) == kHashMax, "CTA table size");
@@ -582,6 +636,11 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
         mbar_wait(&sm.mbar, stage_phase ^ 1u);
         return;
       }
+      if (threadIdx.x == 0) {
+        sm.ranged = passes > 1;
+        sm.vlo = pk == 0 ? INT_MIN : stage[skip];
+        sm.vhi = pk + 1 == passes ? INT_MAX : __ldg(indp + start + cb_next);
+      }
       for (int j = threadIdx.x; j < clen; j += kThreads) hash_insert(L.hkeys, bits, stage[skip + j]);
       __syncwarp();
       __syncthreads();
@@ -596,8 +655,8 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
         g = __shfl_sync(kFull, g, 0);
         if (g >= ngroups) break;
         const int gk = k0 + g * kWarp;
-        process_group<PV>(n, c, a, ind + start + gk, min(kWarp, k1 - gk), L.hkeys, bits, L.cnt, dplus, offp, indp,
-                          out, sp, tri, c_acc);
+        process_group<PV, true>(n, c, a, ind + start + gk, min(kWarp, k1 - gk), L.hkeys, bits, L.cnt, dplus, offp,
+                                indp, out, sp, tri, c_acc);
       }
       __syncwarp();
       __syncthreads();
@@ -610,6 +669,7 @@ __global__ void __launch_bounds__(kThreads, 12) k_count(const int32_t n, const i
       __syncwarp();
       __syncthreads();
     }
+    if (threadIdx.x == 0) sm.ranged = 0;  // the next item sets it again before its first group
     if (PV != TC_PV_NONE) {
       c_acc = __reduce_add_sync(kFull, c_acc);
       if (lane == 0 && c_acc) out_add<PV>(out, c, c_acc);

@@ -1,4 +1,6 @@
 """Static triangle count on the GPU through the C ABI, bit-exact against the oracle/fixtures."""
+import functools
+
 import numpy as np
 import pytest
 
@@ -102,6 +104,52 @@ def test_large_out_degree_chunking():
     assert T == n * (n - 1) * (n - 2) // 6
     assert np.array_equal(pv, np.full(n, (n - 1) * (n - 2), dtype=np.int64).astype(np.int32))
     assert info.max_out_degree == n - 1
+
+
+@functools.lru_cache(maxsize=1)
+def _core_periphery_graph():
+    """A dense core of 1200 vertices (edge probability 0.92, so the lowest-ranked core vertices
+    have out-degree above the 1024 entries one CTA table holds, and take two value-range passes)
+    joined to 6000 sparse periphery vertices, whose short lists of core ids are walked whole in
+    each pass, plus a few hundred mid-degree vertices with lists that need the range cut."""
+    rng = np.random.default_rng(1200)
+    core = 1200
+    i, j = np.triu_indices(core, 1)
+    keep = rng.random(i.size) < 0.92
+    src, dst = [i[keep]], [j[keep]]
+    per = np.arange(core, core + 6000)
+    for k in range(3):  # every periphery vertex joins three random core vertices
+        src.append(per)
+        dst.append(rng.integers(0, core, per.size))
+    mid = np.arange(core + 6000, core + 6400)
+    for k in range(150):  # mid-degree vertices: ~150 core neighbours each
+        src.append(mid)
+        dst.append(rng.integers(0, core, mid.size))
+    src.append(rng.integers(core, core + 6400, 20000))  # sparse edges among the rest
+    dst.append(rng.integers(core, core + 6400, 20000))
+    return G.from_pairs(core + 6400, np.concatenate(src), np.concatenate(dst), name="core_periphery")
+
+
+@functools.lru_cache(maxsize=1)
+def _core_periphery_oracle():
+    g = _core_periphery_graph()
+    tot, pv_handle = O.fast_count(g.n, g.off, g.ind)
+    return tot, pv_handle, O.csr_per_vertex(g.n, g.off, g.ind)
+
+
+@pytest.mark.parametrize("sname", ["default", "never_lane_walk", "packed_everywhere", "lane_walk_up_to_64"])
+def test_value_range_passes_vs_oracle(sname):
+    g = _core_periphery_graph()
+    tot, pv_handle, pv_csr = _core_periphery_oracle()
+    kw = SCHEDS[sname]
+    s = sched(**kw) if kw else None
+    T, pv, info = run_handle(g, N.TC_PV_HANDLE, s)
+    assert info.max_out_degree > 1024, "the graph must hold centres that take several passes"
+    assert 6 * T == tot and np.array_equal(pv, pv_handle)
+    T, pv, _ = run_handle(g, N.TC_PV_CSR, s)
+    assert 6 * T == tot and np.array_equal(pv, pv_csr)
+    T, _, _ = run_handle(g, N.TC_PV_NONE, s)
+    assert 6 * T == tot
 
 
 @pytest.mark.parametrize("seed", range(10))
