@@ -297,6 +297,7 @@ void tc_sched_default(tc_sched* s) {
   s->shard = 0;
   s->nshards = 1;
   s->cell_filter = -1;
+  s->stream_hub_min = 8;     // streaming: count at an endpoint holding >= 8 of a phase's changed edges
 }
 
 tc_status tc_count_csr32(int32_t nv, const int32_t* d_off, const int32_t* d_ind, int pv_mode, int32_t* per_vertex,

@@ -150,6 +150,7 @@ struct SchedParams {
   int32_t cell_filter;     // -1 all edges, -2 none, >= 0 only that degree cell
   int32_t lane_max;        // static: lists of at most this many entries are walked by one lane
   int32_t packed_max;      // static: longer lists up to this many entries are walked packed
+  int32_t hub_min;         // streaming: changed edges per longer endpoint for the hub count (0 = off)
   uint8_t table[16][16];
 };
 

@@ -1386,6 +1386,7 @@ SchedParams to_params(const tc_sched* s) {
   p.cell_filter = s->cell_filter < -2 ? -1 : s->cell_filter;
   p.lane_max = std::min(64, std::max(0, s->lane_max_deg));
   p.packed_max = std::max(0, s->packed_max_deg);
+  p.hub_min = std::max(0, s->stream_hub_min);
   memcpy(p.table, s->table, sizeof(p.table));
   return p;
 }

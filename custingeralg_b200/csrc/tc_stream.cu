@@ -62,6 +62,10 @@ struct BatchStatus {
   unsigned int bar[2];            // grid-barrier arrivals of the persistent delta kernels
   unsigned int err;
   unsigned int pad;
+  unsigned long long n_hubs[2];   // hub groups of the delta count (deletions, insertions)
+  unsigned long long hub_total[2];  // changed edges placed in hub groups
+  unsigned long long hub_q[2];    // work-queue heads of the hub kernel
+  unsigned long long hub_items[2];  // hub work items queued
 };
 
 __device__ __forceinline__ uint64_t ekey(int32_t a, int32_t b) {
@@ -603,6 +607,11 @@ struct DeltaArgs {
   unsigned* err;
   unsigned bar_extra;
   unsigned long long spin_ns;
+  // hub-centred counting (k_delta_hub): changed edges whose longer endpoint holds at least
+  // hub_min of the phase's changed edges are counted at that endpoint (0 = never); hubbed[e] = 1
+  // marks them for the per-edge kernel to skip (NULL = no hub groups)
+  int hub_min;
+  const uint8_t* hubbed;
   uint8_t table[256];
 };
 
@@ -798,6 +807,7 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
   const int lane = threadIdx.x & 31;
   const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
   for (int64_t e = gw; e < cnt; e += nw) {
+    if (A.hubbed && A.hubbed[e]) continue;  // counted at its hub (k_delta_hub)
     int32_t x, y;
     bool count_total;
     if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
@@ -945,6 +955,340 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, 
   delta_flush(tri_acc, bytes_acc, tri_out, A.bytes_out);
 }
 
+// ---- hub-centred delta count ------------------------------------------------------------------
+//
+// The changed edges of a batch phase concentrate on few endpoints (R-MAT insertions draw both
+// endpoints by degree). An edge {h, s} whose longer-list endpoint h (ties to the smaller id) holds
+// at least hub_min of the phase's changed edges is counted at h: a CTA hashes N(h) into shared
+// memory, each key with bit 31 set when the edge (h, key) is itself changed (the mark array), and
+// its warps stream the partner lists N(s) through the table with coalesced loads, in units of
+// kHubUnit entries that the warps take one at a time (a long partner list, another hub's, is
+// many units, so no warp holds the others up). Per partner entry that is one shared-memory probe,
+// where the per-edge kernel binary-searches it into the longer list. A hub longer than one table
+// (kHubPass entries) is hashed in value-range passes: pass pk holds the entries of N(h) in
+// [vlo, vhi), and a unit is walked only over its entries in that range (its first and last
+// entries tell whether it meets the range; a warp-cooperative sampled search finds where it
+// enters), so every partner entry is probed once over the passes. A hub's work is cut into items
+// (pass, chunk of its units), each one CTA's table build plus walks, sized so the build is a small
+// part of the item; the items of all hubs share one queue, so no hub is a serial tail.
+// The keep rule is the per-edge kernel's: a common neighbour w is kept unless (h, w) or (s, w) is
+// a changed edge with a smaller key, so every triangle is still attributed to exactly one changed
+// edge whichever kernel counts it. Grouping takes three passes over the changed edges: count the
+// edges, units and partner entries per longer endpoint, where a vertex becomes a hub when its
+// edge count reaches hub_min; give each hub a range of unit slots and its items; place the units
+// and flag the edges hubbed. A hub whose units or items do not fit is left to the per-edge kernel.
+
+#ifndef TC_HUB_THREADS
+#define TC_HUB_THREADS 512
+#endif
+constexpr int kHubThreads = TC_HUB_THREADS;
+constexpr int kHubCtasPerSm = 1536 / kHubThreads;
+constexpr int kHubBucketsMax = 2048 * kHubThreads / 256;  // 64 KB of int32 keys for 512 threads
+constexpr int kHubUnit = 1024;               // partner entries per unit of work of a warp
+constexpr int kHubPass = 2 * kHubBucketsMax;  // entries of N(h) per pass (load <= 0.5)
+constexpr int32_t kHubMarkBit = INT32_MIN;    // bit 31 of a stored key: the edge (h, key) is changed
+constexpr int64_t kHubSearchCost = 64;        // an item's estimate of one range search, in probes
+constexpr int64_t kHubItemMin = 1 << 16;      // probes of work per item at least ...
+constexpr int64_t kHubBuildShare = 16;        // ... and at least this many times its table build
+constexpr int64_t kHubItemsPerUpdate = 4;     // item queue capacity per batch update
+constexpr int64_t kHubUnitsPerUpdate = 4;     // unit slots per batch update
+
+struct HubWs {
+  int32_t* cnt;      // [n] changed edges per longer endpoint in this phase (zero between phases)
+  int32_t* uni;      // [n] their partner units (zero between phases)
+  long long* sum;    // [n] sum of their partner list lengths (zero between phases)
+  int32_t* of;       // [n] hub id + 1 of a vertex (zero between phases)
+  int32_t* list;     // [cap] hub vertices
+  int32_t* off;      // [cap] first slot of a hub's units in `units`
+  int32_t* len;      // [cap] number of units of the hub
+  int32_t* chunks;   // [cap] unit chunks of the hub (items per pass)
+  int32_t* fill;     // [cap]
+  int2* units;       // [unit_cap] (partner s, unit r: entries [r kHubUnit, (r + 1) kHubUnit) of N(s))
+  int64_t unit_cap;
+  uint8_t* hubbed;   // [cap] 1 = counted at its hub
+  unsigned long long* items;  // [item_cap] (hub id << 32 | item index within the hub)
+  int64_t item_cap;
+  unsigned long long* n_hubs;
+  unsigned long long* total;
+  unsigned long long* n_items;
+  unsigned long long* q;
+};
+
+// Changed edge e as the hub count sees it: false unless this rank counts it and both lists have
+// at least two entries (the per-edge kernel's filters); h = the endpoint with the longer list.
+__device__ __forceinline__ bool hub_entry(const DeltaArgs& A, int64_t e, int32_t& h, int32_t& s, int32_t& ls) {
+  int32_t x, y;
+  bool count_total;
+  if (!delta_entry<kPredMark>(A, e, x, y, count_total)) return false;
+  if (A.nshards > 1 && edge_shard(x, y, A.nshards) != A.shard) return false;
+  const int32_t lx = A.g.len(x), ly = A.g.len(y);
+  if (lx < 2 || ly < 2) return false;
+  const bool x_long = lx > ly || (lx == ly && x < y);
+  h = x_long ? x : y;
+  s = x_long ? y : x;
+  ls = x_long ? ly : lx;
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads) k_hub_count(const DeltaArgs A, const HubWs H) {
+  const int64_t cnt = (int64_t)*A.count_dev;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+    int32_t h, s, ls;
+    if (!hub_entry(A, e, h, s, ls)) continue;
+    atomicAdd(reinterpret_cast<unsigned long long*>(&H.sum[h]), (unsigned long long)ls);
+    atomicAdd(&H.uni[h], (ls + kHubUnit - 1) / kHubUnit);
+    if (atomicAdd(&H.cnt[h], 1) + 1 == A.hub_min) {  // exactly one edge sees the count reach hub_min
+      const unsigned long long hid = atomicAdd(H.n_hubs, 1ull);
+      H.list[hid] = h;
+      H.of[h] = (int32_t)hid + 1;
+    }
+  }
+}
+
+// Passes of a hub of lh entries, and the value range of pass pk: its entries are N(h)[cb, cb_next).
+__device__ __forceinline__ int hub_passes(int32_t lh) { return (lh + kHubPass - 1) / kHubPass; }
+
+// Unit slots and items per hub, allocated by atomics; a hub whose units or items do not fit drops
+// out (its edges go to the per-edge kernel).
+__global__ void __launch_bounds__(kThreads) k_hub_alloc(const DeltaArgs A, const HubWs H) {
+  const int64_t nh = (int64_t)*H.n_hubs;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nh; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t h = H.list[i];
+    const int32_t k = H.uni[h];
+    const int32_t lh = A.g.len(h);
+    H.len[i] = 0;
+    const unsigned long long off = atomicAdd(H.total, (unsigned long long)k);
+    if (off + k > (unsigned long long)H.unit_cap) {
+      H.of[h] = 0;
+      continue;
+    }
+    const int P = hub_passes(lh);
+    // probes of the hub's walks and searches, over the items' target size
+    const long long work = H.sum[h] + (long long)(P - 1) * k * kHubSearchCost;
+    const long long build = kHubBuildShare * ((long long)lh / P);
+    const long long target = build > (long long)kHubItemMin ? build : (long long)kHubItemMin;
+    const long long want = (work + target - 1) / target;
+    const int C = (int)(want < 1 ? 1 : want > k ? k : want);
+    const long long nitems = (long long)P * C;
+    const unsigned long long base = atomicAdd(H.n_items, (unsigned long long)nitems);
+    if (base + nitems > (unsigned long long)H.item_cap) {
+      for (long long j = 0; j < nitems && base + j < (unsigned long long)H.item_cap; ++j) H.items[base + j] = kNoItem;
+      H.of[h] = 0;
+      continue;
+    }
+    for (long long j = 0; j < nitems; ++j) H.items[base + j] = ((unsigned long long)i << 32) | (unsigned long long)j;
+    H.len[i] = k;
+    H.chunks[i] = C;
+    H.off[i] = (int32_t)off;
+    H.fill[i] = 0;
+  }
+}
+
+// Place the units of every hub edge in its hub's range and flag the edge; clears the per-vertex
+// counts.
+__global__ void __launch_bounds__(kThreads) k_hub_place(const DeltaArgs A, const HubWs H) {
+  const int64_t cnt = (int64_t)*A.count_dev;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += (int64_t)gridDim.x * blockDim.x) {
+    uint8_t f = 0;
+    int32_t h, s, ls;
+    if (hub_entry(A, e, h, s, ls)) {
+      const int32_t hid1 = H.of[h];
+      if (hid1 > 0) {
+        const int32_t u = (ls + kHubUnit - 1) / kHubUnit;
+        const int32_t pos = H.off[hid1 - 1] + atomicAdd(&H.fill[hid1 - 1], u);
+        for (int32_t r = 0; r < u; ++r) H.units[pos + r] = make_int2(s, r);
+        f = 1;
+      }
+      H.cnt[h] = 0;
+      H.uni[h] = 0;
+      H.sum[h] = 0;
+    }
+    H.hubbed[e] = f;
+  }
+}
+
+__device__ __forceinline__ uint32_t hub_bucket(int32_t w, int bits) {
+  return ((uint32_t)w * 0x9E3779B1u) >> (32 - bits);
+}
+
+// Insert a key (id, with kHubMarkBit when the edge to it is changed) into 2^bits buckets of 4
+// slots (load <= 0.5: a bucket with a free slot is always found).
+__device__ __forceinline__ void hub_insert(int32_t* keys, int bits, int32_t id, int32_t key) {
+  const uint32_t bmask = (1u << bits) - 1;
+  uint32_t b = hub_bucket(id, bits);
+  for (uint32_t it = 0; it <= bmask; ++it) {
+#pragma unroll
+    for (int t = 0; t < 4; ++t)
+      if (atomicCAS(&keys[4 * b + t], -1, key) == -1) return;
+    b = (b + 1) & bmask;
+  }
+}
+
+// Is id in the table? If so, `changed` = its stored mark bit (the edge (h, id) is changed).
+__device__ __forceinline__ bool hub_find(const int32_t* keys, int bits, int32_t id, bool& changed) {
+  const uint32_t bmask = (1u << bits) - 1;
+  uint32_t b = hub_bucket(id, bits);
+  for (uint32_t it = 0; it <= bmask; ++it) {
+    const int4 q = *reinterpret_cast<const int4*>(keys + 4 * b);
+    if ((q.x & INT32_MAX) == id) { changed = q.x < 0; return true; }
+    if ((q.y & INT32_MAX) == id) { changed = q.y < 0; return true; }
+    if ((q.z & INT32_MAX) == id) { changed = q.z < 0; return true; }
+    if ((q.w & INT32_MAX) == id) { changed = q.w < 0; return true; }
+    if (q.w == -1) return false;  // slots fill in order: a free slot ends the probe
+    b = (b + 1) & bmask;
+  }
+  return false;
+}
+
+// First index of the ascending list lst[0 .. len) whose entry is >= key, found by the warp: 32
+// evenly spaced samples per round (one load each lane), so a list of up to 32^r entries takes r
+// rounds. Every lane returns the same index.
+__device__ __forceinline__ int32_t warp_lower_bound(const int32_t* __restrict__ lst, int32_t len, int32_t key) {
+  const int lane = threadIdx.x & 31;
+  int32_t lo = 0, hi = len;  // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
+    const int32_t step = (hi - lo + 31) / 32;
+    const int32_t p = lo + lane * step;
+    const int32_t v = p < hi ? lst[p] : INT32_MAX;
+    const int c = __popc(__ballot_sync(kFull, v < key));  // the samples below key are a prefix
+    const int32_t nlo = c > 0 ? lo + (c - 1) * step + 1 : lo;
+    hi = c < 32 ? min(hi, lo + c * step) : hi;
+    lo = nlo;
+  }
+  const int32_t p = lo + lane;
+  const int32_t v = p < hi ? lst[p] : INT32_MAX;
+  return lo + __popc(__ballot_sync(kFull, v < key));
+}
+
+// Work items of the hubs from one queue: item (hub, j) is pass j / C over unit chunk j % C of the
+// hub's C chunks; its warps walk one unit each.
+__global__ void __launch_bounds__(kHubThreads, kHubCtasPerSm) k_delta_hub(const DeltaArgs A, const HubWs H,
+                                                                          uint32_t* __restrict__ pv,
+                                                                          unsigned long long* __restrict__ tri_out) {
+  extern __shared__ __align__(16) int32_t hub_keys[];
+  __shared__ unsigned long long s_item;
+  __shared__ int s_next;
+  __shared__ unsigned long long s_red[kHubThreads / 32][2];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t n_items = (int64_t)min(*H.n_items, (unsigned long long)H.item_cap);
+  const uint32_t inc = A.weight * (uint32_t)A.sign;
+  unsigned long long tri_acc = 0, bytes_acc = 0;
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned long long q = atomicAdd(H.q, 1ull);
+      s_item = q < (unsigned long long)n_items ? H.items[q] : ~1ull;
+      s_next = 0;
+    }
+    __syncthreads();
+    const unsigned long long item = s_item;
+    if (item == ~1ull) break;
+    if (item == kNoItem) {  // a slot of a hub that did not fit
+      __syncthreads();
+      continue;
+    }
+    const int32_t hid = (int32_t)(item >> 32), j = (int32_t)(item & 0xffffffffu);
+    const int32_t h = H.list[hid], base = H.off[hid], k = H.len[hid], C = H.chunks[hid];
+    const int32_t lh = A.g.len(h);
+    const int64_t sh = A.g.start(h);
+    const int P = hub_passes(lh);
+    const int pk = j / C, ci = j % C;
+    const int32_t per = (k + C - 1) / C;
+    const int32_t e0 = ci * per, e1 = min(k, e0 + per);
+    const int cb = (int)(((int64_t)pk * lh) / P);
+    const int cb_next = (int)(((int64_t)(pk + 1) * lh) / P);
+    const int clen = cb_next - cb;
+    int bits = 4;  // buckets >= clen (load <= 0.25) while they fit, else load <= 0.5
+    while ((1 << bits) < clen && (1 << bits) < kHubBucketsMax) ++bits;
+    const int S = 4 << bits;
+    for (int i = threadIdx.x; i < S; i += kHubThreads) hub_keys[i] = -1;
+    __syncthreads();
+    for (int i = threadIdx.x; i < clen; i += kHubThreads) {
+      const int32_t w = A.g.ind[sh + cb + i];
+      hub_insert(hub_keys, bits, w, A.mark[sh + cb + i] ? (w | kHubMarkBit) : w);
+    }
+    const int32_t vlo = pk == 0 ? INT32_MIN : A.g.ind[sh + cb];
+    const int32_t vhi = pk + 1 == P ? INT32_MAX : A.g.ind[sh + cb_next];
+    __syncthreads();
+    uint32_t hub_c = 0;  // triangles kept at h in this item (lane 0 of each warp)
+    while (true) {
+      int i = 0;
+      if (lane == 0) i = atomicAdd(&s_next, 1);
+      i = e0 + __shfl_sync(kFull, i, 0);
+      if (i >= e1) break;
+      const int2 un = H.units[base + i];
+      const int32_t s = un.x;
+      const int32_t ls = A.g.len(s);
+      const int64_t ss = A.g.start(s);
+      const uint64_t key_hs = ekey(h, s);
+      if (pk == 0 && un.y == 0 && lane == 0) bytes_acc += 4ull * (unsigned long long)(lh + ls) + 8ull;
+      const int32_t c0 = un.y * kHubUnit, c1 = min(ls, c0 + kHubUnit);
+      int32_t cur = c0;
+      if (P > 1) {  // the unit's part in [vlo, vhi), if any
+        const int32_t first = A.g.ind[ss + c0], last = A.g.ind[ss + c1 - 1];
+        if (last < vlo || first >= vhi) continue;
+        if (first < vlo) cur = c0 + warp_lower_bound(A.g.ind + ss + c0, c1 - c0, vlo);
+      }
+      uint32_t c = 0;
+      // N(s)[cur, c1) up to the first entry >= vhi, 128 entries per step (four loads per lane)
+      while (cur < c1) {
+        int32_t w[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const int32_t q = cur + lane + 32 * t;
+          w[t] = q < c1 ? A.g.ind[ss + q] : INT32_MAX;
+        }
+        int n_in = 0;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          const bool in = w[t] < vhi;
+          n_in += __popc(__ballot_sync(kFull, in));
+          bool ch = false;
+          if (in && hub_find(hub_keys, bits, w[t], ch)) {
+            const bool cs = A.mark[ss + cur + lane + 32 * t] != 0;
+            if ((!ch || key_hs < ekey(h, w[t])) && (!cs || key_hs < ekey(s, w[t]))) {
+              ++c;
+              atomicAdd(&pv[w[t]], inc);
+            }
+          }
+          __syncwarp();
+        }
+        cur += n_in;  // the entries below vhi are a prefix of the step (the list ascends)
+        if (n_in < 128) break;
+      }
+      c = warp_sum(c);
+      if (lane == 0 && c) {
+        atomicAdd(&pv[s], c * inc);
+        hub_c += c;
+        tri_acc += c;
+      }
+    }
+    // h's per-vertex count: one atomic per item
+    if (lane == 0) s_red[wid][0] = hub_c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long t = 0;
+      for (int w = 0; w < kHubThreads / 32; ++w) t += s_red[w][0];
+      if (t) atomicAdd(&pv[h], (uint32_t)t * inc);
+      if (j == 0) H.of[h] = 0;  // zero between phases (k_hub_place, its last reader, is done)
+    }
+    __syncthreads();
+  }
+  if (lane == 0) {
+    s_red[wid][0] = tri_acc;
+    s_red[wid][1] = bytes_acc;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long t = 0, b = 0;
+    for (int w = 0; w < kHubThreads / 32; ++w) {
+      t += s_red[w][0];
+      b += s_red[w][1];
+    }
+    if (t) atomicAdd(tri_out, t);
+    if (b && A.bytes_out) atomicAdd(A.bytes_out, b);
+  }
+}
+
 // ---- cuStinger-style batch helpers ------------------------------------------------------------
 
 __global__ void k_pack_dir(const int32_t* __restrict__ s, const int32_t* __restrict__ d, const int64_t b,
@@ -1086,6 +1430,19 @@ struct StreamWs {
   int64_t* scan64 = nullptr;    // [n+1]
   int64_t* tiles = nullptr;
   unsigned long long* split_items = nullptr;  // [kDeltaItems] queued chunks of long intersections
+  // hub groups of the delta count (k_delta_hub)
+  int32_t* hub_cnt = nullptr;     // [n] zero between phases
+  long long* hub_sum = nullptr;   // [n] zero between phases
+  int32_t* hub_uni = nullptr;     // [n] zero between phases
+  int32_t* hub_of = nullptr;      // [n] zero between phases
+  int32_t* hub_list = nullptr;    // [b]
+  int32_t* hub_off = nullptr;     // [b]
+  int32_t* hub_len = nullptr;     // [b]
+  int32_t* hub_fill = nullptr;    // [b]
+  int32_t* hub_chunks = nullptr;  // [b]
+  int2* hub_units = nullptr;      // [kHubUnitsPerUpdate * b]
+  uint8_t* hubbed = nullptr;      // [b]
+  unsigned long long* hub_items = nullptr;  // [kHubItemsPerUpdate * b]
   void release();
 };
 
@@ -1095,6 +1452,9 @@ void StreamWs::release() {
   cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
+  cudaFree(hub_cnt); cudaFree(hub_sum); cudaFree(hub_uni); cudaFree(hub_of); cudaFree(hub_list); cudaFree(hub_off);
+  cudaFree(hub_len); cudaFree(hub_fill); cudaFree(hub_chunks); cudaFree(hub_units); cudaFree(hubbed);
+  cudaFree(hub_items);
   *this = StreamWs();
 }
 
@@ -1124,22 +1484,34 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     g->mark = mk;
   }
   if (w.n_cap < (int64_t)g->n + 1) {
-    cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
-    w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
-    w.n_cap = 0;
+    auto free_pv = [&w]() {
+      cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
+      cudaFree(w.hub_cnt); cudaFree(w.hub_sum); cudaFree(w.hub_uni); cudaFree(w.hub_of);
+      w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
+      w.hub_cnt = nullptr; w.hub_sum = nullptr; w.hub_uni = nullptr; w.hub_of = nullptr;
+      w.n_cap = 0;
+    };
+    free_pv();
     ++w.version;
     const size_t n1 = (size_t)g->n + 1;
     if (::tc::dev_malloc(&w.claim, sizeof(unsigned) * n1) != cudaSuccess ||
         ::tc::dev_malloc(&w.d_epoch, sizeof(unsigned)) != cudaSuccess ||
         ::tc::dev_malloc(&w.cnt, sizeof(int32_t) * n1) != cudaSuccess ||
         ::tc::dev_malloc(&w.scan64, sizeof(int64_t) * (n1 + 1)) != cudaSuccess ||
-        ::tc::dev_malloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)) != cudaSuccess) {
-      cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
-      w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
+        ::tc::dev_malloc(&w.tiles, sizeof(int64_t) * (size_t)(scan_tiles(g->n + 1) + 1)) != cudaSuccess ||
+        ::tc::dev_malloc(&w.hub_cnt, sizeof(int32_t) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.hub_sum, sizeof(long long) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.hub_uni, sizeof(int32_t) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.hub_of, sizeof(int32_t) * n1) != cudaSuccess) {
+      free_pv();
       return fail(TC_ERR_OOM, "batch workspace (per vertex): device allocation failed");
     }
     TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * n1));
     TC_CUDA_TRY(cudaMemset(w.d_epoch, 0, sizeof(unsigned)));
+    TC_CUDA_TRY(cudaMemset(w.hub_cnt, 0, sizeof(int32_t) * n1));
+    TC_CUDA_TRY(cudaMemset(w.hub_sum, 0, sizeof(long long) * n1));
+    TC_CUDA_TRY(cudaMemset(w.hub_uni, 0, sizeof(int32_t) * n1));
+    TC_CUDA_TRY(cudaMemset(w.hub_of, 0, sizeof(int32_t) * n1));
     w.n_cap = g->n + 1;
   }
   if (!w.st || !w.st_host || !w.counter || !w.split_items) {
@@ -1161,9 +1533,13 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
     cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
     cudaFree(w.long_runs); cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
+    cudaFree(w.hub_list); cudaFree(w.hub_off); cudaFree(w.hub_len); cudaFree(w.hub_fill); cudaFree(w.hub_chunks);
+    cudaFree(w.hub_units); cudaFree(w.hubbed); cudaFree(w.hub_items);
     w.src = nullptr; w.dst = nullptr; w.isdel = nullptr; w.keys = nullptr; w.keys2 = nullptr; w.head = nullptr;
     w.dlist = nullptr; w.ilist = nullptr; w.dk = nullptr; w.dk2 = nullptr; w.run_start = nullptr;
     w.long_runs = nullptr; w.ins_slot = nullptr; w.vlist = nullptr; w.cub_tmp = nullptr;
+    w.hub_list = nullptr; w.hub_off = nullptr; w.hub_len = nullptr; w.hub_fill = nullptr; w.hub_chunks = nullptr;
+    w.hub_units = nullptr; w.hubbed = nullptr; w.hub_items = nullptr;
     w.b_cap = 0;
     w.cub_bytes = 0;
   };
@@ -1184,6 +1560,14 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
             ::tc::dev_malloc(&w.long_runs, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.ins_slot, sizeof(int64_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.vlist, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_list, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_off, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_len, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_fill, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_chunks, sizeof(int32_t) * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_units, sizeof(int2) * kHubUnitsPerUpdate * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hubbed, nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.hub_items, sizeof(unsigned long long) * kHubItemsPerUpdate * nb) == cudaSuccess &&
             cub::DeviceRadixSort::SortKeys(nullptr, t1, w.keys, w.keys2, (int)(2 * nb)) == cudaSuccess &&
             cub::DeviceRadixSort::SortKeys(nullptr, t2, w.dk, w.dk2, (int)(2 * nb)) == cudaSuccess &&
             ::tc::dev_malloc(&w.cub_tmp, std::max(t1, t2)) == cudaSuccess;
@@ -1241,6 +1625,7 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
   A.shard = sp.shard;
   A.nshards = sp.nshards;
   A.spin_ns = kSpinNs;
+  A.hub_min = sp.hub_min;
   memcpy(A.table, sp.table, sizeof(A.table));
   return A;
 }
@@ -1266,8 +1651,71 @@ tc_status fused_grid(int ctas_per_sm, int* grid) {
   return TC_OK;
 }
 
+constexpr size_t kHubSmem = sizeof(int32_t) * 4 * kHubBucketsMax;
+
+// Grid of the hub kernel: its occupancy limit of CTAs per SM (64 KB of shared memory each).
+tc_status hub_grid(int* grid) {
+  constexpr int kMaxDev = 64;
+  static int occ[kMaxDev] = {};
+  int dev = 0;
+  TC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDev) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
+  if (occ[dev] == 0) {
+    TC_CUDA_TRY(cudaFuncSetAttribute(k_delta_hub, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHubSmem));
+    int b = 0;
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_delta_hub, kHubThreads, kHubSmem));
+    occ[dev] = std::max(1, b);
+  }
+  *grid = device_info().sms * occ[dev];
+  return TC_OK;
+}
+
+// Hub groups and their count for one phase of a batch (deletions: phase 0, insertions: 1) on a
+// grid of `grid` hub CTAs; `cap` bounds the phase's changed edges. Sets A.hubbed for the
+// per-edge kernel that follows (NULL when the hub count is off: hub_min <= 0, or a timing run of
+// one degree cell). Launches only (it can run inside a stream capture).
+void hub_kernels(DeltaArgs& A, StreamWs& w, int phase, int64_t cap, int grid, uint32_t* pv,
+                 unsigned long long* tri_out, cudaStream_t s) {
+  A.hubbed = nullptr;
+  if (A.hub_min <= 0 || A.cell_filter != -1) return;
+  HubWs H;
+  H.cnt = w.hub_cnt;
+  H.sum = w.hub_sum;
+  H.uni = w.hub_uni;
+  H.of = w.hub_of;
+  H.list = w.hub_list;
+  H.off = w.hub_off;
+  H.len = w.hub_len;
+  H.chunks = w.hub_chunks;
+  H.fill = w.hub_fill;
+  H.units = w.hub_units;
+  H.unit_cap = kHubUnitsPerUpdate * w.b_cap;
+  H.hubbed = w.hubbed;
+  H.items = w.hub_items;
+  H.item_cap = kHubItemsPerUpdate * w.b_cap;
+  H.n_hubs = &w.st->n_hubs[phase];
+  H.total = &w.st->hub_total[phase];
+  H.n_items = &w.st->hub_items[phase];
+  H.q = &w.st->hub_q[phase];
+  const int gb = grid_for(cap, kThreads);
+  k_hub_count<<<gb, kThreads, 0, s>>>(A, H);
+  k_hub_alloc<<<gb, kThreads, 0, s>>>(A, H);
+  k_hub_place<<<gb, kThreads, 0, s>>>(A, H);
+  k_delta_hub<<<grid, kHubThreads, kHubSmem, s>>>(A, H, pv, tri_out);
+  A.hubbed = w.hubbed;
+}
+
+tc_status launch_hub(DeltaArgs& A, StreamWs& w, int phase, int64_t cap, uint32_t* pv, unsigned long long* tri_out,
+                     cudaStream_t s) {
+  int grid = 0;
+  TC_TRY(hub_grid(&grid));
+  hub_kernels(A, w, phase, cap, grid, pv, tri_out, s);
+  TC_CUDA_TRY(cudaGetLastError());
+  return TC_OK;
+}
+
 // The persistent delta kernel of one phase of a batch (deletions: phase 0, insertions: 1) on
-// the batch workspace's counters.
+// the batch workspace's counters, after the hub groups' count.
 tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, unsigned long long* tri_out,
                              int ctas_per_sm, cudaStream_t s) {
   A.split_items = w.split_items;
@@ -1275,6 +1723,7 @@ tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, 
   A.bar = &w.st->bar[phase];
   A.err = &w.st->err;
   A.bytes_out = &w.st->delta_bytes;
+  TC_TRY(launch_hub(A, w, phase, w.b_cap, pv, tri_out, s));
   int grid = 0;
   TC_TRY(fused_grid(ctas_per_sm, &grid));
   k_delta_fused<kPredMark><<<grid, kThreads, 0, s>>>(A, pv, tri_out);
@@ -1743,8 +2192,9 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
   const int gb = grid_for(cap, kThreads);
   const int g2 = grid_for(2 * cap, kThreads);
   const int gw = grid_for(2 * cap * 32, kThreads);
-  int gdelta = 0;
+  int gdelta = 0, ghub = 0;
   TC_TRY(fused_grid(pc.ctas, &gdelta));
+  TC_TRY(hub_grid(&ghub));
   cudaGraph_t graph = nullptr;
   TC_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
@@ -1778,6 +2228,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.err = &w.st->err;
     A.bytes_out = &w.st->delta_bytes;
     if (p->profile) cudaEventRecordWithFlags(p->pev[0], s, cudaEventRecordExternal);
+    hub_kernels(A, w, 0, cap, ghub, pv, &w.st->tri_removed, s);
     k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
     if (p->profile) cudaEventRecordWithFlags(p->pev[1], s, cudaEventRecordExternal);
     k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
@@ -1800,6 +2251,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     B.split_cnt = &w.st->n_split[1];
     B.bar = &w.st->bar[1];
     if (p->profile) cudaEventRecordWithFlags(p->pev[2], s, cudaEventRecordExternal);
+    hub_kernels(B, w, 1, cap, ghub, pv, &w.st->tri_added, s);
     k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
     if (p->profile) cudaEventRecordWithFlags(p->pev[3], s, cudaEventRecordExternal);
     k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);

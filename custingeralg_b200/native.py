@@ -46,7 +46,7 @@ class Sched(ctypes.Structure):
     _fields_ = [("warp_max_deg", _i32), ("search_ratio_x16", _i32), ("blocks_per_sm", _i32),
                 ("chunk", _i32), ("use_table", _i32), ("table", (ctypes.c_uint8 * 16) * 16),
                 ("shard", _i32), ("nshards", _i32), ("cell_filter", _i32), ("lane_max_deg", _i32),
-                ("packed_max_deg", _i32)]
+                ("packed_max_deg", _i32), ("stream_hub_min", _i32)]
 
 
 class CountInfo(ctypes.Structure):

@@ -87,6 +87,10 @@ typedef struct tc_sched {
                              of at most this many entries are packed: the warp walks all such lists
                              of a group of 32 neighbours concatenated, 32 entries per step
                              (0 = never); longer lists are streamed one at a time */
+  int32_t stream_hub_min; /* streaming delta count (tc_apply_batch, tc_pipeline): changed edges whose
+                             longer-list endpoint holds at least this many of a batch phase's
+                             changed edges are counted together at that endpoint, its list hashed
+                             once in shared memory (0 = never; every edge on its own) */
 } tc_sched;
 
 typedef struct tc_graph tc_graph;

@@ -395,3 +395,90 @@ def test_split_intersections_between_hubs(path):
         assert torch.equal(pvn, (pv0.to(torch.int64) + pv[:n].to(torch.int64)).to(torch.int32))
     if pipe is not None:
         pipe.close()
+
+
+def _planted_hubs(rng, n):
+    """Hubs 0-3 with 20000, 9000, 3000 and 600 neighbours (hub 0 takes three passes of the hub
+    table, 8192 entries each), a dense block among 10..2999 so partner lists are long and share
+    many neighbours with the hubs, and a random background."""
+    src, dst = [], []
+    for h, deg in ((0, 20000), (1, 9000), (2, 3000), (3, 600)):
+        src.append(np.full(deg, h, np.int32))
+        dst.append(rng.choice(np.arange(10, n, dtype=np.int32), deg, replace=False))
+    src.append(rng.integers(10, 3000, 150000).astype(np.int32))
+    dst.append(rng.integers(10, 3000, 150000).astype(np.int32))
+    src.append(rng.integers(0, n, 80000).astype(np.int32))
+    dst.append(rng.integers(0, n, 80000).astype(np.int32))
+    return G.from_pairs(n, np.concatenate(src), np.concatenate(dst))
+
+
+def _hub_batch(rng, cur, n):
+    """Insertions and deletions of hub edges (many per hub, so they are counted at the hub) mixed
+    with edges inside the dense block, random ones and edges between the hubs, so triangles with
+    two or three changed edges are common."""
+    src_of = np.repeat(np.arange(n, dtype=np.int32), np.diff(cur.off))
+    parts = []
+    hubs = rng.integers(0, 4, 2500).astype(np.int32)
+    parts.append((hubs, rng.integers(10, 3000, 2500).astype(np.int32), np.zeros(2500, np.uint8)))
+    hub_edges = np.flatnonzero(src_of < 4)
+    pick = rng.choice(hub_edges, 1200, replace=False)
+    parts.append((src_of[pick], cur.ind[pick], np.ones(1200, np.uint8)))
+    parts.append((rng.integers(10, 3000, 1500).astype(np.int32), rng.integers(10, 3000, 1500).astype(np.int32),
+                  np.zeros(1500, np.uint8)))
+    pick = rng.integers(0, cur.m, 1500)
+    parts.append((src_of[pick], cur.ind[pick], np.ones(1500, np.uint8)))
+    # edges between the hubs: partner lists of thousands of entries (several units of work)
+    present = set(zip(src_of[hub_edges].tolist(), cur.ind[hub_edges].tolist()))
+    pairs = [(a, b) for a in range(4) for b in range(a + 1, 4)]
+    parts.append((np.array([a for a, _ in pairs], np.int32), np.array([b for _, b in pairs], np.int32),
+                  np.array([1 if (a, b) in present else 0 for a, b in pairs], np.uint8)))
+    s = np.concatenate([p[0] for p in parts])
+    d = np.concatenate([p[1] for p in parts])
+    x = np.concatenate([p[2] for p in parts])
+    perm = rng.permutation(s.size)
+    return s[perm], d[perm], x[perm]
+
+
+@pytest.mark.parametrize("path", ["pipeline", "apply"])
+def test_hub_groups_match_the_per_edge_count(path):
+    """Changed edges that share their longer endpoint are counted at it (k_delta_hub: the hub's
+    list hashed once, in value-range passes when it is longer than one table). Totals and
+    per-vertex deltas must equal the per-edge kernel's (stream_hub_min = 0) and the recount,
+    batch after batch, for deletions and insertions alike."""
+    torch = _torch()
+    rng = np.random.default_rng(2024)
+    n = 40000
+    base = _planted_hubs(rng, n)
+    assert np.diff(base.off)[0] > 2 * 8192
+    off_hub = N.default_sched()
+    off_hub.stream_hub_min = 0
+    g_hub = api.Graph.from_csr(base, slack=0.25)
+    g_edge = api.Graph.from_csr(base, slack=0.25)
+    T0, pv0 = _recount(g_hub, n)
+    if path == "pipeline":
+        p_hub, p_edge = api.Pipeline(g_hub, 1 << 13), api.Pipeline(g_edge, 1 << 13, sched=off_hub)
+    pv_h = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    pv_e = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
+    d_h = torch.zeros(1, dtype=torch.int64, device="cuda")
+    d_e = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cur = base
+    for it in range(3):
+        ts, td, tx = _dev(torch, *_hub_batch(rng, cur, n))
+        if path == "pipeline":
+            p_hub.apply(ts, td, tx, per_vertex=pv_h, delta_dev=d_h)
+            p_hub.sync()
+            p_edge.apply(ts, td, tx, per_vertex=pv_e, delta_dev=d_e)
+            p_edge.sync()
+        else:
+            g_hub.apply_batch(ts, td, tx, per_vertex=pv_h, delta_dev=d_h)
+            g_edge.apply_batch(ts, td, tx, per_vertex=pv_e, delta_dev=d_e, sched=off_hub)
+        assert int(d_h.item()) == int(d_e.item())
+        assert torch.equal(pv_h, pv_e)
+        T, pvn = _recount(g_hub, n)
+        assert T == T0 + int(d_h.item())
+        assert torch.equal(pvn, (pv0.to(torch.int64) + pv_h[:n].to(torch.int64)).to(torch.int32))
+        off, ind = g_hub.export()
+        cur = G.Csr(n, off, ind)
+    if path == "pipeline":
+        p_hub.close()
+        p_edge.close()
