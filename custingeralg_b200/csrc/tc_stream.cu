@@ -36,6 +36,7 @@ constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longe
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
 constexpr int64_t kDeltaItems = 1 << 20;  // capacity of the split-item queue
 constexpr unsigned long long kNoItem = ~0ull;
+constexpr int kGrab = 4;  // changed edges a warp takes per grab from the delta kernel's queue
 // Bounded wait of the persistent delta kernel's grid barrier (a wait that runs out reports
 // kErrTimeout and the kernel skips the work after the barrier).
 constexpr unsigned long long kSpinNs = 2000000000ull;  // 2 s
@@ -66,6 +67,8 @@ struct BatchStatus {
   unsigned long long hub_total[2];  // changed edges placed in hub groups
   unsigned long long hub_q[2];    // work-queue heads of the hub kernel
   unsigned long long hub_items[2];  // hub work items queued
+  unsigned long long e_next[2];   // work-queue heads of the delta kernel's entry and item passes
+  unsigned long long i_next[2];
 };
 
 __device__ __forceinline__ uint64_t ekey(int32_t a, int32_t b) {
@@ -612,6 +615,9 @@ struct DeltaArgs {
   // marks them for the per-edge kernel to skip (NULL = no hub groups)
   int hub_min;
   const uint8_t* hubbed;
+  // dynamic work queues of k_delta_fused's two passes (zero at launch; NULL = warp-strided)
+  unsigned long long* e_next;
+  unsigned long long* i_next;
   uint8_t table[256];
 };
 
@@ -806,7 +812,23 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
                                               unsigned long long& bytes_acc) {
   const int lane = threadIdx.x & 31;
   const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
-  for (int64_t e = gw; e < cnt; e += nw) {
+  int64_t next = gw, next_end = 0;
+  for (;;) {
+    // the next entry: warp-strided, or from runs of kGrab entries taken from the queue
+    if (A.e_next) {
+      if (next >= next_end) {
+        unsigned long long g = 0;
+        if (lane == 0) g = atomicAdd(A.e_next, (unsigned long long)kGrab);
+        g = __shfl_sync(kFull, g, 0);
+        if ((int64_t)g >= cnt) break;
+        next = (int64_t)g;
+        next_end = min(cnt, next + kGrab);
+      }
+    } else if (next >= cnt) {
+      break;
+    }
+    const int64_t e = next;
+    next += A.e_next ? 1 : nw;
     if (A.hubbed && A.hubbed[e]) continue;  // counted at its hub (k_delta_hub)
     int32_t x, y;
     bool count_total;
@@ -859,7 +881,17 @@ __device__ __forceinline__ void delta_items(const DeltaArgs& A, uint32_t* __rest
   const unsigned long long queued = kCoherent ? __ldcg(A.split_cnt) : *A.split_cnt;
   const int64_t n_items = (int64_t)min(queued, (unsigned long long)kDeltaItems);
   const int64_t cnt = A.count_dev ? (int64_t)(kCoherent ? __ldcg(A.count_dev) : *A.count_dev) : A.count_host;
-  for (int64_t q = gw; q < n_items; q += nw) {
+  for (int64_t q0 = gw;;) {
+    // the next item: warp-strided, or taken one at a time from the queue
+    int64_t q = q0;
+    if (A.i_next) {
+      unsigned long long g = 0;
+      if (lane == 0) g = atomicAdd(A.i_next, 1ull);
+      q = (int64_t)__shfl_sync(kFull, g, 0);
+    } else {
+      q0 += nw;
+    }
+    if (q >= n_items) break;
     const unsigned long long item = kCoherent ? __ldcg(A.split_items + q) : A.split_items[q];
     if (item == kNoItem) continue;
     const int64_t e = (int64_t)(item >> 24);
@@ -1723,6 +1755,8 @@ tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, 
   A.bar = &w.st->bar[phase];
   A.err = &w.st->err;
   A.bytes_out = &w.st->delta_bytes;
+  A.e_next = &w.st->e_next[phase];
+  A.i_next = &w.st->i_next[phase];
   TC_TRY(launch_hub(A, w, phase, w.b_cap, pv, tri_out, s));
   int grid = 0;
   TC_TRY(fused_grid(ctas_per_sm, &grid));
@@ -2042,8 +2076,8 @@ struct PipeCand {
 };
 constexpr int kPipeCands = 5;
 constexpr PipeCand kPipeCand[kPipeCands] = {
-    {0, kDeltaChunk, kDeltaSplit}, {4, kDeltaChunk, kDeltaSplit}, {2, kDeltaChunk, kDeltaSplit},
-    {0, kDeltaChunk / 2, kDeltaSplit / 2}, {0, kDeltaChunk * 2, kDeltaSplit * 2}};
+    {0, kDeltaChunk, kDeltaSplit}, {4, kDeltaChunk, kDeltaSplit}, {0, kDeltaChunk / 2, kDeltaSplit / 2},
+    {0, kDeltaChunk / 4, kDeltaSplit / 4}, {0, kDeltaChunk / 8, kDeltaSplit / 8}};
 constexpr int kPipeArms = kPipeCands + 1;  // + the default shape in the next bin's graph
 constexpr double kMergeSlack = 1.03;
 }  // namespace
@@ -2227,6 +2261,8 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.bar = &w.st->bar[0];
     A.err = &w.st->err;
     A.bytes_out = &w.st->delta_bytes;
+    A.e_next = &w.st->e_next[0];
+    A.i_next = &w.st->i_next[0];
     if (p->profile) cudaEventRecordWithFlags(p->pev[0], s, cudaEventRecordExternal);
     hub_kernels(A, w, 0, cap, ghub, pv, &w.st->tri_removed, s);
     k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
@@ -2250,6 +2286,8 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     B.sign = 1;
     B.split_cnt = &w.st->n_split[1];
     B.bar = &w.st->bar[1];
+    B.e_next = &w.st->e_next[1];
+    B.i_next = &w.st->i_next[1];
     if (p->profile) cudaEventRecordWithFlags(p->pev[2], s, cudaEventRecordExternal);
     hub_kernels(B, w, 1, cap, ghub, pv, &w.st->tri_added, s);
     k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
