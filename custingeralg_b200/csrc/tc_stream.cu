@@ -31,6 +31,7 @@ constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
 constexpr int kRunStage = 4096;  // new entries of one long list staged in shared memory
+constexpr int kLongThreads = 256;  // CTA of the long-list insertions (one list per CTA)
 // Tile shape of the delta count (defaults; the pipeline's autotuner picks per batch-size bin):
 constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
@@ -374,11 +375,12 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
 
 
 // One CTA per long insertion run: the same merge as k_insert_runs (new entries' slots first, old
-// entries backwards in chunks, then the new entries into the holes), 256 entries per step. The
+// entries backwards in chunks, then the new entries into the holes), 2048 entries per step; a
+// list merged in place moves only its entries at or above the first new entry's slot. The
 // barrier between reading and writing a chunk keeps the in-place merge safe: targets never
 // precede their sources, so the writes of a chunk land on entries of that chunk (read before the
 // barrier) or of the chunks above it (already moved).
-__global__ void __launch_bounds__(kThreads) k_insert_long(
+__global__ void __launch_bounds__(kLongThreads) k_insert_long(
     const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ long_runs,
     int64_t* __restrict__ start, int32_t* __restrict__ used, int32_t* __restrict__ cap, int32_t* __restrict__ pool,
     const int64_t pool_cap, uint8_t* __restrict__ mark, int64_t* __restrict__ slot,
@@ -425,7 +427,7 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
     const int64_t s_new = sh_new;
     const int32_t c = (int32_t)(i1 - i0);
     if (state == 2) {
-      for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) slot[j] = -1;
+      for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) slot[j] = -1;
       __syncthreads();
       continue;
     }
@@ -433,7 +435,7 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
     // the run's new entries, staged in shared memory when they fit (the existing entries each
     // look up how many new ones sort before them)
     const bool staged = c <= kRunStage;
-    for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) {
+    for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) {
       const int32_t val = (int32_t)(uint32_t)dk[j];
       if (staged) sh_run[j - i0] = val;
       int32_t lo = 0, hi = a;
@@ -447,18 +449,20 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
     __syncthreads();
     // Existing entries move up by the number of new entries below them, from the list's end
     // down, kInsPer per thread per step: a step reads all its entries before any is written,
-    // and its targets lie at or above its own start, where every entry was read already.
-    constexpr int kInsPer = 4;
-    constexpr int kStep = kThreads * kInsPer;
-    for (int32_t base = ((a - 1) / kStep) * kStep; base >= 0 && a > 0; base -= kStep) {
+    // and its targets lie at or above its own start, where every entry was read already. In
+    // place, the entries below the first new entry's slot keep their positions.
+    constexpr int kInsPer = 8;
+    constexpr int kStep = kLongThreads * kInsPer;
+    const int32_t first = state == 0 && c > 0 ? (int32_t)slot[i0] : 0;
+    for (int32_t base = ((a - 1) / kStep) * kStep; base >= 0 && base + kStep > first && a > 0; base -= kStep) {
       int32_t val[kInsPer];
       int64_t pos[kInsPer];
 #pragma unroll
       for (int q = 0; q < kInsPer; ++q) {
-        const int32_t i = base + q * kThreads + (int32_t)threadIdx.x;
+        const int32_t i = base + q * kLongThreads + (int32_t)threadIdx.x;
         val[q] = 0;
         pos[q] = -1;
-        if (i < a) {
+        if (i < a && i >= first) {
           val[q] = A[i];
           int32_t lo = 0, hi = c;
           while (lo < hi) {
@@ -480,7 +484,7 @@ __global__ void __launch_bounds__(kThreads) k_insert_long(
       }
       __syncthreads();
     }
-    for (int64_t j = i0 + threadIdx.x; j < i1; j += kThreads) {
+    for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) {
       const int64_t pos = s_new + slot[j];
       pool[pos] = (int32_t)(uint32_t)dk[j];
       if (mark) mark[pos] = 1;
@@ -1663,7 +1667,8 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
 }
 
 int delta_grid() { return device_info().sms * 8; }
-int long_grid() { return device_info().sms * 8; }
+int long_grid() { return device_info().sms * (2048 / kLongThreads); }
+int compact_grid() { return device_info().sms * 8; }
 
 // Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
 // more than can be resident at once (its grid barrier needs every CTA running).
@@ -1848,7 +1853,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
         w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch, w.st);
-    k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used,
+    k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used,
                                                      g->pool, g->mark, w.claim, w.d_epoch, w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
@@ -1857,7 +1862,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, 2 * b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, g->mark, w.ins_slot,
         g->d_pool_top, g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, 2 * b, w.long_runs, g->start, g->used, g->cap, g->pool,
+    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, 2 * b, w.long_runs, g->start, g->used, g->cap, g->pool,
                                                     g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
                                                     w.st);
     DeltaArgs A = delta_args(g, sp);
@@ -1967,7 +1972,7 @@ tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, nullptr, w.ins_slot, g->d_pool_top,
         g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, b, w.long_runs, g->start, g->used, g->cap, g->pool,
+    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, b, w.long_runs, g->start, g->used, g->cap, g->pool,
                                                     g->pool_cap, nullptr, w.ins_slot, g->d_pool_top, g->slack_q10,
                                                     w.st);
     TC_CUDA_TRY(cudaGetLastError());
@@ -1997,7 +2002,7 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
   k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
                                                                    g->pool, g->mark, w.claim, w.d_epoch, w.st);
-  k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used, g->pool, g->mark,
+  k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used, g->pool, g->mark,
                                                    w.claim, w.d_epoch, w.st);
   TC_CUDA_TRY(cudaGetLastError());
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
@@ -2271,12 +2276,12 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
                                              w.claim, w.d_epoch, w.st);
-    k_compact_long<<<long_grid(), kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool,
+    k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool,
                                                      g->mark, w.claim, w.d_epoch, w.st);
     // insertions: merge, count on the post-insertion graph, clear the marks
     k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
                                           g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kThreads, 0, s>>>(w.dk2, 2 * cap, w.long_runs, g->start, g->used, g->cap, g->pool,
+    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, 2 * cap, w.long_runs, g->start, g->used, g->cap, g->pool,
                                                     g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
                                                     w.st);
     DeltaArgs B = A;
