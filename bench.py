@@ -77,6 +77,8 @@ def parse(argv=None):
     ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-rule comparison runs")
     ap.add_argument("--no-split", action="store_true", help="skip the one-GPU measurement of the multi-GPU split")
     ap.add_argument("--no-streaming", action="store_true")
+    ap.add_argument("--no-stream-tune", action="store_true",
+                    help="run the streaming pipeline with its default plan (no untimed autotuning first)")
     ap.add_argument("--stream-scale", type=int, default=22)
     ap.add_argument("--stream-batches", type=int, default=200)
     ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
@@ -677,10 +679,14 @@ def run_streaming(ctx, sched_kind, verify_every=None):
     if a.stream_path == "pipeline":
         max_b = max(s.numel() for s, _, _ in dbat)
         t_tune = time.perf_counter()
-        plan = tune_pipeline(base, max_b, sched, a.stream_scale, dev)
+        if not a.no_stream_tune:
+            plan = tune_pipeline(base, max_b, sched, a.stream_scale, dev)
         tune_s = time.perf_counter() - t_tune
         pipe = api.Pipeline(graph, max_b, sched=sched)
-        pipe.set_plan(plan)
+        if plan is not None:
+            pipe.set_plan(plan)
+        else:
+            plan = pipe.plan()
         pipe.profile(True)  # delta-kernel event times and algorithmic bytes per batch
         pipe.prepare(per_vertex=pv, delta_dev=delta)  # pool headroom and captures, before timing
     torch.cuda.synchronize()
@@ -733,7 +739,8 @@ def run_streaming(ctx, sched_kind, verify_every=None):
         res["bins"] = [{"capacity": int(plan.bin_cap[i]), "served_by_capacity": int(plan.bin_cap[plan.serve[i]]),
                         "delta_ctas_per_sm": bps, "split_min": int(plan.split_min[i]), "chunk": int(plan.chunk[i])}
                        for i, (_, bps) in enumerate(pipe.info())]
-        res["autotune"] = (f"on a twin of the base graph before the timed run ({tune_s:.1f} s, untimed): per bin, "
+        res["autotune"] = ("off: the pipeline's default plan" if a.no_stream_tune else
+                           f"on a twin of the base graph before the timed run ({tune_s:.1f} s, untimed): per bin, "
                            "two batches per arm (tile shapes, and the next bin's graph)")
         res["delta_kernel_ms"] = round(st["delta_ms"], 3)
         if st["delta_ms"] > 0:
