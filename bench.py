@@ -55,6 +55,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "edges intersected/s (static triangle count)"
+# Host threads of the graph generators per rank (0 = all cores): with N ranks on one node each
+# rank takes its share, so N concurrent generators do not oversubscribe the host.
+GEN_THREADS = 0
 UNIT = "edges/s"
 RMAT_ABC = (0.57, 0.19, 0.19)
 
@@ -126,6 +129,24 @@ def read_tccsr(path):
         off = np.fromfile(f, dtype="<i8", count=n + 1)
         ind = np.fromfile(f, dtype="<i4", count=m)
     return HostCsr(n, off, ind)
+
+
+def rmat_graph(ctx, scale, ef, seed):
+    """The R-MAT graph of a workload. With several ranks, rank 0 generates it once and the others
+    read it back from a binary CSR file (the generator is a pure function of its parameters)."""
+    from custingeralg_b200 import generators as G
+    if ctx.world == 1:
+        return G.rmat(scale, ef, *RMAT_ABC, seed=seed, nthreads=GEN_THREADS)
+    path = os.path.join(tempfile.gettempdir(),
+                        f"tc_bench_{os.environ.get('MASTER_PORT', '0')}_rmat{scale}_{ef}_{seed}.tccsr")
+    if ctx.rank == 0:
+        G.write_binary(G.rmat(scale, ef, *RMAT_ABC, seed=seed), path)
+    ctx.barrier()
+    g = read_tccsr(path)
+    ctx.barrier()
+    if ctx.rank == 0:
+        os.remove(path)
+    return g
 
 
 def generate_in_child(family_args, path):
@@ -531,11 +552,14 @@ def e2e_static(ctx, g, e_int, out, tri, sched, steps, warmup, T_full):
 
 def run_ours(a, rank, world, local_rank):
     from custingeralg_b200 import generators as G
+    global GEN_THREADS
+    if world > 1:
+        GEN_THREADS = max(1, (os.cpu_count() or 1) // world)
     ctx = Ctx(a, rank, world, local_rank)
     clocks = ClockSampler(local_rank)
     clocks.start()
 
-    g = G.rmat(a.scale, a.edge_factor, *RMAT_ABC, seed=a.seed)
+    g = rmat_graph(ctx, a.scale, a.edge_factor, a.seed)
     main, graph = static_workload(ctx, g, a.scale, a.edge_factor, a.seed, a.steps, a.warmup,
                                   fixed_too=not a.no_fixed, e2e=not a.no_e2e)
     graph.close()
@@ -554,7 +578,7 @@ def run_ours(a, rank, world, local_rank):
     del g
 
     if a.c3_scale:
-        c3g = G.rmat(a.c3_scale, a.edge_factor, *RMAT_ABC, seed=a.c3_seed)
+        c3g = rmat_graph(ctx, a.c3_scale, a.edge_factor, a.c3_seed)
         c3, graph = static_workload(ctx, c3g, a.c3_scale, a.edge_factor, a.c3_seed, a.c3_steps, a.warmup,
                                     fixed_too=not a.no_fixed, e2e=not a.no_e2e)
         graph.close()
@@ -607,7 +631,7 @@ def streaming_batches(scale, nbatch, base, seed=4):
     for i, b in enumerate(sizes.tolist()):
         n_del = n_dels[i]
         n_ins = b - n_del
-        s_ins, d_ins = G.rmat_pairs(scale, n_ins, seed=seed, stream=i + 1)
+        s_ins, d_ins = G.rmat_pairs(scale, n_ins, seed=seed, stream=i + 1, nthreads=GEN_THREADS)
         pick = picks[at:at + n_del]
         at += n_del
         s = np.concatenate([s_ins, src_of[pick]]).astype(np.int32)
@@ -637,7 +661,7 @@ def tune_pipeline(base, max_b, sched, scale, dev, per_arm=2, seed=104):
     for k, b in enumerate(sizes):
         b = max(1, min(b, max_b))
         n_del = int(round(0.3 * b))
-        s_ins, d_ins = G.rmat_pairs(scale, b - n_del, seed=seed, stream=k + 1)
+        s_ins, d_ins = G.rmat_pairs(scale, b - n_del, seed=seed, stream=k + 1, nthreads=GEN_THREADS)
         pick = rng.integers(0, base.m, n_del)
         s = torch.from_numpy(np.concatenate([s_ins, src_of[pick]]).astype(np.int32)).to(dev)
         d = torch.from_numpy(np.concatenate([d_ins, base.ind[pick]]).astype(np.int32)).to(dev)
@@ -657,7 +681,7 @@ def run_streaming(ctx, sched_kind, verify_every=None):
     from custingeralg_b200 import api, generators as G, native as N
     a, dev = ctx.a, ctx.dev
     verify_every = a.stream_verify if verify_every is None else verify_every
-    base = G.rmat(a.stream_scale, 16, *RMAT_ABC, seed=4)
+    base = rmat_graph(ctx, a.stream_scale, 16, 4)
     graph = api.Graph.from_csr(base, slack=0.25)
     pv = torch.zeros(base.n + 1, dtype=torch.int32, device=dev)
     delta = torch.zeros(1, dtype=torch.int64, device=dev)

@@ -48,3 +48,52 @@ def test_launcher_refuses_a_rank_count_it_cannot_honour():
     # more ranks than visible devices (none here): refused, not run as one rank
     r = _run(["--gpus", "2"], {"CUDA_VISIBLE_DEVICES": ""})
     assert r.returncode != 0 and "CUDA devices are visible" in (r.stdout + r.stderr)
+
+
+class _GlooCtx:
+    """The part of bench.Ctx that rmat_graph uses, over a gloo process group."""
+
+    def __init__(self, rank, world):
+        self.rank, self.world = rank, world
+
+    def barrier(self):
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def _shared_graph_worker(rank, world, port, q):
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    import bench as B
+    from custingeralg_b200 import generators as G
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port)})
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g = B.rmat_graph(_GlooCtx(rank, world), 11, 16, 3)
+        ref = G.rmat(11, 16, seed=3)
+        q.put((rank, g.n == ref.n and np.array_equal(g.off, ref.off) and np.array_equal(g.ind, ref.ind)))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_ranks_share_one_generated_graph():
+    """With several ranks, rank 0 generates each bench graph once and the others read it back
+    from a binary file: every rank must hold the generator's CSR, and the file is removed."""
+    import socket
+    import tempfile
+
+    import torch.multiprocessing as mp
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_shared_graph_worker, args=(r, 3, port, q)) for r in range(3)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=240)
+    assert all(p.exitcode == 0 for p in procs)
+    got = dict(q.get(timeout=5) for _ in procs)
+    assert got == {0: True, 1: True, 2: True}
+    assert not os.path.exists(os.path.join(tempfile.gettempdir(), f"tc_bench_{port}_rmat11_16_3.tccsr"))
