@@ -660,10 +660,13 @@ def streaming_batches(scale, nbatch, base, seed=4):
     return out
 
 
-def tune_pipeline(base, max_b, sched, scale, dev, per_arm=2, seed=104):
+def tune_pipeline(base, max_b, sched, scale, dev, per_arm=2, small_per_arm=6, small_cap=4096, seed=104):
     """Autotune a pipeline on a twin of the base graph (untimed) and return its plan: for every
     bin of the ladder, batches of sizes inside that bin, two per arm of the tuner (five tile
-    shapes and the next bin's graph), in the 70/30 insertion/deletion mix of the workload."""
+    shapes and the next bin's graph; six per arm in the bins up to 4096, whose batches differ
+    most in size and cost little), in the 70/30 insertion/deletion mix of the workload. The tuner
+    gives each batch to the arm with the fewest samples, so every size is drawn once and repeated
+    for each arm in turn: the arms are compared on the same sizes."""
     import torch
     from custingeralg_b200 import api, generators as G
     twin = api.Graph.from_csr(base, slack=0.25)
@@ -674,7 +677,9 @@ def tune_pipeline(base, max_b, sched, scale, dev, per_arm=2, seed=104):
     sizes = []
     for i, c in enumerate(caps):
         lo = 1 if i == 0 else caps[i - 1] + 1
-        sizes += [int(np.exp(rng.uniform(np.log(lo), np.log(c + 1)))) for _ in range(per_arm * 6)]
+        k = small_per_arm if c <= small_cap else per_arm
+        for _ in range(k):
+            sizes += [int(np.exp(rng.uniform(np.log(lo), np.log(c + 1))))] * 6
     tp.autotune(len(sizes))
     for k, b in enumerate(sizes):
         b = max(1, min(b, max_b))

@@ -2081,8 +2081,8 @@ struct PipeCand {
 };
 constexpr int kPipeCands = 5;
 constexpr PipeCand kPipeCand[kPipeCands] = {
-    {0, kDeltaChunk, kDeltaSplit}, {4, kDeltaChunk, kDeltaSplit}, {0, kDeltaChunk / 2, kDeltaSplit / 2},
-    {0, kDeltaChunk / 4, kDeltaSplit / 4}, {0, kDeltaChunk / 8, kDeltaSplit / 8}};
+    {0, kDeltaChunk, kDeltaSplit}, {0, kDeltaChunk / 2, kDeltaSplit / 2}, {0, kDeltaChunk / 4, kDeltaSplit / 4},
+    {0, kDeltaChunk / 8, kDeltaSplit / 8}, {0, kDeltaChunk / 16, kDeltaSplit / 16}};
 constexpr int kPipeArms = kPipeCands + 1;  // + the default shape in the next bin's graph
 constexpr double kMergeSlack = 1.03;
 }  // namespace

@@ -263,8 +263,8 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  *                     TC_ERR_TIMEOUT when a delta kernel's barrier wait ran out).
  * tc_pipeline_autotune: explore over the next `batches` batches: each runs under one arm of its
  *                     natural bin, a candidate tile shape of the delta kernel (CTAs per SM: the
- *                     occupancy limit or 4; split threshold / split-item size 2048/1024,
- *                     1024/512, 512/256 or 256/128 entries) or the default shape in the next bin's graph,
+ *                     occupancy limit; split threshold / split-item size 2048/1024, 1024/512,
+ *                     512/256, 256/128 or 128/64 entries) or the default shape in the next bin's graph,
  *                     timed with events. Afterwards each bin keeps its fastest shape, and a bin
  *                     whose batches ran at most 3 % slower in the next bin's graph is merged into
  *                     it (its threshold dropped).

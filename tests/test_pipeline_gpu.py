@@ -106,8 +106,8 @@ def _apply_both(torch, pipe, g_ref, batches, n):
     return int(dp.item())
 
 
-@pytest.mark.parametrize("shape", [(0, 1024, 2048), (4, 1024, 2048), (0, 512, 1024), (0, 256, 512),
-                                   (0, 128, 256)])
+@pytest.mark.parametrize("shape", [(0, 1024, 2048), (0, 512, 1024), (0, 256, 512), (0, 128, 256),
+                                   (0, 64, 128)])
 def test_every_tile_shape_counts_the_same(shape):
     """Each candidate tile shape of the persistent delta kernel (CTAs per SM, split-item size,
     split threshold), set through a plan, gives tc_apply_batch's results on hub-heavy batches
