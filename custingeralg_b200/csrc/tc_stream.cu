@@ -31,7 +31,6 @@ constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
 constexpr int kRunStage = 4096;  // new entries of one long list staged in shared memory
-constexpr int kLongThreads = 256;  // CTA of the long-list insertions (one list per CTA)
 // Tile shape of the delta count (defaults; the pipeline's autotuner picks per batch-size bin):
 constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
@@ -43,7 +42,8 @@ constexpr int kGrab = 4;  // changed edges a warp takes per grab from the delta 
 constexpr unsigned long long kSpinNs = 2000000000ull;  // 2 s
 constexpr unsigned kSpinMaxIters = 1u << 24;
 
-enum : unsigned { kErrRange = 1u, kErrPool = 2u, kErrTimeout = 4u };
+enum : unsigned { kErrRange = 1u, kErrPool = 2u, kErrTimeout = 4u, kErrScratch = 8u };
+constexpr unsigned long long kNoLongItem = ~0ull;
 
 struct BatchStatus {
   unsigned long long n_uniq;      // unique undirected edges
@@ -58,7 +58,9 @@ struct BatchStatus {
   unsigned long long dir_added;   // directed entries inserted (cuStinger path)
   unsigned long long dir_removed; // directed entries deleted (cuStinger path)
   unsigned long long not_fitting;
-  unsigned long long n_long;      // insertion runs whose list is long (CTA kernel)
+  unsigned long long n_long;      // insertion runs whose list is long (k_long_plan)
+  unsigned long long long_scr;
+  unsigned long long long_items;
   unsigned long long n_split[2];  // split-intersection items queued (deletions, insertions)
   unsigned long long delta_bytes; // algorithmic bytes of the batch's intersections (4(deg x + deg y) + 8 each)
   unsigned int bar[2];            // grid-barrier arrivals of the persistent delta kernels
@@ -173,10 +175,11 @@ __global__ void k_classify(const SlackView g, const uint64_t* __restrict__ keys,
 // Heads of source-vertex runs in the sorted directed entries, and the pool slots the lists that
 // must move could take (computed on the pre-deletion lengths, an upper bound).
 // A run whose list will be long (used + new > kLongList) is stored as -1 - start and also listed
-// in long_runs for the CTA kernel; the warp kernel skips it.
+// (start, length) in long_runs / long_cnt for the long-list insertion; the warp kernel skips it.
 __global__ void k_dir_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ used,
                            const int32_t* __restrict__ cap, const int32_t slack_q10, int32_t* __restrict__ run_start,
-                           int32_t* __restrict__ long_runs, BatchStatus* __restrict__ st) {
+                           int32_t* __restrict__ long_runs, int32_t* __restrict__ long_cnt,
+                           BatchStatus* __restrict__ st) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd_cap; i += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = dk[i];
     if (k == kSentinel) continue;
@@ -189,7 +192,9 @@ __global__ void k_dir_runs(const uint64_t* __restrict__ dk, const int64_t nd_cap
     const int32_t need = used[v] + c;
     if (need > kLongList) {
       run_start[r] = -1 - (int32_t)i;
-      long_runs[atomicAdd(&st->n_long, 1ull)] = (int32_t)i;
+      const unsigned long long q = atomicAdd(&st->n_long, 1ull);
+      long_runs[q] = (int32_t)i;
+      long_cnt[q] = c;
     } else {
       run_start[r] = (int32_t)i;
     }
@@ -211,7 +216,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
   const int64_t nruns = (int64_t)st->n_runs;
   for (int64_t r = gw; r < nruns; r += nw) {
     const int64_t i0 = run_start[r];
-    if (i0 < 0) continue;  // a long list: k_insert_long
+    if (i0 < 0) continue;  // a long list: k_long_plan / k_long_stage / k_long_write
     const int32_t v = (int32_t)(dk[i0] >> 32);
     int64_t i1 = i0;  // run end (exclusive), found cooperatively
     {
@@ -374,133 +379,145 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
 }
 
 
-// One CTA per long insertion run: the same merge as k_insert_runs (new entries' slots first, old
-// entries backwards in chunks, then the new entries into the holes), 2048 entries per step; a
-// list merged in place moves only its entries at or above the first new entry's slot. The
-// barrier between reading and writing a chunk keeps the in-place merge safe: targets never
-// precede their sources, so the writes of a chunk land on entries of that chunk (read before the
-// barrier) or of the chunks above it (already moved).
-__global__ void __launch_bounds__(kLongThreads) k_insert_long(
-    const uint64_t* __restrict__ dk, const int64_t nd_cap, const int32_t* __restrict__ long_runs,
-    int64_t* __restrict__ start, int32_t* __restrict__ used, int32_t* __restrict__ cap, int32_t* __restrict__ pool,
-    const int64_t pool_cap, uint8_t* __restrict__ mark, int64_t* __restrict__ slot,
-    unsigned long long* __restrict__ pool_top, const int32_t slack_q10, BatchStatus* __restrict__ st) {
-  __shared__ int64_t sh_i1, sh_new;
-  __shared__ int32_t sh_nc;
-  __shared__ int sh_state;  // 0 in place, 1 moved, 2 pool exhausted
-  __shared__ int32_t sh_run[kRunStage];
+// Insertion into long lists (more than kLongList entries after the batch), in three launches
+// over all of the batch's long runs at once:
+//   k_long_plan   one thread per run: relocation (when the list outgrows its capacity) or the
+//                 in-place merge's first moving entry (the first new entry's slot), the list's
+//                 new length, a range of the scratch buffer and work items of kLongChunk entries;
+//   k_long_stage  one CTA per item: each moving old entry and each new entry computes its place
+//                 in the merged suffix (an old entry shifts by the number of new entries below it,
+//                 a new entry lands after the old entries below it) and writes there in scratch;
+//   k_long_write  one CTA per item: the merged suffix back into the list, with the new entries'
+//                 marks.
+// The launch boundary between staging and writing takes the place of an in-place merge's block
+// barriers: every source is read before any target is written, so a hub list of 10^5 entries is
+// spread over many CTAs instead of being one CTA's chain of steps.
+constexpr int kLongChunk = 4096;
+
+struct LongPlan {
+  int64_t s_old;   // list start before the batch
+  int64_t s_new;   // list start after it (s_old unless relocated)
+  int64_t soff;    // the run's range in the scratch buffer
+  int32_t a;       // entries before the batch
+  int32_t c;       // new entries
+  int32_t first;   // first moving entry (0 when relocated)
+  int32_t len;     // entries staged: a - first + c (0 = nothing to do)
+  int32_t i0;      // the run's first entry in the sorted directed keys
+  int32_t pad;
+};
+
+__global__ void __launch_bounds__(kThreads) k_long_plan(
+    const uint64_t* __restrict__ dk, const int32_t* __restrict__ long_runs, const int32_t* __restrict__ long_cnt,
+    int64_t* __restrict__ start, int32_t* __restrict__ used, int32_t* __restrict__ cap,
+    const int32_t* __restrict__ pool, const int64_t pool_cap, int64_t* __restrict__ slot,
+    unsigned long long* __restrict__ pool_top, const int32_t slack_q10, LongPlan* __restrict__ plan,
+    unsigned long long* __restrict__ items, const int64_t item_cap, const int64_t scr_cap,
+    BatchStatus* __restrict__ st) {
   const int64_t nlong = (int64_t)st->n_long;
-  for (int64_t r = blockIdx.x; r < nlong; r += gridDim.x) {
-    const int64_t i0 = long_runs[r];
-    const int32_t v = (int32_t)(dk[i0] >> 32);
-    const int32_t a = used[v];
-    const int64_t s_old = start[v];
-    if (threadIdx.x == 0) {
-      // run end: the first entry at or past i0 whose source is not v (sentinels sort last)
-      const uint64_t lim = ((uint64_t)(uint32_t)v + 1) << 32;
-      int64_t lo = i0, hi = nd_cap;
-      while (lo < hi) {
-        const int64_t mid = lo + ((hi - lo) >> 1);
-        if (dk[mid] < lim) lo = mid + 1;
-        else hi = mid;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nlong; r += (int64_t)gridDim.x * blockDim.x) {
+    LongPlan P;
+    P.i0 = long_runs[r];
+    P.c = long_cnt[r];
+    P.pad = 0;
+    const int32_t v = (int32_t)(dk[P.i0] >> 32);
+    P.a = used[v];
+    P.s_old = start[v];
+    P.s_new = P.s_old;
+    P.len = 0;
+    P.soff = 0;
+    P.first = 0;
+    bool ok = true;
+    if (P.a + P.c > cap[v]) {
+      const int32_t nc = slack_capacity(P.a + P.c, max(slack_q10, 256));
+      const unsigned long long at = atomicAdd(pool_top, (unsigned long long)nc);
+      if ((int64_t)at + nc > pool_cap) {
+        atomicOr(&st->err, kErrPool);
+        ok = false;
+      } else {
+        P.s_new = (int64_t)at;
+        start[v] = P.s_new;
+        cap[v] = nc;
+        atomicAdd(&st->not_fitting, (unsigned long long)P.c);
       }
-      sh_i1 = lo;
-      const int32_t c = (int32_t)(lo - i0);
-      sh_state = 0;
-      sh_new = s_old;
-      if (a + c > cap[v]) {
-        const int32_t nc = slack_capacity(a + c, max(slack_q10, 256));
-        const unsigned long long at = atomicAdd(pool_top, (unsigned long long)nc);
-        if ((int64_t)at + nc > pool_cap) {
-          atomicOr(&st->err, kErrPool);
-          sh_state = 2;
-        } else {
-          sh_new = (int64_t)at;
-          sh_nc = nc;
-          sh_state = 1;
+    } else {
+      P.first = (int32_t)(lower_bound(pool, P.s_old, P.s_old + P.a, (int32_t)(uint32_t)dk[P.i0]) - P.s_old);
+    }
+    if (ok) {
+      P.len = P.a - P.first + P.c;
+      const int32_t nch = (P.len + kLongChunk - 1) / kLongChunk;
+      const unsigned long long so = atomicAdd(&st->long_scr, (unsigned long long)P.len);
+      const unsigned long long ib = atomicAdd(&st->long_items, (unsigned long long)nch);
+      if ((int64_t)(so + P.len) > scr_cap || (int64_t)(ib + nch) > item_cap) {
+        atomicOr(&st->err, kErrScratch);  // unreachable while the scratch follows the pool's size
+        ok = false;
+        for (int32_t j = 0; j < nch && (int64_t)(ib + j) < item_cap; ++j) items[ib + j] = kNoLongItem;
+      } else {
+        P.soff = (int64_t)so;
+        for (int32_t j = 0; j < nch; ++j) items[ib + j] = ((unsigned long long)r << 32) | (unsigned)j;
+        used[v] = P.a + P.c;
+        atomicAdd(&st->dir_added, (unsigned long long)P.c);
+      }
+    }
+    if (!ok) {
+      P.len = 0;
+      for (int32_t j = 0; j < P.c; ++j) slot[P.i0 + j] = -1;
+    }
+    plan[r] = P;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_long_stage(
+    const uint64_t* __restrict__ dk, const int32_t* __restrict__ pool, const LongPlan* __restrict__ plan,
+    const unsigned long long* __restrict__ items, const int64_t item_cap, int32_t* __restrict__ scr,
+    uint8_t* __restrict__ smark, int64_t* __restrict__ slot, const BatchStatus* __restrict__ st) {
+  const int64_t n_items = min((int64_t)st->long_items, item_cap);
+  for (int64_t q = blockIdx.x; q < n_items; q += gridDim.x) {
+    const unsigned long long item = items[q];
+    if (item == kNoLongItem) continue;
+    const LongPlan P = plan[item >> 32];
+    const int32_t k0 = (int32_t)(uint32_t)item * kLongChunk, k1 = min(P.len, k0 + kLongChunk);
+    const int32_t suffix = P.a - P.first;
+    for (int32_t k = k0 + (int32_t)threadIdx.x; k < k1; k += kThreads) {
+      int32_t val, pos;
+      uint8_t mk;
+      if (k < suffix) {  // an old entry: shifts by the new entries below it
+        val = pool[P.s_old + P.first + k];
+        int32_t lo = 0, hi = P.c;
+        while (lo < hi) {
+          const int32_t mid = (lo + hi) >> 1;
+          if ((int32_t)(uint32_t)dk[P.i0 + mid] < val) lo = mid + 1;
+          else hi = mid;
         }
+        pos = k + lo;
+        mk = 0;
+      } else {  // a new entry: lands after the old entries below it
+        const int32_t j = k - suffix;
+        val = (int32_t)(uint32_t)dk[P.i0 + j];
+        pos = j + (int32_t)(lower_bound(pool, P.s_old, P.s_old + P.a, val) - P.s_old) - P.first;
+        slot[P.i0 + j] = P.s_new + P.first + pos;
+        mk = 1;
       }
+      scr[P.soff + pos] = val;
+      smark[P.soff + pos] = mk;
     }
-    __syncthreads();
-    const int64_t i1 = sh_i1;
-    const int state = sh_state;
-    const int64_t s_new = sh_new;
-    const int32_t c = (int32_t)(i1 - i0);
-    if (state == 2) {
-      for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) slot[j] = -1;
-      __syncthreads();
-      continue;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_long_write(
+    const LongPlan* __restrict__ plan, const unsigned long long* __restrict__ items, const int64_t item_cap,
+    const int32_t* __restrict__ scr, const uint8_t* __restrict__ smark, int32_t* __restrict__ pool,
+    uint8_t* __restrict__ mark, const BatchStatus* __restrict__ st) {
+  const int64_t n_items = min((int64_t)st->long_items, item_cap);
+  for (int64_t q = blockIdx.x; q < n_items; q += gridDim.x) {
+    const unsigned long long item = items[q];
+    if (item == kNoLongItem) continue;
+    const LongPlan P = plan[item >> 32];
+    const int32_t k0 = (int32_t)(uint32_t)item * kLongChunk, k1 = min(P.len, k0 + kLongChunk);
+    for (int32_t k = k0 + (int32_t)threadIdx.x; k < k1; k += kThreads) {
+      const int64_t dest = P.s_new + P.first + k;
+      pool[dest] = scr[P.soff + k];
+      if (mark) mark[dest] = smark[P.soff + k];
     }
-    const int32_t* A = pool + s_old;
-    // the run's new entries, staged in shared memory when they fit (the existing entries each
-    // look up how many new ones sort before them)
-    const bool staged = c <= kRunStage;
-    for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) {
-      const int32_t val = (int32_t)(uint32_t)dk[j];
-      if (staged) sh_run[j - i0] = val;
-      int32_t lo = 0, hi = a;
-      while (lo < hi) {
-        const int32_t mid = (lo + hi) >> 1;
-        if (A[mid] < val) lo = mid + 1;
-        else hi = mid;
-      }
-      slot[j] = (j - i0) + lo;
-    }
-    __syncthreads();
-    // Existing entries move up by the number of new entries below them, from the list's end
-    // down, kInsPer per thread per step: a step reads all its entries before any is written,
-    // and its targets lie at or above its own start, where every entry was read already. In
-    // place, the entries below the first new entry's slot keep their positions.
-    constexpr int kInsPer = 8;
-    constexpr int kStep = kLongThreads * kInsPer;
-    const int32_t first = state == 0 && c > 0 ? (int32_t)slot[i0] : 0;
-    for (int32_t base = ((a - 1) / kStep) * kStep; base >= 0 && base + kStep > first && a > 0; base -= kStep) {
-      int32_t val[kInsPer];
-      int64_t pos[kInsPer];
-#pragma unroll
-      for (int q = 0; q < kInsPer; ++q) {
-        const int32_t i = base + q * kLongThreads + (int32_t)threadIdx.x;
-        val[q] = 0;
-        pos[q] = -1;
-        if (i < a && i >= first) {
-          val[q] = A[i];
-          int32_t lo = 0, hi = c;
-          while (lo < hi) {
-            const int32_t mid = (lo + hi) >> 1;
-            const int32_t x = staged ? sh_run[mid] : (int32_t)(uint32_t)dk[i0 + mid];
-            if (x < val[q]) lo = mid + 1;
-            else hi = mid;
-          }
-          pos[q] = i + lo;
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int q = 0; q < kInsPer; ++q) {
-        if (pos[q] >= 0) {
-          pool[s_new + pos[q]] = val[q];
-          if (mark) mark[s_new + pos[q]] = 0;
-        }
-      }
-      __syncthreads();
-    }
-    for (int64_t j = i0 + threadIdx.x; j < i1; j += kLongThreads) {
-      const int64_t pos = s_new + slot[j];
-      pool[pos] = (int32_t)(uint32_t)dk[j];
-      if (mark) mark[pos] = 1;
-      slot[j] = pos;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      used[v] = a + c;
-      if (state == 1) {
-        start[v] = s_new;
-        cap[v] = sh_nc;
-        atomicAdd(&st->not_fitting, (unsigned long long)c);
-      }
-      atomicAdd(&st->dir_added, (unsigned long long)c);
-    }
-    __syncthreads();
   }
 }
 
@@ -1452,6 +1469,14 @@ struct StreamWs {
   uint64_t* dk2 = nullptr;      // [2b]
   int32_t* run_start = nullptr; // [2b]
   int32_t* long_runs = nullptr; // [2b] starts of the runs whose list is long
+  int32_t* long_cnt = nullptr;  // [2b] their lengths
+  LongPlan* long_plan = nullptr;  // [2b]
+  // long-list insertion scratch, sized with the pool (ensure_long_scratch)
+  int32_t* long_scr = nullptr;
+  uint8_t* long_smark = nullptr;
+  unsigned long long* long_items = nullptr;
+  int64_t scr_cap = 0;
+  int64_t long_item_cap = 0;
   int64_t* ins_slot = nullptr;  // [2b]
   int32_t* vlist = nullptr;     // [2b]
   unsigned* claim = nullptr;    // [n]
@@ -1485,6 +1510,7 @@ struct StreamWs {
 void StreamWs::release() {
   cudaFree(src); cudaFree(dst); cudaFree(isdel); cudaFree(keys); cudaFree(keys2); cudaFree(head);
   cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(long_runs);
+  cudaFree(long_cnt); cudaFree(long_plan); cudaFree(long_scr); cudaFree(long_smark); cudaFree(long_items);
   cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
@@ -1569,6 +1595,8 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
     cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
     cudaFree(w.long_runs); cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
+    cudaFree(w.long_cnt); cudaFree(w.long_plan);
+    w.long_cnt = nullptr; w.long_plan = nullptr;
     cudaFree(w.hub_list); cudaFree(w.hub_off); cudaFree(w.hub_len); cudaFree(w.hub_fill); cudaFree(w.hub_chunks);
     cudaFree(w.hub_units); cudaFree(w.hubbed); cudaFree(w.hub_items);
     w.src = nullptr; w.dst = nullptr; w.isdel = nullptr; w.keys = nullptr; w.keys2 = nullptr; w.head = nullptr;
@@ -1594,6 +1622,8 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
             ::tc::dev_malloc(&w.dk2, sizeof(uint64_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.run_start, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.long_runs, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.long_cnt, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.long_plan, sizeof(LongPlan) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.ins_slot, sizeof(int64_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.vlist, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.hub_list, sizeof(int32_t) * nb) == cudaSuccess &&
@@ -1616,10 +1646,46 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   return TC_OK;
 }
 
-// Make room for `extra` slots past pool_top (grow the pool and the mark array by copying).
+// Scratch of the long-list insertion: the merged suffixes of one batch's long lists, at most every
+// entry of the pool plus the batch's new ones (pool_cap + 2 b), and their work items. Follows the
+// pool's capacity; a reallocation bumps the workspace version (captured graphs hold the pointers).
+tc_status ensure_long_scratch(tc_graph* g) {
+  if (!g->sw) return TC_OK;
+  StreamWs& w = *g->sw;
+  const int64_t need = g->pool_cap + 2 * w.b_cap;
+  if (w.scr_cap >= need && w.long_scr && w.long_smark && w.long_items) return TC_OK;
+  cudaFree(w.long_scr);
+  cudaFree(w.long_smark);
+  cudaFree(w.long_items);
+  w.long_scr = nullptr;
+  w.long_smark = nullptr;
+  w.long_items = nullptr;
+  w.scr_cap = 0;
+  w.long_item_cap = 0;
+  ++w.version;
+  const int64_t cap = need + need / 4;
+  const int64_t icap = cap / kLongChunk + 2 * w.b_cap + 1;
+  if (::tc::dev_malloc(&w.long_scr, sizeof(int32_t) * (size_t)cap) != cudaSuccess ||
+      ::tc::dev_malloc(&w.long_smark, (size_t)cap) != cudaSuccess ||
+      ::tc::dev_malloc(&w.long_items, sizeof(unsigned long long) * (size_t)icap) != cudaSuccess) {
+    cudaFree(w.long_scr);
+    cudaFree(w.long_smark);
+    cudaFree(w.long_items);
+    w.long_scr = nullptr;
+    w.long_smark = nullptr;
+    w.long_items = nullptr;
+    return fail(TC_ERR_OOM, "long-list insertion scratch: device allocation failed");
+  }
+  w.scr_cap = cap;
+  w.long_item_cap = icap;
+  return TC_OK;
+}
+
+// Make room for `extra` slots past pool_top (grow the pool and the mark array by copying), and
+// size the long-list insertion scratch to the pool.
 tc_status ensure_pool(tc_graph* g, int64_t extra, cudaStream_t s) {
   const int64_t need = g->pool_top + extra;
-  if (need <= g->pool_cap) return TC_OK;
+  if (need <= g->pool_cap) return ensure_long_scratch(g);
   const int64_t ncap = std::max<int64_t>(need + need / 4, g->pool_cap * 3 / 2);
   int32_t* np = nullptr;
   uint8_t* nm = nullptr;
@@ -1639,7 +1705,7 @@ tc_status ensure_pool(tc_graph* g, int64_t extra, cudaStream_t s) {
   g->mark = nm;
   g->pool_cap = ncap;
   g->view_version++;
-  return TC_OK;
+  return ensure_long_scratch(g);
 }
 
 int bits_for(int32_t n) {
@@ -1667,7 +1733,19 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
 }
 
 int delta_grid() { return device_info().sms * 8; }
-int long_grid() { return device_info().sms * (2048 / kLongThreads); }
+int long_grid() { return device_info().sms * 8; }
+
+// Insertion into the batch's long lists (k_long_plan, k_long_stage, k_long_write); `nd_cap` bounds
+// the long runs (the directed entries' capacity). The scratch must be sized (ensure_pool).
+void long_insert(tc_graph* g, StreamWs& w, int64_t nd_cap, uint8_t* mark, cudaStream_t s) {
+  k_long_plan<<<grid_for(nd_cap, kThreads), kThreads, 0, s>>>(
+      w.dk2, w.long_runs, w.long_cnt, g->start, g->used, g->cap, g->pool, g->pool_cap, w.ins_slot, g->d_pool_top,
+      g->slack_q10, w.long_plan, w.long_items, w.long_item_cap, w.scr_cap, w.st);
+  k_long_stage<<<long_grid(), kThreads, 0, s>>>(w.dk2, g->pool, w.long_plan, w.long_items, w.long_item_cap, w.long_scr,
+                                                w.long_smark, w.ins_slot, w.st);
+  k_long_write<<<long_grid(), kThreads, 0, s>>>(w.long_plan, w.long_items, w.long_item_cap, w.long_scr, w.long_smark,
+                                                g->pool, mark, w.st);
+}
 int compact_grid() { return device_info().sms * 8; }
 
 // Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
@@ -1814,8 +1892,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_classify<<<gb, kThreads, 0, s>>>(view, w.keys2, b, L, w.head, w.dlist, w.ilist, w.dk, w.st);
     size_t tb2 = w.cub_bytes;
     TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * b), 0, 64, s));
-    k_dir_runs<<<grid_for(2 * b, kThreads), kThreads, 0, s>>>(w.dk2, 2 * b, g->used, g->cap, g->slack_q10, w.run_start,
-                                                               w.long_runs, w.st);
+    k_dir_runs<<<grid_for(2 * b, kThreads), kThreads, 0, s>>>(w.dk2, 2 * b, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.long_cnt, w.st);
     TC_CUDA_TRY(cudaGetLastError());
   }
   // 2. one synchronisation: sizes and the pool demand
@@ -1862,9 +1939,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, 2 * b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, g->mark, w.ins_slot,
         g->d_pool_top, g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, 2 * b, w.long_runs, g->start, g->used, g->cap, g->pool,
-                                                    g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
-                                                    w.st);
+    long_insert(g, w, 2 * b, g->mark, s);
     DeltaArgs A = delta_args(g, sp);
     A.ilist = w.ilist;
     A.count_dev = &w.st->n_ins;
@@ -1883,7 +1958,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
     TC_CUDA_TRY(cudaStreamSynchronize(s));
     const BatchStatus& f = *w.st_host;
-    if (f.err & kErrPool) return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+    if (f.err & (kErrPool | kErrScratch)) return fail(TC_ERR_CAPACITY, "adjacency pool or insertion scratch exhausted");
     if (f.err & kErrTimeout) return fail(TC_ERR_TIMEOUT, "the delta kernel's grid barrier gave up waiting");
     info->updates = b;
     info->inserted = (int64_t)f.n_ins;
@@ -1961,7 +2036,7 @@ tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   k_flag_present<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, w.dk);
   size_t tb = w.cub_bytes;
   TC_CUDA_TRY(cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb, w.dk, w.dk2, (int)b, 0, 64, s));
-  k_dir_runs<<<grid_for(b, kThreads), kThreads, 0, s>>>(w.dk2, b, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.st);
+  k_dir_runs<<<grid_for(b, kThreads), kThreads, 0, s>>>(w.dk2, b, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.long_cnt, w.st);
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaMemcpyAsync(&w.st_host->pool_top, g->d_pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -1972,14 +2047,12 @@ tc_status tc_insert_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
     k_insert_runs<<<grid_for((int64_t)h.n_runs * 32, kThreads), kThreads, 0, s>>>(
         w.dk2, b, w.run_start, g->start, g->used, g->cap, g->pool, g->pool_cap, nullptr, w.ins_slot, g->d_pool_top,
         g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, b, w.long_runs, g->start, g->used, g->cap, g->pool,
-                                                    g->pool_cap, nullptr, w.ins_slot, g->d_pool_top, g->slack_q10,
-                                                    w.st);
+    long_insert(g, w, b, nullptr, s);
     TC_CUDA_TRY(cudaGetLastError());
   }
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
-  if (w.st_host->err & kErrPool) return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+  if (w.st_host->err & (kErrPool | kErrScratch)) return fail(TC_ERR_CAPACITY, "adjacency pool or insertion scratch exhausted");
   g->m += (int64_t)w.st_host->dir_added;
   g->pool_top += (int64_t)h.demand;  // host bound until the next read of the device counter
   g->view_version++;
@@ -2185,9 +2258,9 @@ tc_status pipe_settle(tc_pipeline* p) {
     p->last.status = TC_ERR_INVALID_ARG;
     return fail(TC_ERR_INVALID_ARG, "batch had vertex ids outside [0, %d); they were ignored", g->n);
   }
-  if (f.err & kErrPool) {
+  if (f.err & (kErrPool | kErrScratch)) {
     p->last.status = TC_ERR_CAPACITY;
-    return fail(TC_ERR_CAPACITY, "adjacency pool exhausted during insertion");
+    return fail(TC_ERR_CAPACITY, "adjacency pool or insertion scratch exhausted");
   }
   if (f.err & kErrTimeout) {
     p->last.status = TC_ERR_TIMEOUT;
@@ -2249,7 +2322,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     size_t tb2 = w.cub_bytes;
     if ((e = cub::DeviceRadixSort::SortKeys(w.cub_tmp, tb2, w.dk, w.dk2, (int)(2 * cap), 0, 64, s)) != cudaSuccess)
       break;
-    k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.st);
+    k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.long_cnt, w.st);
     // deletions: mark, count on the pre-deletion graph, compact
     k_mark_deletions<<<gb, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
     DeltaArgs A = delta_args(g, p->sp);
@@ -2281,9 +2354,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     // insertions: merge, count on the post-insertion graph, clear the marks
     k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
                                           g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10, w.st);
-    k_insert_long<<<long_grid(), kLongThreads, 0, s>>>(w.dk2, 2 * cap, w.long_runs, g->start, g->used, g->cap, g->pool,
-                                                    g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10,
-                                                    w.st);
+    long_insert(g, w, 2 * cap, g->mark, s);
     DeltaArgs B = A;
     B.dlist = nullptr;
     B.ilist = w.ilist;
@@ -2448,6 +2519,7 @@ tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t*
   const int64_t worst = pipe_worst_demand(g, b);
   if (g->pool_cap - g->pool_top < worst) TC_TRY(ensure_pool(g, worst + worst / 2, s));
   TC_TRY(ensure_stream_ws(g, p->b_max));
+  TC_TRY(ensure_long_scratch(g));
   uint32_t* pv = per_vertex ? reinterpret_cast<uint32_t*>(per_vertex) : p->pv_scratch;
   int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
   StreamWs& w = *g->sw;
@@ -2499,6 +2571,7 @@ tc_status tc_pipeline_prepare(tc_pipeline* p, int32_t* per_vertex, int64_t* delt
   const int64_t worst = pipe_worst_demand(g, p->b_max);
   if (g->pool_cap - g->pool_top < worst) TC_TRY(ensure_pool(g, 2 * worst, (cudaStream_t)stream));
   TC_TRY(ensure_stream_ws(g, p->b_max));
+  TC_TRY(ensure_long_scratch(g));
   uint32_t* pv = per_vertex ? reinterpret_cast<uint32_t*>(per_vertex) : p->pv_scratch;
   int64_t* delta = delta_dev ? delta_dev : p->delta_scratch;
   pipe_check_keys(p, pv, delta);

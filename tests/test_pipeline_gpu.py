@@ -263,7 +263,7 @@ def test_pipeline_rejects_oversize_batch_and_recaptures_on_new_outputs():
 
 @pytest.mark.parametrize("path", ["pipeline", "apply"])
 def test_long_lists_insert_and_delete(path):
-    """Hub lists above 2048 entries take the CTA kernels (k_insert_long, k_compact_long)."""
+    """Hub lists above 2048 entries take the long-list kernels (k_long_plan/stage/write, k_compact_long)."""
     torch = _torch()
     rng = np.random.default_rng(21)
     n = 12000
