@@ -59,8 +59,11 @@ struct BatchStatus {
   unsigned long long dir_removed; // directed entries deleted (cuStinger path)
   unsigned long long not_fitting;
   unsigned long long n_long;      // insertion runs whose list is long (k_long_plan)
-  unsigned long long long_scr;
+  unsigned long long long_scr;    // scratch entries and work items of the long-list insertion
   unsigned long long long_items;
+  unsigned long long n_cmp;       // long lists compacted, their scratch entries and work items
+  unsigned long long cmp_scr;
+  unsigned long long cmp_items;
   unsigned long long n_split[2];  // split-intersection items queued (deletions, insertions)
   unsigned long long delta_bytes; // algorithmic bytes of the batch's intersections (4(deg x + deg y) + 8 each)
   unsigned int bar[2];            // grid-barrier arrivals of the persistent delta kernels
@@ -346,7 +349,7 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
   const unsigned lt = (1u << lane) - 1u;
   for (int64_t k = gw; k < cnt; k += nw) {
     const int32_t v = vlist[k];
-    if (used[v] > kLongList) continue;  // k_compact_long
+    if (used[v] > kLongList) continue;  // a long list: k_cmp_plan / stage / prefix / write
     unsigned old = 0;
     if (lane == 0) old = atomicMax(&claim[v], epoch);
     __syncwarp();
@@ -521,72 +524,146 @@ __global__ void __launch_bounds__(kThreads) k_long_write(
   }
 }
 
-// One CTA per long list with deletions: the compaction of k_compact_marked, 256 entries per
-// step with a block-wide prefix of the kept entries (targets never pass their sources).
-__global__ void __launch_bounds__(kThreads) k_compact_long(
+// Deletions from long lists (more than kLongList entries), in four launches over all of the
+// batch's long lists at once, through the insertion's scratch buffer:
+//   k_cmp_plan    one thread per vertex of the deletions: claims the list (the epoch) and gives it
+//                 work items of kLongChunk entries and a range of the scratch;
+//   k_cmp_stage   one CTA per item: the chunk's kept entries, compacted within the chunk, into
+//                 scratch, and their count; the chunk's marks cleared;
+//   k_cmp_prefix  one thread per list: its chunks' output offsets (a prefix of the counts) and
+//                 its new length;
+//   k_cmp_write   one CTA per item: the chunk's kept entries from scratch to their place.
+// The scratch keeps sources and targets apart, so chunks of one list proceed on many CTAs.
+struct CmpPlan {
+  int64_t s;       // list start
+  int64_t soff;    // the list's range in the scratch buffer
+  int64_t ib;      // its first work item
+  int32_t v;
+  int32_t a;       // entries before the deletions
+  int32_t nch;     // work items (chunks)
+  int32_t pad;
+};
+
+__global__ void __launch_bounds__(kThreads) k_cmp_plan(
     const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
-    const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start, int32_t* __restrict__ used,
-    int32_t* __restrict__ pool, uint8_t* __restrict__ mark, unsigned* __restrict__ claim,
-    const unsigned* __restrict__ epoch_dev, BatchStatus* __restrict__ st) {
-  __shared__ unsigned sh_old;
-  __shared__ int32_t sh_wsum[kThreads / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start,
+    const int32_t* __restrict__ used, unsigned* __restrict__ claim, const unsigned* __restrict__ epoch_dev,
+    CmpPlan* __restrict__ plan, unsigned long long* __restrict__ items, const int64_t item_cap,
+    const int64_t scr_cap, BatchStatus* __restrict__ st) {
   const unsigned epoch = *epoch_dev;
   const int64_t cnt = nv_dev ? (int64_t)(*nv_dev) * stride : nv_list;
-  for (int64_t k = blockIdx.x; k < cnt; k += gridDim.x) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = vlist[k];
     const int32_t a = used[v];
     if (a <= kLongList) continue;  // k_compact_marked's
-    if (threadIdx.x == 0) sh_old = atomicMax(&claim[v], epoch);
-    __syncthreads();
-    const unsigned old = sh_old;
-    __syncthreads();
-    if (old >= epoch) continue;
-    const int64_t s = start[v];
-    int32_t wp = 0;
-    // kCmpPer consecutive entries per thread per step; a step reads all its entries before the
-    // barrier, and its targets lie below the next step's start (targets never pass sources)
-    constexpr int kCmpPer = 4;
-    for (int32_t base = 0; base < a; base += kThreads * kCmpPer) {
-      const int32_t i0 = base + (int32_t)threadIdx.x * kCmpPer;
-      int32_t val[kCmpPer];
-      int kept = 0;
-      unsigned keepm = 0;
-#pragma unroll
-      for (int q = 0; q < kCmpPer; ++q) {
-        const int32_t i = i0 + q;
-        const bool keep = i < a && mark[s + i] == 0;
-        val[q] = keep ? pool[s + i] : 0;
-        keepm |= (unsigned)keep << q;
-        kept += keep;
-      }
-      int incl = kept;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-      }
-      if (lane == 31) sh_wsum[wid] = incl;
-      __syncthreads();
-      int32_t before = 0, total = 0;
-      for (int w = 0; w < kThreads / 32; ++w) {
-        const int32_t x = sh_wsum[w];
-        if (w < wid) before += x;
-        total += x;
-      }
-      int32_t at = wp + before + incl - kept;
-#pragma unroll
-      for (int q = 0; q < kCmpPer; ++q)
-        if (keepm >> q & 1u) pool[s + at++] = val[q];
-      wp += total;
-      __syncthreads();
+    if (atomicMax(&claim[v], epoch) >= epoch) continue;  // claimed by another entry of v
+    CmpPlan P;
+    P.v = v;
+    P.a = a;
+    P.s = start[v];
+    P.nch = (a + kLongChunk - 1) / kLongChunk;
+    P.pad = 0;
+    const unsigned long long so = atomicAdd(&st->cmp_scr, (unsigned long long)a);
+    const unsigned long long ib = atomicAdd(&st->cmp_items, (unsigned long long)P.nch);
+    const unsigned long long r = atomicAdd(&st->n_cmp, 1ull);
+    if ((int64_t)(so + a) > scr_cap || (int64_t)(ib + P.nch) > item_cap) {
+      atomicOr(&st->err, kErrScratch);  // unreachable while the scratch follows the pool's size
+      for (int32_t j = 0; j < P.nch && (int64_t)(ib + j) < item_cap; ++j) items[ib + j] = kNoLongItem;
+      P.nch = 0;
+    } else {
+      for (int32_t j = 0; j < P.nch; ++j) items[ib + j] = (r << 32) | (unsigned)j;
     }
-    for (int32_t i = threadIdx.x; i < a; i += kThreads) mark[s + i] = 0;
-    if (threadIdx.x == 0) {
-      used[v] = wp;
-      atomicAdd(&st->dir_removed, (unsigned long long)(a - wp));
+    P.soff = (int64_t)so;
+    P.ib = (int64_t)ib;
+    plan[r] = P;
+  }
+}
+
+// Each thread holds kCmpPer consecutive entries of the chunk (256 threads x 16 = kLongChunk).
+constexpr int kCmpPer = kLongChunk / kThreads;
+
+__global__ void __launch_bounds__(kThreads) k_cmp_stage(
+    const CmpPlan* __restrict__ plan, const unsigned long long* __restrict__ items, const int64_t item_cap,
+    const int32_t* __restrict__ pool, uint8_t* __restrict__ mark, int32_t* __restrict__ scr,
+    int2* __restrict__ chunk, const BatchStatus* __restrict__ st) {
+  __shared__ int32_t sh_wsum[kThreads / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int64_t n_items = min((int64_t)st->cmp_items, item_cap);
+  for (int64_t q = blockIdx.x; q < n_items; q += gridDim.x) {
+    const unsigned long long item = items[q];
+    if (item == kNoLongItem) continue;
+    const CmpPlan P = plan[item >> 32];
+    const int32_t j = (int32_t)(uint32_t)item;
+    const int32_t c0 = j * kLongChunk;
+    const int32_t i0 = c0 + (int32_t)threadIdx.x * kCmpPer;
+    int32_t val[kCmpPer];
+    unsigned keepm = 0;
+    int32_t kept = 0;
+#pragma unroll
+    for (int t = 0; t < kCmpPer; ++t) {
+      const int32_t i = i0 + t;
+      bool keep = false;
+      val[t] = 0;
+      if (i < P.a) {
+        keep = mark[P.s + i] == 0;
+        if (keep) val[t] = pool[P.s + i];
+        else mark[P.s + i] = 0;
+      }
+      keepm |= (unsigned)keep << t;
+      kept += keep;
     }
+    int32_t incl = kept;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int32_t y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) sh_wsum[wid] = incl;
     __syncthreads();
+    int32_t before = 0, total = 0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      const int32_t x = sh_wsum[w];
+      if (w < wid) before += x;
+      total += x;
+    }
+    int32_t at = before + incl - kept;
+#pragma unroll
+    for (int t = 0; t < kCmpPer; ++t)
+      if (keepm >> t & 1u) scr[P.soff + c0 + at++] = val[t];
+    if (threadIdx.x == 0) chunk[P.ib + j] = make_int2(0, total);
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cmp_prefix(const CmpPlan* __restrict__ plan, int2* __restrict__ chunk,
+                                                         int32_t* __restrict__ used, BatchStatus* __restrict__ st) {
+  const int64_t n = (int64_t)st->n_cmp;
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+    const CmpPlan P = plan[r];
+    if (P.nch == 0) continue;
+    int32_t off = 0;
+    for (int32_t j = 0; j < P.nch; ++j) {
+      const int32_t c = chunk[P.ib + j].y;
+      chunk[P.ib + j].x = off;
+      off += c;
+    }
+    used[P.v] = off;
+    atomicAdd(&st->dir_removed, (unsigned long long)(P.a - off));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_cmp_write(
+    const CmpPlan* __restrict__ plan, const unsigned long long* __restrict__ items, const int64_t item_cap,
+    const int32_t* __restrict__ scr, const int2* __restrict__ chunk, int32_t* __restrict__ pool,
+    const BatchStatus* __restrict__ st) {
+  const int64_t n_items = min((int64_t)st->cmp_items, item_cap);
+  for (int64_t q = blockIdx.x; q < n_items; q += gridDim.x) {
+    const unsigned long long item = items[q];
+    if (item == kNoLongItem) continue;
+    const CmpPlan P = plan[item >> 32];
+    const int32_t j = (int32_t)(uint32_t)item;
+    const int2 oc = chunk[P.ib + j];
+    for (int32_t t = threadIdx.x; t < oc.y; t += kThreads) pool[P.s + oc.x + t] = scr[P.soff + j * kLongChunk + t];
   }
 }
 
@@ -1471,10 +1548,12 @@ struct StreamWs {
   int32_t* long_runs = nullptr; // [2b] starts of the runs whose list is long
   int32_t* long_cnt = nullptr;  // [2b] their lengths
   LongPlan* long_plan = nullptr;  // [2b]
+  CmpPlan* cmp_plan = nullptr;    // [2b] long lists with deletions
   // long-list insertion scratch, sized with the pool (ensure_long_scratch)
   int32_t* long_scr = nullptr;
   uint8_t* long_smark = nullptr;
   unsigned long long* long_items = nullptr;
+  int2* long_chunk = nullptr;     // per work item: (output offset, kept entries) of a compacted chunk
   int64_t scr_cap = 0;
   int64_t long_item_cap = 0;
   int64_t* ins_slot = nullptr;  // [2b]
@@ -1511,6 +1590,7 @@ void StreamWs::release() {
   cudaFree(src); cudaFree(dst); cudaFree(isdel); cudaFree(keys); cudaFree(keys2); cudaFree(head);
   cudaFree(dlist); cudaFree(ilist); cudaFree(dk); cudaFree(dk2); cudaFree(run_start); cudaFree(long_runs);
   cudaFree(long_cnt); cudaFree(long_plan); cudaFree(long_scr); cudaFree(long_smark); cudaFree(long_items);
+  cudaFree(cmp_plan); cudaFree(long_chunk);
   cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
@@ -1595,8 +1675,8 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     cudaFree(w.src); cudaFree(w.dst); cudaFree(w.isdel); cudaFree(w.keys); cudaFree(w.keys2); cudaFree(w.head);
     cudaFree(w.dlist); cudaFree(w.ilist); cudaFree(w.dk); cudaFree(w.dk2); cudaFree(w.run_start);
     cudaFree(w.long_runs); cudaFree(w.ins_slot); cudaFree(w.vlist); cudaFree(w.cub_tmp);
-    cudaFree(w.long_cnt); cudaFree(w.long_plan);
-    w.long_cnt = nullptr; w.long_plan = nullptr;
+    cudaFree(w.long_cnt); cudaFree(w.long_plan); cudaFree(w.cmp_plan);
+    w.long_cnt = nullptr; w.long_plan = nullptr; w.cmp_plan = nullptr;
     cudaFree(w.hub_list); cudaFree(w.hub_off); cudaFree(w.hub_len); cudaFree(w.hub_fill); cudaFree(w.hub_chunks);
     cudaFree(w.hub_units); cudaFree(w.hubbed); cudaFree(w.hub_items);
     w.src = nullptr; w.dst = nullptr; w.isdel = nullptr; w.keys = nullptr; w.keys2 = nullptr; w.head = nullptr;
@@ -1624,6 +1704,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
             ::tc::dev_malloc(&w.long_runs, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.long_cnt, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.long_plan, sizeof(LongPlan) * 2 * nb) == cudaSuccess &&
+            ::tc::dev_malloc(&w.cmp_plan, sizeof(CmpPlan) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.ins_slot, sizeof(int64_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.vlist, sizeof(int32_t) * 2 * nb) == cudaSuccess &&
             ::tc::dev_malloc(&w.hub_list, sizeof(int32_t) * nb) == cudaSuccess &&
@@ -1653,13 +1734,15 @@ tc_status ensure_long_scratch(tc_graph* g) {
   if (!g->sw) return TC_OK;
   StreamWs& w = *g->sw;
   const int64_t need = g->pool_cap + 2 * w.b_cap;
-  if (w.scr_cap >= need && w.long_scr && w.long_smark && w.long_items) return TC_OK;
+  if (w.scr_cap >= need && w.long_scr && w.long_smark && w.long_items && w.long_chunk) return TC_OK;
   cudaFree(w.long_scr);
   cudaFree(w.long_smark);
   cudaFree(w.long_items);
+  cudaFree(w.long_chunk);
   w.long_scr = nullptr;
   w.long_smark = nullptr;
   w.long_items = nullptr;
+  w.long_chunk = nullptr;
   w.scr_cap = 0;
   w.long_item_cap = 0;
   ++w.version;
@@ -1667,13 +1750,16 @@ tc_status ensure_long_scratch(tc_graph* g) {
   const int64_t icap = cap / kLongChunk + 2 * w.b_cap + 1;
   if (::tc::dev_malloc(&w.long_scr, sizeof(int32_t) * (size_t)cap) != cudaSuccess ||
       ::tc::dev_malloc(&w.long_smark, (size_t)cap) != cudaSuccess ||
-      ::tc::dev_malloc(&w.long_items, sizeof(unsigned long long) * (size_t)icap) != cudaSuccess) {
+      ::tc::dev_malloc(&w.long_items, sizeof(unsigned long long) * (size_t)icap) != cudaSuccess ||
+      ::tc::dev_malloc(&w.long_chunk, sizeof(int2) * (size_t)icap) != cudaSuccess) {
     cudaFree(w.long_scr);
     cudaFree(w.long_smark);
     cudaFree(w.long_items);
+    cudaFree(w.long_chunk);
     w.long_scr = nullptr;
     w.long_smark = nullptr;
     w.long_items = nullptr;
+    w.long_chunk = nullptr;
     return fail(TC_ERR_OOM, "long-list insertion scratch: device allocation failed");
   }
   w.scr_cap = cap;
@@ -1735,6 +1821,21 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
 int delta_grid() { return device_info().sms * 8; }
 int long_grid() { return device_info().sms * 8; }
 
+// Deletions from the batch's long lists (k_cmp_plan, k_cmp_stage, k_cmp_prefix, k_cmp_write): the
+// vertices vlist[0 .. nv) (nv = nv_dev * stride when nv_dev is set, else nv_list, at most
+// nv_cap). The scratch must be sized (ensure_long_scratch).
+void long_compact(tc_graph* g, StreamWs& w, const int32_t* vlist, int64_t nv_list, int stride,
+                  const unsigned long long* nv_dev, int64_t nv_cap, cudaStream_t s) {
+  k_cmp_plan<<<grid_for(nv_cap, kThreads), kThreads, 0, s>>>(vlist, nv_list, stride, nv_dev, g->start, g->used, w.claim,
+                                                            w.d_epoch, w.cmp_plan, w.long_items, w.long_item_cap,
+                                                            w.scr_cap, w.st);
+  k_cmp_stage<<<long_grid(), kThreads, 0, s>>>(w.cmp_plan, w.long_items, w.long_item_cap, g->pool, g->mark, w.long_scr,
+                                               w.long_chunk, w.st);
+  k_cmp_prefix<<<grid_for(nv_cap, kThreads), kThreads, 0, s>>>(w.cmp_plan, w.long_chunk, g->used, w.st);
+  k_cmp_write<<<long_grid(), kThreads, 0, s>>>(w.cmp_plan, w.long_items, w.long_item_cap, w.long_scr, w.long_chunk,
+                                               g->pool, w.st);
+}
+
 // Insertion into the batch's long lists (k_long_plan, k_long_stage, k_long_write); `nd_cap` bounds
 // the long runs (the directed entries' capacity). The scratch must be sized (ensure_pool).
 void long_insert(tc_graph* g, StreamWs& w, int64_t nd_cap, uint8_t* mark, cudaStream_t s) {
@@ -1746,7 +1847,6 @@ void long_insert(tc_graph* g, StreamWs& w, int64_t nd_cap, uint8_t* mark, cudaSt
   k_long_write<<<long_grid(), kThreads, 0, s>>>(w.long_plan, w.long_items, w.long_item_cap, w.long_scr, w.long_smark,
                                                 g->pool, mark, w.st);
 }
-int compact_grid() { return device_info().sms * 8; }
 
 // Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
 // more than can be resident at once (its grid barrier needs every CTA running).
@@ -1930,8 +2030,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
         w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch, w.st);
-    k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used,
-                                                     g->pool, g->mark, w.claim, w.d_epoch, w.st);
+    long_compact(g, w, w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, 2 * (int64_t)h.n_del, s);
     TC_CUDA_TRY(cudaGetLastError());
   }
   // 4. insertions: merge into the lists, count on the post-insertion graph, clear marks
@@ -2065,6 +2164,7 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   if (!g || b < 0 || (b > 0 && (!d_src || !d_dst || !d_dup))) return fail(TC_ERR_INVALID_ARG, "invalid arguments");
   cudaStream_t s = (cudaStream_t)stream;
   TC_TRY(ensure_stream_ws(g, (b + 1) / 2 + 1));
+  TC_TRY(ensure_long_scratch(g));
   StreamWs& w = *g->sw;
   TC_CUDA_TRY(cudaMemsetAsync(w.st, 0, sizeof(BatchStatus), s));
   if (b == 0) return TC_OK;
@@ -2075,8 +2175,7 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
   k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
                                                                    g->pool, g->mark, w.claim, w.d_epoch, w.st);
-  k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used, g->pool, g->mark,
-                                                   w.claim, w.d_epoch, w.st);
+  long_compact(g, w, w.vlist, b, 1, w.counter, b, s);
   TC_CUDA_TRY(cudaGetLastError());
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
   TC_CUDA_TRY(cudaStreamSynchronize(s));
@@ -2349,8 +2448,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
                                              w.claim, w.d_epoch, w.st);
-    k_compact_long<<<compact_grid(), kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool,
-                                                     g->mark, w.claim, w.d_epoch, w.st);
+    long_compact(g, w, w.vlist, 0, 2, &w.st->n_del, 2 * cap, s);
     // insertions: merge, count on the post-insertion graph, clear the marks
     k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
                                           g->pool_cap, g->mark, w.ins_slot, g->d_pool_top, g->slack_q10, w.st);
