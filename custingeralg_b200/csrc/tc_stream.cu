@@ -11,11 +11,12 @@
 // edge is changed comes either from a per-slot mark array parallel to the adjacency pool
 // (tc_apply_batch) or from a lookup in the sorted batch (the cuStinger-style path).
 //
-// Per changed edge the warp intersects the two full lists with one of two strategies chosen by
-// their lengths: binary search of the shorter list's entries into the longer ("search", for
-// skewed pairs) or a partitioned merge in which each lane owns a contiguous slice of the shorter
-// list and merges it against the longer one from a binary-searched start ("merge", for balanced
-// pairs).
+// Per changed edge the warp intersects the two full lists with a strategy chosen by their
+// lengths: binary search of the shorter list's entries into the longer ("search", for skewed
+// pairs), a partitioned merge in which each lane owns a contiguous slice of the shorter list and
+// merges it against the longer one from a binary-searched start ("merge", for balanced pairs), or,
+// where the strategy table asks for it, the longer list staged into shared memory piece by piece
+// with cp.async and searched there ("stage").
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -30,7 +31,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr uint64_t kSentinel = ~0ull;
 constexpr int kLongList = 2048;  // lists longer than this are rewritten by a whole CTA
-constexpr int kRunStage = 4096;  // new entries of one long list staged in shared memory
 // Tile shape of the delta count (defaults; the pipeline's autotuner picks per batch-size bin):
 constexpr int kDeltaSplit = 2048;   // intersections whose shorter list is longer are split ...
 constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of the shorter list
@@ -43,6 +43,8 @@ constexpr unsigned long long kSpinNs = 2000000000ull;  // 2 s
 constexpr unsigned kSpinMaxIters = 1u << 24;
 
 enum : unsigned { kErrRange = 1u, kErrPool = 2u, kErrTimeout = 4u, kErrScratch = 8u };
+// first_del[v] between batches: no deletion marked in v's list (0x7f7f7f7f, a byte memset)
+constexpr int32_t kNoDel = 0x7f7f7f7f;
 constexpr unsigned long long kNoLongItem = ~0ull;
 
 struct BatchStatus {
@@ -98,6 +100,34 @@ __device__ __forceinline__ int64_t lower_bound(const int32_t* __restrict__ list,
   }
   return lo;
 }
+
+// First index of the ascending list lst[0 .. len) whose entry is >= key, found by the warp: 32
+// evenly spaced samples per round (one load each lane), so a list of up to 32^r entries takes r
+// rounds. Every lane returns the same index.
+__device__ __forceinline__ int32_t warp_lower_bound(const int32_t* __restrict__ lst, int32_t len, int32_t key) {
+  const int lane = threadIdx.x & 31;
+  int32_t lo = 0, hi = len;  // the answer lies in [lo, hi]
+  while (hi - lo > 32) {
+    const int32_t step = (hi - lo + 31) / 32;
+    const int32_t p = lo + lane * step;
+    const int32_t v = p < hi ? lst[p] : INT32_MAX;
+    const int c = __popc(__ballot_sync(kFull, v < key));  // the samples below key are a prefix
+    const int32_t nlo = c > 0 ? lo + (c - 1) * step + 1 : lo;
+    hi = c < 32 ? min(hi, lo + c * step) : hi;
+    lo = nlo;
+  }
+  const int32_t p = lo + lane;
+  const int32_t v = p < hi ? lst[p] : INT32_MAX;
+  return lo + __popc(__ballot_sync(kFull, v < key));
+}
+
+// Asynchronous 4-byte copy from global to shared memory (cp.async, no register round trip); the
+// copies of a thread complete at cp_async_wait_all.
+__device__ __forceinline__ void cp_async4(int32_t* smem_dst, const int32_t* gsrc) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 int grid_for(int64_t items, int per_block) {
   const int64_t want = std::max<int64_t>(1, (items + per_block - 1) / per_block);
@@ -262,6 +292,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
     }
     const int32_t* A = pool + s_old;
     // New entries first, while A is intact: final position j + #(old < B[j]) (relative).
+    int32_t first_new = a;  // old entries below the smallest new entry keep their slots
     for (int64_t j = i0 + lane; j < i1; j += 32) {
       const int32_t val = (int32_t)(uint32_t)dk[j];
       int32_t lo = 0, hi = a;
@@ -271,15 +302,18 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
         else hi = mid;
       }
       slot[j] = (j - i0) + lo;
+      if (j == i0) first_new = lo;
     }
     __syncwarp();
+    // In place, old entries below the first new entry do not move; relocated, all of them do.
+    const int32_t keep_below = moved ? 0 : __shfl_sync(kFull, first_new, 0);
     // Old entries: final position i + #(new < A[i]); backwards in chunks so that, in place, no
     // unread entry is overwritten (targets never precede sources).
-    for (int32_t base = ((a - 1) / 32) * 32; base >= 0 && a > 0; base -= 32) {
+    for (int32_t base = ((a - 1) / 32) * 32; base >= (keep_below / 32) * 32 && a > 0; base -= 32) {
       const int32_t i = base + lane;
       int32_t val = 0;
       int64_t pos = 0;
-      if (i < a) {
+      if (i < a && i >= keep_below) {
         val = A[i];
         int64_t lo = i0, hi = i1;
         while (lo < hi) {
@@ -290,7 +324,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
         pos = i + (lo - i0);
       }
       __syncwarp();
-      if (i < a) {
+      if (i < a && i >= keep_below) {
         pool[s_new + pos] = val;
         if (mark) mark[s_new + pos] = 0;
       }
@@ -324,23 +358,29 @@ __global__ void k_clear_slots(const int64_t* __restrict__ slot, const int64_t n_
 
 // ---- deletion -------------------------------------------------------------------------------
 
+// Mark the slots of the batch's deletions and keep each list's smallest marked slot (the
+// compaction leaves the entries below it in place).
 __global__ void k_mark_deletions(const int4* __restrict__ dlist, const BatchStatus* __restrict__ st,
-                                 const int64_t* __restrict__ start, uint8_t* __restrict__ mark) {
+                                 const int64_t* __restrict__ start, uint8_t* __restrict__ mark,
+                                 int32_t* __restrict__ first_del) {
   const int64_t nd = (int64_t)st->n_del;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd; i += (int64_t)gridDim.x * blockDim.x) {
     const int4 d = dlist[i];
     mark[start[d.x] + d.z] = 1;
     mark[start[d.y] + d.w] = 1;
+    atomicMin(&first_del[d.x], d.z);
+    atomicMin(&first_del[d.y], d.w);
   }
 }
 
 // Remove marked slots from the lists of the vertices in vlist (each vertex once: the first warp
-// to claim it with this epoch compacts it), then clear the marks of the old range.
+// to claim it with this epoch compacts it), then clear the marks of the old range. The entries
+// below the list's first marked slot (first_del, reset here to kNoDel) stay where they are.
 __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
                                  const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start,
                                  int32_t* __restrict__ used, int32_t* __restrict__ pool, uint8_t* __restrict__ mark,
                                  unsigned* __restrict__ claim, const unsigned* __restrict__ epoch_dev,
-                                 BatchStatus* __restrict__ st) {
+                                 int32_t* __restrict__ first_del, BatchStatus* __restrict__ st) {
   const int lane = threadIdx.x & 31;
   const unsigned epoch = *epoch_dev;
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -357,8 +397,11 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
     if (old >= epoch) continue;
     const int64_t s = start[v];
     const int32_t a = used[v];
-    int32_t wp = 0;
-    for (int32_t base = 0; base < a; base += 32) {
+    const int32_t f = min(first_del[v], a);
+    __syncwarp();
+    if (lane == 0) first_del[v] = kNoDel;
+    int32_t wp = f;
+    for (int32_t base = f; base < a; base += 32) {
       const int32_t i = base + lane;
       int32_t val = 0;
       bool keep = false;
@@ -373,7 +416,7 @@ __global__ void k_compact_marked(const int32_t* __restrict__ vlist, const int64_
       wp += __popc(m);
       __syncwarp();
     }
-    for (int32_t i = lane; i < a; i += 32) mark[s + i] = 0;
+    for (int32_t i = f + lane; i < a; i += 32) mark[s + i] = 0;
     if (lane == 0) {
       used[v] = wp;
       atomicAdd(&st->dir_removed, (unsigned long long)(a - wp));
@@ -536,20 +579,20 @@ __global__ void __launch_bounds__(kThreads) k_long_write(
 // The scratch keeps sources and targets apart, so chunks of one list proceed on many CTAs.
 struct CmpPlan {
   int64_t s;       // list start
-  int64_t soff;    // the list's range in the scratch buffer
+  int64_t soff;    // the list's range in the scratch buffer (chunks j0 on)
   int64_t ib;      // its first work item
   int32_t v;
   int32_t a;       // entries before the deletions
-  int32_t nch;     // work items (chunks)
-  int32_t pad;
+  int32_t nch;     // work items: chunks j0 .. j0 + nch - 1
+  int32_t j0;      // the chunk of the first marked slot; the chunks below it stay in place
 };
 
 __global__ void __launch_bounds__(kThreads) k_cmp_plan(
     const int32_t* __restrict__ vlist, const int64_t nv_list, const int stride,
     const unsigned long long* __restrict__ nv_dev, const int64_t* __restrict__ start,
     const int32_t* __restrict__ used, unsigned* __restrict__ claim, const unsigned* __restrict__ epoch_dev,
-    CmpPlan* __restrict__ plan, unsigned long long* __restrict__ items, const int64_t item_cap,
-    const int64_t scr_cap, BatchStatus* __restrict__ st) {
+    int32_t* __restrict__ first_del, CmpPlan* __restrict__ plan, unsigned long long* __restrict__ items,
+    const int64_t item_cap, const int64_t scr_cap, BatchStatus* __restrict__ st) {
   const unsigned epoch = *epoch_dev;
   const int64_t cnt = nv_dev ? (int64_t)(*nv_dev) * stride : nv_list;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x) {
@@ -561,17 +604,20 @@ __global__ void __launch_bounds__(kThreads) k_cmp_plan(
     P.v = v;
     P.a = a;
     P.s = start[v];
-    P.nch = (a + kLongChunk - 1) / kLongChunk;
-    P.pad = 0;
-    const unsigned long long so = atomicAdd(&st->cmp_scr, (unsigned long long)a);
+    const int32_t f = min(first_del[v], a);
+    first_del[v] = kNoDel;
+    P.j0 = f / kLongChunk;
+    P.nch = f < a ? (a + kLongChunk - 1) / kLongChunk - P.j0 : 0;
+    const int32_t span = a - P.j0 * kLongChunk;  // entries from chunk j0 on
+    const unsigned long long so = atomicAdd(&st->cmp_scr, (unsigned long long)span);
     const unsigned long long ib = atomicAdd(&st->cmp_items, (unsigned long long)P.nch);
     const unsigned long long r = atomicAdd(&st->n_cmp, 1ull);
-    if ((int64_t)(so + a) > scr_cap || (int64_t)(ib + P.nch) > item_cap) {
+    if ((int64_t)(so + span) > scr_cap || (int64_t)(ib + P.nch) > item_cap) {
       atomicOr(&st->err, kErrScratch);  // unreachable while the scratch follows the pool's size
       for (int32_t j = 0; j < P.nch && (int64_t)(ib + j) < item_cap; ++j) items[ib + j] = kNoLongItem;
       P.nch = 0;
     } else {
-      for (int32_t j = 0; j < P.nch; ++j) items[ib + j] = (r << 32) | (unsigned)j;
+      for (int32_t j = 0; j < P.nch; ++j) items[ib + j] = (r << 32) | (unsigned)(P.j0 + j);
     }
     P.soff = (int64_t)so;
     P.ib = (int64_t)ib;
@@ -595,6 +641,7 @@ __global__ void __launch_bounds__(kThreads) k_cmp_stage(
     const CmpPlan P = plan[item >> 32];
     const int32_t j = (int32_t)(uint32_t)item;
     const int32_t c0 = j * kLongChunk;
+    const int32_t r0 = (j - P.j0) * kLongChunk;  // the chunk's place in the list's scratch range
     const int32_t i0 = c0 + (int32_t)threadIdx.x * kCmpPer;
     int32_t val[kCmpPer];
     unsigned keepm = 0;
@@ -629,8 +676,8 @@ __global__ void __launch_bounds__(kThreads) k_cmp_stage(
     int32_t at = before + incl - kept;
 #pragma unroll
     for (int t = 0; t < kCmpPer; ++t)
-      if (keepm >> t & 1u) scr[P.soff + c0 + at++] = val[t];
-    if (threadIdx.x == 0) chunk[P.ib + j] = make_int2(0, total);
+      if (keepm >> t & 1u) scr[P.soff + r0 + at++] = val[t];
+    if (threadIdx.x == 0) chunk[P.ib + (j - P.j0)] = make_int2(0, total);
     __syncthreads();
   }
 }
@@ -641,7 +688,7 @@ __global__ void __launch_bounds__(kThreads) k_cmp_prefix(const CmpPlan* __restri
   for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
     const CmpPlan P = plan[r];
     if (P.nch == 0) continue;
-    int32_t off = 0;
+    int32_t off = P.j0 * kLongChunk;  // the chunks below j0 keep their entries in place
     for (int32_t j = 0; j < P.nch; ++j) {
       const int32_t c = chunk[P.ib + j].y;
       chunk[P.ib + j].x = off;
@@ -661,7 +708,7 @@ __global__ void __launch_bounds__(kThreads) k_cmp_write(
     const unsigned long long item = items[q];
     if (item == kNoLongItem) continue;
     const CmpPlan P = plan[item >> 32];
-    const int32_t j = (int32_t)(uint32_t)item;
+    const int32_t j = (int32_t)(uint32_t)item - P.j0;
     const int2 oc = chunk[P.ib + j];
     for (int32_t t = threadIdx.x; t < oc.y; t += kThreads) pool[P.s + oc.x + t] = scr[P.soff + j * kLongChunk + t];
   }
@@ -716,6 +763,7 @@ struct DeltaArgs {
   // dynamic work queues of k_delta_fused's two passes (zero at launch; NULL = warp-strided)
   unsigned long long* e_next;
   unsigned long long* i_next;
+  int stage_ok;      // the launch has kStageSmem of dynamic shared memory: staged cells may stage
   uint8_t table[256];
 };
 
@@ -761,12 +809,19 @@ __device__ __forceinline__ bool delta_entry(const DeltaArgs& A, int64_t e, int32
   return x != y;
 }
 
+// Intersection strategies of the delta count (the streaming strategy table's values).
+enum : int { kStratSearch = 0, kStratMerge = 1, kStratStage = 2 };
+constexpr int kStageEntries = 1024;  // entries of the longer list a warp stages per piece
+// Dynamic shared memory of a delta kernel launch that may stage (one buffer per warp); a launch
+// without it runs the staged cells as merges.
+constexpr size_t kStageSmem = sizeof(int32_t) * kStageEntries * (kThreads / 32);
+
 // The two lists of edge {x, y} as the intersection takes them: A the shorter, B the longer.
 struct DeltaPair {
   int32_t oa, ob, la, lb;
   int64_t sa, sb;
   uint64_t key;
-  bool search;
+  int strat;
   int cell;
 };
 
@@ -783,7 +838,12 @@ __device__ __forceinline__ DeltaPair delta_pair(const DeltaArgs& A, int32_t x, i
   P.key = ekey(x, y);
   P.cell = cell_of(P.la, P.lb);
   const int lg = 32 - __clz(P.lb);
-  P.search = A.use_table ? A.table[P.cell] == 0 : 16LL * P.lb > (long long)A.search_ratio_x16 * P.la * lg;
+  if (A.use_table) {
+    const int t = A.table[P.cell];
+    P.strat = t == kStratSearch ? kStratSearch : (t == kStratStage && A.stage_ok) ? kStratStage : kStratMerge;
+  } else {
+    P.strat = 16LL * P.lb > (long long)A.search_ratio_x16 * P.la * lg ? kStratSearch : kStratMerge;
+  }
   return P;
 }
 
@@ -806,7 +866,47 @@ __device__ __forceinline__ uint32_t delta_range(const DeltaArgs& A, const DeltaP
     }
   };
   const int64_t sb = P.sb, eb = P.sb + P.lb;
-  if (P.search) {
+  if (P.strat == kStratStage) {
+    // The part of the longer list that can meet entries [i_begin, i_end) of the shorter one,
+    // [lo, hi), is staged into this warp's shared-memory buffer in pieces of kStageEntries
+    // (cp.async: every copy of a piece in flight at once); each lane then binary-searches one
+    // shorter-list entry in the piece. A piece takes the shorter-list entries up to its last
+    // entry (the last piece takes the rest), so each is searched once.
+    extern __shared__ __align__(16) int32_t s_stage[];  // kStageSmem bytes (A.stage_ok)
+    int32_t* buf = s_stage + (threadIdx.x >> 5) * kStageEntries;
+    const int32_t a_first = L[P.sa + i_begin], a_last = L[P.sa + i_end - 1];
+    const int32_t lo = warp_lower_bound(L + sb, P.lb, a_first);
+    const int32_t hi = warp_lower_bound(L + sb, P.lb, a_last + 1);
+    int32_t ia = i_begin;
+    for (int32_t cb = lo; cb < hi && ia < i_end; cb += kStageEntries) {
+      const int32_t n = min(hi - cb, kStageEntries);
+      __syncwarp();  // the previous piece's searches are done with the buffer
+      for (int32_t k = lane; k < n; k += 32) cp_async4(buf + k, L + sb + cb + k);
+      cp_async_wait_all();
+      __syncwarp();
+      const int32_t bmax = buf[n - 1];
+      const bool last = cb + n >= hi;
+      while (ia < i_end) {
+        const int32_t i = ia + lane;
+        const int32_t w = i < i_end ? L[P.sa + i] : INT32_MAX;
+        // the lanes that take part are a prefix (the shorter list ascends with the lane)
+        const bool in = i < i_end && (last || w <= bmax);
+        const int k = __popc(__ballot_sync(kFull, in));
+        if (in) {
+          int32_t l = 0, h = n;
+          while (l < h) {
+            const int32_t mid = (l + h) >> 1;
+            if (buf[mid] < w) l = mid + 1;
+            else h = mid;
+          }
+          if (l < n && buf[l] == w) on_match(i, (int64_t)cb + l, w);
+        }
+        __syncwarp();
+        ia += k;
+        if (k < 32) break;
+      }
+    }
+  } else if (P.strat == kStratSearch) {
     // The first five search levels come from 32 evenly spaced samples of the longer list, one
     // per lane (a single coalesced load): a lane counts the samples below its key with
     // shuffles, then searches memory only inside that bucket.
@@ -1114,14 +1214,20 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, 
 constexpr int kHubThreads = TC_HUB_THREADS;
 constexpr int kHubCtasPerSm = 1536 / kHubThreads;
 constexpr int kHubBucketsMax = 2048 * kHubThreads / 256;  // 64 KB of int32 keys for 512 threads
-constexpr int kHubUnit = 1024;               // partner entries per unit of work of a warp
+#ifndef TC_HUB_UNIT
+#define TC_HUB_UNIT 512
+#endif
+// Partner entries per unit of work of a warp. Smaller units shorten the wait at the end of an
+// item for the warp with the last unit; on the streaming workload 512 entries measured 5 % less
+// time than 1024 over the whole run (prefetching the next 128 entries changed nothing).
+constexpr int kHubUnit = TC_HUB_UNIT;
 constexpr int kHubPass = 2 * kHubBucketsMax;  // entries of N(h) per pass (load <= 0.5)
 constexpr int32_t kHubMarkBit = INT32_MIN;    // bit 31 of a stored key: the edge (h, key) is changed
 constexpr int64_t kHubSearchCost = 64;        // an item's estimate of one range search, in probes
 constexpr int64_t kHubItemMin = 1 << 16;      // probes of work per item at least ...
 constexpr int64_t kHubBuildShare = 16;        // ... and at least this many times its table build
 constexpr int64_t kHubItemsPerUpdate = 4;     // item queue capacity per batch update
-constexpr int64_t kHubUnitsPerUpdate = 4;     // unit slots per batch update
+constexpr int64_t kHubUnitsPerUpdate = kHubUnit >= 1024 ? 4 : 4 * 1024 / kHubUnit;  // unit slots per update
 
 struct HubWs {
   int32_t* cnt;      // [n] changed edges per longer endpoint in this phase (zero between phases)
@@ -1268,26 +1374,6 @@ __device__ __forceinline__ bool hub_find(const int32_t* keys, int bits, int32_t 
     b = (b + 1) & bmask;
   }
   return false;
-}
-
-// First index of the ascending list lst[0 .. len) whose entry is >= key, found by the warp: 32
-// evenly spaced samples per round (one load each lane), so a list of up to 32^r entries takes r
-// rounds. Every lane returns the same index.
-__device__ __forceinline__ int32_t warp_lower_bound(const int32_t* __restrict__ lst, int32_t len, int32_t key) {
-  const int lane = threadIdx.x & 31;
-  int32_t lo = 0, hi = len;  // the answer lies in [lo, hi]
-  while (hi - lo > 32) {
-    const int32_t step = (hi - lo + 31) / 32;
-    const int32_t p = lo + lane * step;
-    const int32_t v = p < hi ? lst[p] : INT32_MAX;
-    const int c = __popc(__ballot_sync(kFull, v < key));  // the samples below key are a prefix
-    const int32_t nlo = c > 0 ? lo + (c - 1) * step + 1 : lo;
-    hi = c < 32 ? min(hi, lo + c * step) : hi;
-    lo = nlo;
-  }
-  const int32_t p = lo + lane;
-  const int32_t v = p < hi ? lst[p] : INT32_MAX;
-  return lo + __popc(__ballot_sync(kFull, v < key));
 }
 
 // Work items of the hubs from one queue: item (hub, j) is pass j / C over unit chunk j % C of the
@@ -1467,7 +1553,8 @@ __global__ void k_flag_present(const SlackView g, const int32_t* __restrict__ s,
 // Mark the slots of present, non-duplicate entries for deletion; list their source vertices.
 __global__ void k_mark_dir_deletions(const SlackView g, const int32_t* __restrict__ s, const int32_t* __restrict__ d,
                                      const int32_t* __restrict__ dup, const int64_t b, uint8_t* __restrict__ mark,
-                                     int32_t* __restrict__ vlist, unsigned long long* __restrict__ nvl) {
+                                     int32_t* __restrict__ first_del, int32_t* __restrict__ vlist,
+                                     unsigned long long* __restrict__ nvl) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
     if (dup[i]) continue;
     const int32_t x = s[i], y = d[i];
@@ -1476,6 +1563,7 @@ __global__ void k_mark_dir_deletions(const SlackView g, const int32_t* __restric
     const int64_t p = lower_bound(g.ind, sx, sx + lx, y);
     if (p < sx + lx && g.ind[p] == y) {
       mark[p] = 1;
+      atomicMin(&first_del[x], (int32_t)(p - sx));
       vlist[atomicAdd(nvl, 1ull)] = x;
     }
   }
@@ -1559,6 +1647,7 @@ struct StreamWs {
   int64_t* ins_slot = nullptr;  // [2b]
   int32_t* vlist = nullptr;     // [2b]
   unsigned* claim = nullptr;    // [n]
+  int32_t* first_del = nullptr; // [n] smallest marked slot of a list in this batch (kNoDel otherwise)
   unsigned* d_epoch = nullptr;  // [1] compaction epoch
   uint64_t version = 0;         // bumped when the batch-sized buffers are reallocated
   void* cub_tmp = nullptr;
@@ -1592,7 +1681,7 @@ void StreamWs::release() {
   cudaFree(long_cnt); cudaFree(long_plan); cudaFree(long_scr); cudaFree(long_smark); cudaFree(long_items);
   cudaFree(cmp_plan); cudaFree(long_chunk);
   cudaFree(ins_slot);
-  cudaFree(vlist); cudaFree(claim); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
+  cudaFree(vlist); cudaFree(claim); cudaFree(first_del); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
   cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
   cudaFree(hub_cnt); cudaFree(hub_sum); cudaFree(hub_uni); cudaFree(hub_of); cudaFree(hub_list); cudaFree(hub_off);
   cudaFree(hub_len); cudaFree(hub_fill); cudaFree(hub_chunks); cudaFree(hub_units); cudaFree(hubbed);
@@ -1627,9 +1716,11 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
   }
   if (w.n_cap < (int64_t)g->n + 1) {
     auto free_pv = [&w]() {
-      cudaFree(w.claim); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles); cudaFree(w.d_epoch);
+      cudaFree(w.claim); cudaFree(w.first_del); cudaFree(w.cnt); cudaFree(w.scan64); cudaFree(w.tiles);
+      cudaFree(w.d_epoch);
       cudaFree(w.hub_cnt); cudaFree(w.hub_sum); cudaFree(w.hub_uni); cudaFree(w.hub_of);
-      w.claim = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr; w.d_epoch = nullptr;
+      w.claim = nullptr; w.first_del = nullptr; w.cnt = nullptr; w.scan64 = nullptr; w.tiles = nullptr;
+      w.d_epoch = nullptr;
       w.hub_cnt = nullptr; w.hub_sum = nullptr; w.hub_uni = nullptr; w.hub_of = nullptr;
       w.n_cap = 0;
     };
@@ -1637,6 +1728,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     ++w.version;
     const size_t n1 = (size_t)g->n + 1;
     if (::tc::dev_malloc(&w.claim, sizeof(unsigned) * n1) != cudaSuccess ||
+        ::tc::dev_malloc(&w.first_del, sizeof(int32_t) * n1) != cudaSuccess ||
         ::tc::dev_malloc(&w.d_epoch, sizeof(unsigned)) != cudaSuccess ||
         ::tc::dev_malloc(&w.cnt, sizeof(int32_t) * n1) != cudaSuccess ||
         ::tc::dev_malloc(&w.scan64, sizeof(int64_t) * (n1 + 1)) != cudaSuccess ||
@@ -1649,6 +1741,7 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
       return fail(TC_ERR_OOM, "batch workspace (per vertex): device allocation failed");
     }
     TC_CUDA_TRY(cudaMemset(w.claim, 0, sizeof(unsigned) * n1));
+    TC_CUDA_TRY(cudaMemset(w.first_del, 0x7f, sizeof(int32_t) * n1));  // kNoDel
     TC_CUDA_TRY(cudaMemset(w.d_epoch, 0, sizeof(unsigned)));
     TC_CUDA_TRY(cudaMemset(w.hub_cnt, 0, sizeof(int32_t) * n1));
     TC_CUDA_TRY(cudaMemset(w.hub_sum, 0, sizeof(long long) * n1));
@@ -1815,8 +1908,14 @@ DeltaArgs delta_args(tc_graph* g, const SchedParams& sp) {
   A.spin_ns = kSpinNs;
   A.hub_min = sp.hub_min;
   memcpy(A.table, sp.table, sizeof(A.table));
+  // staging buffers only for launches whose strategy table stages somewhere
+  if (A.use_table)
+    for (int c = 0; c < 256; ++c) A.stage_ok |= A.table[c] == kStratStage;
   return A;
 }
+
+// Dynamic shared memory of a delta-kernel launch with these arguments.
+size_t delta_smem(const DeltaArgs& A) { return A.stage_ok ? kStageSmem : 0; }
 
 int delta_grid() { return device_info().sms * 8; }
 int long_grid() { return device_info().sms * 8; }
@@ -1827,8 +1926,8 @@ int long_grid() { return device_info().sms * 8; }
 void long_compact(tc_graph* g, StreamWs& w, const int32_t* vlist, int64_t nv_list, int stride,
                   const unsigned long long* nv_dev, int64_t nv_cap, cudaStream_t s) {
   k_cmp_plan<<<grid_for(nv_cap, kThreads), kThreads, 0, s>>>(vlist, nv_list, stride, nv_dev, g->start, g->used, w.claim,
-                                                            w.d_epoch, w.cmp_plan, w.long_items, w.long_item_cap,
-                                                            w.scr_cap, w.st);
+                                                            w.d_epoch, w.first_del, w.cmp_plan, w.long_items,
+                                                            w.long_item_cap, w.scr_cap, w.st);
   k_cmp_stage<<<long_grid(), kThreads, 0, s>>>(w.cmp_plan, w.long_items, w.long_item_cap, g->pool, g->mark, w.long_scr,
                                                w.long_chunk, w.st);
   k_cmp_prefix<<<grid_for(nv_cap, kThreads), kThreads, 0, s>>>(w.cmp_plan, w.long_chunk, g->used, w.st);
@@ -1850,18 +1949,19 @@ void long_insert(tc_graph* g, StreamWs& w, int64_t nd_cap, uint8_t* mark, cudaSt
 
 // Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
 // more than can be resident at once (its grid barrier needs every CTA running).
-tc_status fused_grid(int ctas_per_sm, int* grid) {
+tc_status fused_grid(int ctas_per_sm, size_t smem, int* grid) {
   constexpr int kMaxDev = 64;
-  static int occ[kMaxDev] = {};
+  static int occ[kMaxDev][2] = {};  // without, with the staging buffers
   int dev = 0;
   TC_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDev) return fail(TC_ERR_INVALID_ARG, "device %d out of range", dev);
-  if (occ[dev] == 0) {
+  const int k = smem > 0 ? 1 : 0;
+  if (occ[dev][k] == 0) {
     int b = 0;
-    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_delta_fused<kPredMark>, kThreads, 0));
-    occ[dev] = std::max(1, b);
+    TC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_delta_fused<kPredMark>, kThreads, k ? kStageSmem : 0));
+    occ[dev][k] = std::max(1, b);
   }
-  const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ[dev]) : occ[dev];
+  const int per_sm = ctas_per_sm > 0 ? std::min(ctas_per_sm, occ[dev][k]) : occ[dev][k];
   *grid = device_info().sms * per_sm;
   return TC_OK;
 }
@@ -1942,8 +2042,8 @@ tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, 
   A.i_next = &w.st->i_next[phase];
   TC_TRY(launch_hub(A, w, phase, w.b_cap, pv, tri_out, s));
   int grid = 0;
-  TC_TRY(fused_grid(ctas_per_sm, &grid));
-  k_delta_fused<kPredMark><<<grid, kThreads, 0, s>>>(A, pv, tri_out);
+  TC_TRY(fused_grid(ctas_per_sm, delta_smem(A), &grid));
+  k_delta_fused<kPredMark><<<grid, kThreads, delta_smem(A), s>>>(A, pv, tri_out);
   return TC_OK;
 }
 
@@ -2019,7 +2119,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
   // 3. deletions: mark, count on the pre-deletion graph, compact
   if (h.n_del > 0) {
     const int gd = grid_for((int64_t)h.n_del, kThreads);
-    k_mark_deletions<<<gd, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
+    k_mark_deletions<<<gd, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark, w.first_del);
     DeltaArgs A = delta_args(g, sp);
     A.dlist = w.dlist;
     A.count_dev = &w.st->n_del;
@@ -2029,7 +2129,8 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     k_endpoints<<<gd, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<grid_for(2 * (int64_t)h.n_del * 32, kThreads), kThreads, 0, s>>>(
-        w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch, w.st);
+        w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, g->start, g->used, g->pool, g->mark, w.claim, w.d_epoch,
+        w.first_del, w.st);
     long_compact(g, w, w.vlist, 2 * (int64_t)h.n_del, 1, nullptr, 2 * (int64_t)h.n_del, s);
     TC_CUDA_TRY(cudaGetLastError());
   }
@@ -2170,11 +2271,12 @@ tc_status tc_delete_sorted(tc_graph* g, const int32_t* d_src, const int32_t* d_d
   if (b == 0) return TC_OK;
   TC_CUDA_TRY(cudaMemsetAsync(w.counter, 0, sizeof(unsigned long long), s));
   SlackView view{g->start, g->used, g->pool};
-  k_mark_dir_deletions<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, g->mark, w.vlist,
-                                                                   w.counter);
+  k_mark_dir_deletions<<<grid_for(b, kThreads), kThreads, 0, s>>>(view, d_src, d_dst, d_dup, b, g->mark, w.first_del,
+                                                                   w.vlist, w.counter);
   k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
   k_compact_marked<<<grid_for(b * 32, kThreads), kThreads, 0, s>>>(w.vlist, b, 1, w.counter, g->start, g->used,
-                                                                   g->pool, g->mark, w.claim, w.d_epoch, w.st);
+                                                                   g->pool, g->mark, w.claim, w.d_epoch, w.first_del,
+                                                                   w.st);
   long_compact(g, w, w.vlist, b, 1, w.counter, b, s);
   TC_CUDA_TRY(cudaGetLastError());
   TC_CUDA_TRY(cudaMemcpyAsync(w.st_host, w.st, sizeof(BatchStatus), cudaMemcpyDeviceToHost, s));
@@ -2204,9 +2306,10 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
     A.split_items = w.split_items;
     A.split_cnt = &w.st->n_split[0];
     TC_CUDA_TRY(cudaMemsetAsync(A.split_cnt, 0, sizeof(unsigned long long), s));
-    k_delta<kPredBatch><<<delta_grid(), kThreads, 0, s>>>(A, reinterpret_cast<uint32_t*>(per_vertex), w.counter);
-    k_delta_split<kPredBatch><<<delta_grid(), kThreads, 0, s>>>(A, reinterpret_cast<uint32_t*>(per_vertex),
-                                                                 w.counter);
+    k_delta<kPredBatch><<<delta_grid(), kThreads, delta_smem(A), s>>>(A, reinterpret_cast<uint32_t*>(per_vertex),
+                                                                     w.counter);
+    k_delta_split<kPredBatch><<<delta_grid(), kThreads, delta_smem(A), s>>>(A, reinterpret_cast<uint32_t*>(per_vertex),
+                                                                           w.counter);
     TC_CUDA_TRY(cudaGetLastError());
   }
   if (delta_dev) {
@@ -2404,7 +2507,8 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
   const int g2 = grid_for(2 * cap, kThreads);
   const int gw = grid_for(2 * cap * 32, kThreads);
   int gdelta = 0, ghub = 0;
-  TC_TRY(fused_grid(pc.ctas, &gdelta));
+  const size_t dsm = delta_smem(delta_args(g, p->sp));
+  TC_TRY(fused_grid(pc.ctas, dsm, &gdelta));
   TC_TRY(hub_grid(&ghub));
   cudaGraph_t graph = nullptr;
   TC_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
@@ -2423,7 +2527,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
       break;
     k_dir_runs<<<g2, kThreads, 0, s>>>(w.dk2, 2 * cap, g->used, g->cap, g->slack_q10, w.run_start, w.long_runs, w.long_cnt, w.st);
     // deletions: mark, count on the pre-deletion graph, compact
-    k_mark_deletions<<<gb, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark);
+    k_mark_deletions<<<gb, kThreads, 0, s>>>(w.dlist, w.st, g->start, g->mark, w.first_del);
     DeltaArgs A = delta_args(g, p->sp);
     A.dlist = w.dlist;
     A.count_dev = &w.st->n_del;
@@ -2442,12 +2546,12 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.i_next = &w.st->i_next[0];
     if (p->profile) cudaEventRecordWithFlags(p->pev[0], s, cudaEventRecordExternal);
     hub_kernels(A, w, 0, cap, ghub, pv, &w.st->tri_removed, s);
-    k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(A, pv, &w.st->tri_removed);
+    k_delta_fused<kPredMark><<<gdelta, kThreads, dsm, s>>>(A, pv, &w.st->tri_removed);
     if (p->profile) cudaEventRecordWithFlags(p->pev[1], s, cudaEventRecordExternal);
     k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
     k_bump_epoch<<<1, 32, 0, s>>>(w.d_epoch);
     k_compact_marked<<<gw, kThreads, 0, s>>>(w.vlist, 0, 2, &w.st->n_del, g->start, g->used, g->pool, g->mark,
-                                             w.claim, w.d_epoch, w.st);
+                                             w.claim, w.d_epoch, w.first_del, w.st);
     long_compact(g, w, w.vlist, 0, 2, &w.st->n_del, 2 * cap, s);
     // insertions: merge, count on the post-insertion graph, clear the marks
     k_insert_runs<<<gw, kThreads, 0, s>>>(w.dk2, 2 * cap, w.run_start, g->start, g->used, g->cap, g->pool,
@@ -2464,7 +2568,7 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     B.i_next = &w.st->i_next[1];
     if (p->profile) cudaEventRecordWithFlags(p->pev[2], s, cudaEventRecordExternal);
     hub_kernels(B, w, 1, cap, ghub, pv, &w.st->tri_added, s);
-    k_delta_fused<kPredMark><<<gdelta, kThreads, 0, s>>>(B, pv, &w.st->tri_added);
+    k_delta_fused<kPredMark><<<gdelta, kThreads, dsm, s>>>(B, pv, &w.st->tri_added);
     if (p->profile) cudaEventRecordWithFlags(p->pev[3], s, cudaEventRecordExternal);
     k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);
     k_add_delta<<<1, 32, 0, s>>>(delta, &w.st->tri_added, &w.st->tri_removed);
@@ -2705,7 +2809,8 @@ tc_status tc_pipeline_info(const tc_pipeline* p, int32_t* nbins, int64_t* bin_ca
     if (bin_cap) bin_cap[i] = p->bin_cap[i];
     if (delta_blocks_per_sm) {
       int grid = 0;
-      if (fused_grid(kPipeCand[p->cand[bin]].ctas, &grid) != TC_OK) return TC_ERR_CUDA;
+      if (fused_grid(kPipeCand[p->cand[bin]].ctas, delta_smem(delta_args(p->g, p->sp)), &grid) != TC_OK)
+        return TC_ERR_CUDA;
       delta_blocks_per_sm[i] = grid / device_info().sms;
     }
   }

@@ -349,10 +349,25 @@ def _hub_graph(rng, n, hubs, per_hub, pool_size, extra):
     return G.from_pairs(n, np.concatenate(src), np.concatenate(dst))
 
 
+def _strategy_sched(strategy):
+    """None: the default rule; "staged": every degree cell staged (the longer list copied into
+    shared memory piece by piece, the shorter list's entries searched there); "staged_per_edge":
+    the same with the hub count off, so every changed edge, hub-hub ones included, is staged."""
+    if strategy is None:
+        return None
+    from custingeralg_b200 import sched_learn as L
+    s = L.forced(2)
+    if strategy == "staged_per_edge":
+        s.stream_hub_min = 0
+    return s
+
+
+@pytest.mark.parametrize("strategy", [None, "staged", "staged_per_edge"])
 @pytest.mark.parametrize("path", ["pipeline", "apply"])
-def test_split_intersections_between_hubs(path):
+def test_split_intersections_between_hubs(path, strategy):
     """Edges whose both lists exceed 2048 entries are split into queued chunks (k_delta_split):
-    inserting and deleting hub-hub edges must still give the recount, total and per vertex."""
+    inserting and deleting hub-hub edges must still give the recount, total and per vertex, with
+    each intersection strategy."""
     torch = _torch()
     rng = np.random.default_rng(77)
     n, hubs = 16000, 6
@@ -360,7 +375,8 @@ def test_split_intersections_between_hubs(path):
     assert np.sort(np.diff(base.off))[-hubs] > 2048
     graph = api.Graph.from_csr(base, slack=0.25)
     T0, pv0 = _recount(graph, n)
-    pipe = api.Pipeline(graph, 1 << 14) if path == "pipeline" else None
+    sched = _strategy_sched(strategy)
+    pipe = api.Pipeline(graph, 1 << 14, sched=sched) if path == "pipeline" else None
     pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
     delta = torch.zeros(1, dtype=torch.int64, device="cuda")
     cur = base
@@ -384,7 +400,7 @@ def test_split_intersections_between_hubs(path):
             pipe.apply(ts, td, tx, per_vertex=pv, delta_dev=delta)
             pipe.sync()
         else:
-            graph.apply_batch(ts, td, tx, per_vertex=pv, delta_dev=delta)
+            graph.apply_batch(ts, td, tx, per_vertex=pv, delta_dev=delta, sched=sched)
         want = expected_after(n, es, s, d, x)
         off, ind = graph.export()
         assert np.array_equal(off, want.off) and np.array_equal(ind, want.ind)

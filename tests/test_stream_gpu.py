@@ -156,9 +156,15 @@ def _cus_batch(n, s, d, graph):
     return ds, dd, off, dup
 
 
+@pytest.mark.parametrize("strategy", [None, 0, 1, 2])
 @pytest.mark.parametrize("seed", range(8))
-def test_custinger_path_matches_reference_kernels(seed):
-    """sortDeviceBUD + edgeInsertionsSorted + callDeviceNewTriangles == K1 + K2 - K3 (oracle)."""
+def test_custinger_path_matches_reference_kernels(seed, strategy):
+    """sortDeviceBUD + edgeInsertionsSorted + callDeviceNewTriangles == K1 + K2 - K3 (oracle),
+    with the default rule and with every degree cell forced to one intersection strategy
+    (0 search, 1 merge, 2 staged in shared memory)."""
+    from custingeralg_b200 import sched_learn as L
+    sched = None if strategy is None else L.forced(strategy)
+    sp = None if sched is None else ctypes.byref(sched)
     torch = _torch()
     rng = np.random.default_rng(50 + seed)
     n = int(rng.integers(8, 800))
@@ -190,7 +196,7 @@ def test_custinger_path_matches_reference_kernels(seed):
     pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
     delta = torch.zeros(1, dtype=torch.int64, device="cuda")
     N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
-                                   bs.size, 1, pv.data_ptr(), delta.data_ptr(), None, None))
+                                   bs.size, 1, pv.data_ptr(), delta.data_ptr(), sp, None))
     want = O.new_triangles(n, after.off, after.ind, ss, sd, boff, odup)
     assert np.array_equal(pv[:n].cpu().numpy(), want)
     assert int(delta.item()) == (O.host_count_triangles(n, after.off, after.ind)[0]
@@ -198,7 +204,7 @@ def test_custinger_path_matches_reference_kernels(seed):
     # deletion of the same batch: count before, then delete, back to the base graph
     pv2 = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
     N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
-                                   bs.size, -1, pv2.data_ptr(), None, None, None))
+                                   bs.size, -1, pv2.data_ptr(), None, sp, None))
     # dup now flags the pre-existing entries, so exactly the inserted edges go away
     N.check(N.lib().tc_delete_sorted(graph.handle, ds.data_ptr(), dd.data_ptr(), dup.data_ptr(), bs.size, None))
     o3, i3 = graph.export()
@@ -206,10 +212,13 @@ def test_custinger_path_matches_reference_kernels(seed):
     assert np.array_equal(pv2[:n].cpu().numpy(), (-want.astype(np.int64)).astype(np.int32))
 
 
-def test_custinger_path_splits_hub_hub_intersections():
+@pytest.mark.parametrize("strategy", [None, 2])
+def test_custinger_path_splits_hub_hub_intersections(strategy):
     """callDeviceNewTriangles on hub-hub edges (both lists > 2048, counted in queued chunks)
     equals the reference's K1 + K2 - K3 on the oracle, per vertex; the deletion count of the same
-    edges gives the negative."""
+    edges gives the negative. Strategy 2 stages every intersection in shared memory."""
+    from custingeralg_b200 import sched_learn as L
+    sp = None if strategy is None else ctypes.byref(L.forced(strategy))
     torch = _torch()
     rng = np.random.default_rng(91)
     n, hubs = 9000, 4
@@ -233,7 +242,7 @@ def test_custinger_path_splits_hub_hub_intersections():
     pv = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
     delta = torch.zeros(1, dtype=torch.int64, device="cuda")
     N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
-                                   bs.size, 1, pv.data_ptr(), delta.data_ptr(), None, None))
+                                   bs.size, 1, pv.data_ptr(), delta.data_ptr(), sp, None))
     want = O.new_triangles(n, after.off, after.ind, ss, sd, boff, odup)
     assert np.array_equal(pv[:n].cpu().numpy(), want)
     t_after = O.host_count_triangles(n, after.off, after.ind)[0] // 6
@@ -242,6 +251,6 @@ def test_custinger_path_splits_hub_hub_intersections():
     pv2 = torch.zeros(n + 1, dtype=torch.int32, device="cuda")
     delta2 = torch.zeros(1, dtype=torch.int64, device="cuda")
     N.check(N.lib().tc_count_batch(graph.handle, ds.data_ptr(), dd.data_ptr(), off.data_ptr(), dup.data_ptr(),
-                                   bs.size, -1, pv2.data_ptr(), delta2.data_ptr(), None, None))
+                                   bs.size, -1, pv2.data_ptr(), delta2.data_ptr(), sp, None))
     assert np.array_equal(pv2[:n].cpu().numpy(), -want)
     assert int(delta2.item()) == -(t_after - t_base)
