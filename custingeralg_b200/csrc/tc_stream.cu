@@ -68,7 +68,7 @@ struct BatchStatus {
   unsigned long long cmp_items;
   unsigned long long n_split[2];  // split-intersection items queued (deletions, insertions)
   unsigned long long delta_bytes; // algorithmic bytes of the batch's intersections (4(deg x + deg y) + 8 each)
-  unsigned int bar[2];            // grid-barrier arrivals of the persistent delta kernels
+  unsigned int entry_done[2];     // warps of the persistent delta kernel done with the entry pass
   unsigned int err;
   unsigned int pad;
   unsigned long long n_hubs[2];   // hub groups of the delta count (deletions, insertions)
@@ -128,6 +128,21 @@ __device__ __forceinline__ void cp_async4(int32_t* smem_dst, const int32_t* gsrc
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// GPU-scope release store and acquire loads (publication of work items between CTAs).
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
 
 int grid_for(int64_t items, int per_block) {
   const int64_t want = std::max<int64_t>(1, (items + per_block - 1) / per_block);
@@ -627,6 +642,7 @@ __global__ void __launch_bounds__(kThreads) k_cmp_plan(
 
 // Each thread holds kCmpPer consecutive entries of the chunk (256 threads x 16 = kLongChunk).
 constexpr int kCmpPer = kLongChunk / kThreads;
+static_assert(kCmpPer % 4 == 0, "a thread's run of entries is whole 16-byte units");
 
 __global__ void __launch_bounds__(kThreads) k_cmp_stage(
     const CmpPlan* __restrict__ plan, const unsigned long long* __restrict__ items, const int64_t item_cap,
@@ -646,18 +662,41 @@ __global__ void __launch_bounds__(kThreads) k_cmp_stage(
     int32_t val[kCmpPer];
     unsigned keepm = 0;
     int32_t kept = 0;
+    if (i0 + kCmpPer <= P.a) {
+      // a full run of kCmpPer entries: 16-byte loads of the entries (list starts are multiples of
+      // 4 entries and i0 of kCmpPer) and 4-byte loads of their marks, all independent
+      const int4* e4 = reinterpret_cast<const int4*>(pool + P.s + i0);
+      uint32_t* m4 = reinterpret_cast<uint32_t*>(mark + P.s + i0);
 #pragma unroll
-    for (int t = 0; t < kCmpPer; ++t) {
-      const int32_t i = i0 + t;
-      bool keep = false;
-      val[t] = 0;
-      if (i < P.a) {
-        keep = mark[P.s + i] == 0;
-        if (keep) val[t] = pool[P.s + i];
-        else mark[P.s + i] = 0;
+      for (int u = 0; u < kCmpPer / 4; ++u) {
+        const int4 v = e4[u];
+        const uint32_t m = m4[u];
+        val[4 * u] = v.x;
+        val[4 * u + 1] = v.y;
+        val[4 * u + 2] = v.z;
+        val[4 * u + 3] = v.w;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const bool keep = ((m >> (8 * b)) & 0xffu) == 0;
+          keepm |= (unsigned)keep << (4 * u + b);
+          kept += keep;
+        }
+        if (m) m4[u] = 0u;  // the deleted slots' marks are cleared (kept slots' are zero)
       }
-      keepm |= (unsigned)keep << t;
-      kept += keep;
+    } else {
+#pragma unroll
+      for (int t = 0; t < kCmpPer; ++t) {
+        const int32_t i = i0 + t;
+        bool keep = false;
+        val[t] = 0;
+        if (i < P.a) {
+          keep = mark[P.s + i] == 0;
+          if (keep) val[t] = pool[P.s + i];
+          else mark[P.s + i] = 0;
+        }
+        keepm |= (unsigned)keep << t;
+        kept += keep;
+      }
     }
     int32_t incl = kept;
 #pragma unroll
@@ -748,10 +787,15 @@ struct DeltaArgs {
   int shard;         // this rank counts the entries e with e % nshards == shard
   int nshards;
   unsigned long long* bytes_out;  // algorithmic bytes of the intersections run (NULL = not kept)
-  // persistent kernel (k_delta_fused): grid-barrier arrivals (zero at launch), where a wait
-  // that runs out reports kErrTimeout, the arrivals it waits for beyond the grid (0; a test sets
-  // 1 to make the wait run out) and its bound
-  unsigned* bar;
+  // persistent kernel (k_delta_fused): its warps take split items while other warps still run
+  // the entry pass. An item slot is published by writing the launch's epoch (*item_epoch, bumped
+  // before each launch) into item_tag[slot]; entry_done counts the warps done with the entry
+  // pass (zero at launch). A wait for an item that runs out reports kErrTimeout in err; bar_extra
+  // is added to the warps the item pass waits for (0; a test sets 1 to make the wait run out);
+  // spin_ns bounds each wait.
+  unsigned* entry_done;
+  unsigned* item_tag;
+  const unsigned* item_epoch;
   unsigned* err;
   unsigned bar_extra;
   unsigned long long spin_ns;
@@ -1010,6 +1054,7 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
                                               unsigned long long& bytes_acc) {
   const int lane = threadIdx.x & 31;
   const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
+  const unsigned epoch = A.item_tag ? *A.item_epoch : 0u;
   int64_t next = gw, next_end = 0;
   for (;;) {
     // the next entry: warp-strided, or from runs of kGrab entries taken from the queue
@@ -1055,8 +1100,10 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
       at = __shfl_sync(kFull, at, 0);
       const bool fits = at + (unsigned long long)nch <= (unsigned long long)kDeltaItems;
       for (int j = lane; j < nch; j += 32)
-        if (at + j < (unsigned long long)kDeltaItems)
+        if (at + j < (unsigned long long)kDeltaItems) {
           A.split_items[at + j] = fits ? ((unsigned long long)e << 24) | (unsigned long long)j : kNoItem;
+          if (A.item_tag) st_release(A.item_tag + at + j, epoch);  // the slot is ready
+        }
       if (fits) continue;
     }
     const uint32_t c = delta_range<PRED>(A, P, 0, P.la, pv);
@@ -1068,19 +1115,43 @@ __device__ __forceinline__ void delta_entries(const DeltaArgs& A, uint32_t* __re
   }
 }
 
-// The queued chunks of the split intersections, one warp per item. An item's edge passed every
-// check of the entry pass already; its endpoints' per-vertex updates and the total add up per
-// chunk. kCoherent: the items were written by other CTAs of the same launch, so they are read
-// past the (non-coherent) L1.
-template <int PRED, bool kCoherent>
+// One queued chunk of a split intersection, run by the warp. The item's edge passed every check
+// of the entry pass already; its endpoints' per-vertex updates and the total add up per chunk.
+template <int PRED>
+__device__ __forceinline__ void delta_item_run(const DeltaArgs& A, uint32_t* __restrict__ pv,
+                                               const unsigned long long item, const int64_t cnt,
+                                               unsigned long long& tri_acc) {
+  const int lane = threadIdx.x & 31;
+  if (item == kNoItem) return;
+  const int64_t e = (int64_t)(item >> 24);
+  const int32_t k = (int32_t)(item & 0xffffffu);
+  if (e >= cnt) return;  // only an item of an abandoned pass could hold one
+  int32_t x, y;
+  bool count_total;
+  if (!delta_entry<PRED>(A, e, x, y, count_total)) return;
+  const int32_t lx = A.g.len(x), ly = A.g.len(y);
+  const int64_t sx = A.g.start(x), sy = A.g.start(y);
+  const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
+  const int32_t i0 = k * A.chunk;
+  if (i0 >= P.la) return;
+  const uint32_t c = delta_range<PRED>(A, P, i0, min(P.la, i0 + A.chunk), pv);
+  if (lane == 0 && c) {
+    atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
+    atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
+    if (count_total) tri_acc += c;
+  }
+}
+
+// The queued chunks of the split intersections after the entry pass has finished (the second
+// launch of the cuStinger-style count), one warp per item: warp-strided, or one at a time from
+// the queue.
+template <int PRED>
 __device__ __forceinline__ void delta_items(const DeltaArgs& A, uint32_t* __restrict__ pv, const int64_t gw,
                                             const int64_t nw, unsigned long long& tri_acc) {
   const int lane = threadIdx.x & 31;
-  const unsigned long long queued = kCoherent ? __ldcg(A.split_cnt) : *A.split_cnt;
-  const int64_t n_items = (int64_t)min(queued, (unsigned long long)kDeltaItems);
-  const int64_t cnt = A.count_dev ? (int64_t)(kCoherent ? __ldcg(A.count_dev) : *A.count_dev) : A.count_host;
+  const int64_t n_items = (int64_t)min(*A.split_cnt, (unsigned long long)kDeltaItems);
+  const int64_t cnt = A.count_dev ? (int64_t)(*A.count_dev) : A.count_host;
   for (int64_t q0 = gw;;) {
-    // the next item: warp-strided, or taken one at a time from the queue
     int64_t q = q0;
     if (A.i_next) {
       unsigned long long g = 0;
@@ -1090,60 +1161,57 @@ __device__ __forceinline__ void delta_items(const DeltaArgs& A, uint32_t* __rest
       q0 += nw;
     }
     if (q >= n_items) break;
-    const unsigned long long item = kCoherent ? __ldcg(A.split_items + q) : A.split_items[q];
-    if (item == kNoItem) continue;
-    const int64_t e = (int64_t)(item >> 24);
-    const int32_t k = (int32_t)(item & 0xffffffu);
-    if (e >= cnt) continue;  // only an item of an abandoned pass could hold one
-    int32_t x, y;
-    bool count_total;
-    if (!delta_entry<PRED>(A, e, x, y, count_total)) continue;
-    const int32_t lx = A.g.len(x), ly = A.g.len(y);
-    const int64_t sx = A.g.start(x), sy = A.g.start(y);
-    const DeltaPair P = delta_pair(A, x, y, lx, ly, sx, sy);
-    const int32_t i0 = k * A.chunk;
-    if (i0 >= P.la) continue;
-    const uint32_t c = delta_range<PRED>(A, P, i0, min(P.la, i0 + A.chunk), pv);
-    if (lane == 0 && c) {
-      atomicAdd(&pv[x], c * A.weight * (uint32_t)A.sign);
-      atomicAdd(&pv[y], c * A.weight * (uint32_t)A.sign);
-      if (count_total) tri_acc += c;
-    }
+    delta_item_run<PRED>(A, pv, A.split_items[q], cnt, tri_acc);
   }
 }
 
-// Grid-wide barrier of a resident grid, with a bounded wait: each CTA arrives once, then waits
-// until `expected` CTAs have arrived or the bound (spin_ns of device time, at most kSpinMaxIters
-// polls) runs out, in which case it reports kErrTimeout and the call returns false. The acquire
-// load makes the other CTAs' writes before their arrival visible to this CTA.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, const unsigned expected, const unsigned long long spin_ns,
-                                             unsigned* err) {
-  __shared__ int s_ok;
-  __syncwarp();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    atomicAdd(bar, 1u);
-    unsigned long long t0;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
-    int ok = 1;
-    for (unsigned it = 0;; ++it) {
-      unsigned v;
-      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
-      if (v >= expected) break;
-      unsigned long long t;
-      asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-      if (it >= kSpinMaxIters || t - t0 > spin_ns) {
-        atomicOr(err, kErrTimeout);
-        ok = 0;
-        break;
-      }
-      __nanosleep(64);
+// Wait (lane 0 of a warp) until queue slot q holds a published item of this launch: 1 when it
+// does, 0 when no item will come to slot q (every warp has finished the entry pass and q lies
+// beyond the items they queued, or q beyond the queue's capacity), -1 when the wait ran out
+// (spin_ns of device time, at most kSpinMaxIters polls; kErrTimeout is set). A producer publishes
+// each slot before it counts itself done, so once every warp is done a reserved slot is ready.
+__device__ __forceinline__ int wait_item(const DeltaArgs& A, const unsigned long long q, const unsigned epoch,
+                                         const unsigned total) {
+  if (q >= (unsigned long long)kDeltaItems) return 0;
+  unsigned long long t0;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  for (unsigned it = 0;; ++it) {
+    if (ld_acquire(A.item_tag + q) == epoch) return 1;
+    if (ld_acquire(A.entry_done) >= total && q >= ld_acquire64(A.split_cnt)) return 0;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (it >= kSpinMaxIters || t - t0 > A.spin_ns) {
+      atomicOr(A.err, kErrTimeout);
+      return -1;
     }
-    s_ok = ok;
+    __nanosleep(64);
   }
-  __syncthreads();
-  return s_ok != 0;
+}
+
+// The item pass of the persistent kernel: it starts as soon as the warp's own entry pass ends,
+// while other warps may still queue items. Slots are taken in order from the queue head; a slot
+// is read once its tag carries this launch's epoch (items written by other CTAs are read past
+// the non-coherent L1 after the acquire).
+template <int PRED>
+__device__ __forceinline__ void delta_items_stream(const DeltaArgs& A, uint32_t* __restrict__ pv,
+                                                   unsigned long long& tri_acc) {
+  const int lane = threadIdx.x & 31;
+  const unsigned epoch = *A.item_epoch;
+  const unsigned total = (unsigned)(((int64_t)gridDim.x * blockDim.x) >> 5) + A.bar_extra;
+  const int64_t cnt = (int64_t)__ldcg(A.count_dev);
+  for (;;) {
+    unsigned long long q = 0;
+    int state = 0;
+    if (lane == 0) {
+      q = atomicAdd(A.i_next, 1ull);
+      state = wait_item(A, q, epoch, total);
+    }
+    __syncwarp();
+    state = __shfl_sync(kFull, state, 0);
+    q = __shfl_sync(kFull, q, 0);
+    if (state != 1) break;
+    delta_item_run<PRED>(A, pv, __ldcg(A.split_items + q), cnt, tri_acc);
+  }
 }
 
 // Two launches: the entry pass, then the item pass (the cuStinger-style count, tc_count_batch).
@@ -1163,16 +1231,18 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta_split(const DeltaArgs A, 
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long tri_acc = 0;
-  delta_items<PRED, false>(A, pv, gw, nw, tri_acc);
+  delta_items<PRED>(A, pv, gw, nw, tri_acc);
   delta_flush(tri_acc, 0ull, tri_out, nullptr);
 }
 
-// One persistent launch (a resident grid, at most the occupancy limit of CTAs per SM): the
-// entry pass, a grid-wide barrier, then the item pass over the chunks every CTA queued. The
-// batch size is read from device memory, so one captured launch serves every batch of a bin. A
-// barrier wait that runs out (the grid was not resident, or a test forces it) sets kErrTimeout
-// and the CTA skips the item pass: the batch's count is then incomplete and the host reports
-// TC_ERR_TIMEOUT.
+// One persistent launch (a resident grid, at most the occupancy limit of CTAs per SM): every warp
+// runs its share of the entry pass, queueing the chunks of split intersections, counts itself
+// done, and then takes queued chunks until none is left: no grid-wide barrier, so warps whose
+// entry work ends early start on the chunks while others still queue them. The batch size is
+// read from device memory, so one captured launch serves every batch of a bin. The launch's
+// epoch (bumped before it) marks the slots published in this launch. A wait that runs out (the
+// grid was not resident, or a test forces it) sets kErrTimeout and the warp leaves the item
+// pass: the batch's count is then incomplete and the host reports TC_ERR_TIMEOUT.
 template <int PRED>
 __global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, uint32_t* __restrict__ pv,
                                                           unsigned long long* __restrict__ tri_out) {
@@ -1180,8 +1250,14 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, 
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   unsigned long long tri_acc = 0, bytes_acc = 0;
   delta_entries<PRED>(A, pv, gw, nw, tri_acc, bytes_acc);
-  if (grid_barrier(A.bar, gridDim.x + A.bar_extra, A.spin_ns, A.err))
-    delta_items<PRED, true>(A, pv, gw, nw, tri_acc);
+  // this warp's items are published: count it done (its lanes' releases before lane 0's add)
+  __threadfence();
+  __syncwarp();
+  if ((threadIdx.x & 31) == 0) {
+    __threadfence();
+    atomicAdd(A.entry_done, 1u);
+  }
+  delta_items_stream<PRED>(A, pv, tri_acc);
   delta_flush(tri_acc, bytes_acc, tri_out, A.bytes_out);
 }
 
@@ -1577,7 +1653,8 @@ __global__ void k_endpoints(const int4* __restrict__ dlist, const BatchStatus* _
   }
 }
 
-// The compaction epoch lives on the device so that a captured launch sequence advances it.
+// The compaction epoch and the delta kernel's item epoch live on the device so that a captured
+// launch sequence advances them.
 __global__ void k_bump_epoch(unsigned* __restrict__ epoch) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *epoch += 1u;
 }
@@ -1659,6 +1736,8 @@ struct StreamWs {
   int64_t* scan64 = nullptr;    // [n+1]
   int64_t* tiles = nullptr;
   unsigned long long* split_items = nullptr;  // [kDeltaItems] queued chunks of long intersections
+  unsigned* item_tag = nullptr;    // [kDeltaItems] launch epoch that published each item slot
+  unsigned* item_epoch = nullptr;  // [1] epoch of the current persistent delta launch
   // hub groups of the delta count (k_delta_hub)
   int32_t* hub_cnt = nullptr;     // [n] zero between phases
   long long* hub_sum = nullptr;   // [n] zero between phases
@@ -1682,7 +1761,7 @@ void StreamWs::release() {
   cudaFree(cmp_plan); cudaFree(long_chunk);
   cudaFree(ins_slot);
   cudaFree(vlist); cudaFree(claim); cudaFree(first_del); cudaFree(d_epoch); cudaFree(cub_tmp); cudaFree(st); cudaFreeHost(st_host); cudaFree(counter);
-  cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items);
+  cudaFree(cnt); cudaFree(scan64); cudaFree(tiles); cudaFree(split_items); cudaFree(item_tag); cudaFree(item_epoch);
   cudaFree(hub_cnt); cudaFree(hub_sum); cudaFree(hub_uni); cudaFree(hub_of); cudaFree(hub_list); cudaFree(hub_off);
   cudaFree(hub_len); cudaFree(hub_fill); cudaFree(hub_chunks); cudaFree(hub_units); cudaFree(hubbed);
   cudaFree(hub_items);
@@ -1749,17 +1828,25 @@ tc_status ensure_stream_ws(tc_graph* g, int64_t b) {
     TC_CUDA_TRY(cudaMemset(w.hub_of, 0, sizeof(int32_t) * n1));
     w.n_cap = g->n + 1;
   }
-  if (!w.st || !w.st_host || !w.counter || !w.split_items) {
-    cudaFree(w.st); cudaFreeHost(w.st_host); cudaFree(w.counter); cudaFree(w.split_items);
-    w.st = nullptr; w.st_host = nullptr; w.counter = nullptr; w.split_items = nullptr;
+  if (!w.st || !w.st_host || !w.counter || !w.split_items || !w.item_tag || !w.item_epoch) {
+    auto free_st = [&w]() {
+      cudaFree(w.st); cudaFreeHost(w.st_host); cudaFree(w.counter); cudaFree(w.split_items);
+      cudaFree(w.item_tag); cudaFree(w.item_epoch);
+      w.st = nullptr; w.st_host = nullptr; w.counter = nullptr; w.split_items = nullptr;
+      w.item_tag = nullptr; w.item_epoch = nullptr;
+    };
+    free_st();
     if (::tc::dev_malloc(&w.st, sizeof(BatchStatus)) != cudaSuccess ||
         cudaMallocHost(&w.st_host, sizeof(BatchStatus)) != cudaSuccess ||
         ::tc::dev_malloc(&w.counter, sizeof(unsigned long long)) != cudaSuccess ||
-        ::tc::dev_malloc(&w.split_items, sizeof(unsigned long long) * kDeltaItems) != cudaSuccess) {
-      cudaFree(w.st); cudaFreeHost(w.st_host); cudaFree(w.counter); cudaFree(w.split_items);
-      w.st = nullptr; w.st_host = nullptr; w.counter = nullptr; w.split_items = nullptr;
+        ::tc::dev_malloc(&w.split_items, sizeof(unsigned long long) * kDeltaItems) != cudaSuccess ||
+        ::tc::dev_malloc(&w.item_tag, sizeof(unsigned) * kDeltaItems) != cudaSuccess ||
+        ::tc::dev_malloc(&w.item_epoch, sizeof(unsigned)) != cudaSuccess) {
+      free_st();
       return fail(TC_ERR_OOM, "batch status: allocation failed");
     }
+    TC_CUDA_TRY(cudaMemset(w.item_tag, 0, sizeof(unsigned) * kDeltaItems));
+    TC_CUDA_TRY(cudaMemset(w.item_epoch, 0, sizeof(unsigned)));
     ++w.version;
   }
   if (b <= w.b_cap) return TC_OK;
@@ -2035,7 +2122,9 @@ tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, 
                              int ctas_per_sm, cudaStream_t s) {
   A.split_items = w.split_items;
   A.split_cnt = &w.st->n_split[phase];
-  A.bar = &w.st->bar[phase];
+  A.entry_done = &w.st->entry_done[phase];
+  A.item_tag = w.item_tag;
+  A.item_epoch = w.item_epoch;
   A.err = &w.st->err;
   A.bytes_out = &w.st->delta_bytes;
   A.e_next = &w.st->e_next[phase];
@@ -2043,6 +2132,7 @@ tc_status launch_delta_fused(DeltaArgs A, StreamWs& w, int phase, uint32_t* pv, 
   TC_TRY(launch_hub(A, w, phase, w.b_cap, pv, tri_out, s));
   int grid = 0;
   TC_TRY(fused_grid(ctas_per_sm, delta_smem(A), &grid));
+  k_bump_epoch<<<1, 32, 0, s>>>(w.item_epoch);  // marks the item slots this launch publishes
   k_delta_fused<kPredMark><<<grid, kThreads, delta_smem(A), s>>>(A, pv, tri_out);
   return TC_OK;
 }
@@ -2539,13 +2629,16 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     A.bar_extra = p->bar_extra;
     A.split_items = w.split_items;
     A.split_cnt = &w.st->n_split[0];
-    A.bar = &w.st->bar[0];
+    A.entry_done = &w.st->entry_done[0];
+    A.item_tag = w.item_tag;
+    A.item_epoch = w.item_epoch;
     A.err = &w.st->err;
     A.bytes_out = &w.st->delta_bytes;
     A.e_next = &w.st->e_next[0];
     A.i_next = &w.st->i_next[0];
     if (p->profile) cudaEventRecordWithFlags(p->pev[0], s, cudaEventRecordExternal);
     hub_kernels(A, w, 0, cap, ghub, pv, &w.st->tri_removed, s);
+    k_bump_epoch<<<1, 32, 0, s>>>(w.item_epoch);
     k_delta_fused<kPredMark><<<gdelta, kThreads, dsm, s>>>(A, pv, &w.st->tri_removed);
     if (p->profile) cudaEventRecordWithFlags(p->pev[1], s, cudaEventRecordExternal);
     k_endpoints<<<gb, kThreads, 0, s>>>(w.dlist, w.st, w.vlist);
@@ -2563,11 +2656,12 @@ tc_status pipe_capture(tc_pipeline* p, int bin, int cand, uint32_t* pv, int64_t*
     B.count_dev = &w.st->n_ins;
     B.sign = 1;
     B.split_cnt = &w.st->n_split[1];
-    B.bar = &w.st->bar[1];
+    B.entry_done = &w.st->entry_done[1];
     B.e_next = &w.st->e_next[1];
     B.i_next = &w.st->i_next[1];
     if (p->profile) cudaEventRecordWithFlags(p->pev[2], s, cudaEventRecordExternal);
     hub_kernels(B, w, 1, cap, ghub, pv, &w.st->tri_added, s);
+    k_bump_epoch<<<1, 32, 0, s>>>(w.item_epoch);
     k_delta_fused<kPredMark><<<gdelta, kThreads, dsm, s>>>(B, pv, &w.st->tri_added);
     if (p->profile) cudaEventRecordWithFlags(p->pev[3], s, cudaEventRecordExternal);
     k_clear_slots<<<g2, kThreads, 0, s>>>(w.ins_slot, 0, &w.st->n_ins, g->mark);

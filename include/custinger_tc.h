@@ -71,7 +71,9 @@ typedef struct tc_sched {
   uint8_t table[16][16];  /* strategy per cell [log2 d_a][log2 d_b]. Static count (a = the centre's
                              out-degree, b = the other endpoint's): 0 = the warp streams N+(b)
                              through the hash set, 1 = one lane walks it, 2 = packed (see
-                             packed_max_deg). Streaming: 0 = search, 1 = merge */
+                             packed_max_deg). Streaming: 0 = search, 1 = merge, 2 = stage (the
+                             longer list copied into shared memory in pieces with cp.async, each
+                             shorter-list entry binary-searched there) */
   int32_t shard;          /* multi-GPU work split (1 = everything): this call counts shard `shard` of */
   int32_t nshards;        /* `nshards`. Static count: a contiguous range of edge centres, the ranges
                              balanced by each centre's predicted intersection work (every rank
@@ -246,9 +248,10 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  * up to max_batch, until the autotuner merges bins); each bin's graph is captured on first use
  * with launches sized for the bin and reads the batch's counts on the device. The triangle
  * delta of each phase of a batch (deletions, insertions) is one persistent kernel over a
- * resident grid: the per-edge pass, a grid-wide barrier with a bounded wait, then the queued
- * chunks of hub-hub intersections. Pool headroom for the worst case of a batch (every list it
- * touches relocating) is reserved before each launch.
+ * resident grid: each warp runs its share of the per-edge pass, then takes the queued chunks of
+ * long intersections as other warps publish them (each wait for a chunk is bounded). Pool
+ * headroom for the worst case of a batch (every list it touches relocating) is reserved before
+ * each launch.
  *
  * tc_pipeline_create: for batches of at most max_batch updates on graph g (the graph must not be
  *                     updated through other calls while the pipeline has a batch in flight).
@@ -260,7 +263,7 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  * tc_pipeline_prepare: reserve pool headroom for max_batch and capture every bin's graph for these
  *                     outputs now (optional; otherwise both happen on first use).
  * tc_pipeline_sync:   wait for the last batch and report it (errors of that batch surface here;
- *                     TC_ERR_TIMEOUT when a delta kernel's barrier wait ran out).
+ *                     TC_ERR_TIMEOUT when a delta kernel's wait for queued work ran out).
  * tc_pipeline_autotune: explore over the next `batches` batches: each runs under one arm of its
  *                     natural bin, a candidate tile shape of the delta kernel (CTAs per SM: the
  *                     occupancy limit; split threshold / split-item size 2048/1024, 1024/512,
@@ -275,9 +278,9 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
  *                     (drops the graphs when it changes; call before tc_pipeline_prepare) and
  *                     count their algorithmic bytes, sum over changed edges {x,y} of
  *                     4 (deg x + deg y) + 8; tc_pipeline_stats returns the totals since.
- * tc_pipeline_set_wait_bound: the bound of the delta kernels' barrier wait (default 2 s) and a
- *                     number of arrivals it waits for beyond the grid (0 normally; a test gives 1
- *                     to make every wait run out and checks that the batch reports
+ * tc_pipeline_set_wait_bound: the bound of the delta kernels' wait for queued work (default 2 s)
+ *                     and a number of warps it waits for beyond the grid (0 normally; a test gives
+ *                     1 to make the waits run out and checks that the batch reports
  *                     TC_ERR_TIMEOUT with the device still usable). Drops the captured graphs. */
 typedef struct tc_pipeline tc_pipeline;
 typedef struct tc_pipeline_plan {

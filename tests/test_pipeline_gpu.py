@@ -178,10 +178,11 @@ def test_plan_carries_over_to_a_second_pipeline():
 
 
 def test_delta_kernel_wait_bound_reports_timeout_and_device_stays_usable():
-    """The persistent delta kernel's grid barrier has a bounded wait. Made to wait for an arrival
-    that never comes (one beyond the grid), every CTA gives up after the bound (1 ms here), the
-    batch reports TC_ERR_TIMEOUT, and the device keeps working: the structure update completed,
-    a recount runs, and later batches count right again with the normal bound."""
+    """The persistent delta kernel's wait for queued work is bounded. Made to wait for a warp
+    that never finishes its entry pass (one beyond the grid), the waiting warps give up after the
+    bound (1 ms here), the batch reports TC_ERR_TIMEOUT, and the device keeps working: the
+    structure update completed, a recount runs, and later batches count right again with the
+    normal bound."""
     torch = _torch()
     rng = np.random.default_rng(12)
     base = G.rmat(11, 16, seed=3)
