@@ -82,6 +82,9 @@ def parse(argv=None):
     ap.add_argument("--no-streaming", action="store_true")
     ap.add_argument("--no-stream-tune", action="store_true",
                     help="run the streaming pipeline with its default plan (no untimed autotuning first)")
+    ap.add_argument("--stream-plan", default=None,
+                    help="run the streaming pipeline on the plan (bins and tile shapes) recorded in an "
+                         "earlier bench line (a file holding that JSON line) instead of tuning one")
     ap.add_argument("--stream-scale", type=int, default=22)
     ap.add_argument("--stream-batches", type=int, default=200)
     ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
@@ -660,6 +663,23 @@ def streaming_batches(scale, nbatch, base, seed=4):
     return out
 
 
+def plan_from_bench(path):
+    """The pipeline plan recorded in an earlier bench line's streaming block (its bins)."""
+    from custingeralg_b200 import native as N
+    with open(path) as f:
+        bins = json.loads(f.read().strip().splitlines()[-1])["streaming"]["bins"]
+    plan = N.PipelinePlan()
+    plan.nbins = len(bins)
+    caps = [b["capacity"] for b in bins]
+    for i, b in enumerate(bins):
+        plan.bin_cap[i] = b["capacity"]
+        plan.serve[i] = caps.index(b["served_by_capacity"])
+        plan.ctas_per_sm[i] = b.get("plan_ctas_per_sm", 0)
+        plan.chunk[i] = b["chunk"]
+        plan.split_min[i] = b["split_min"]
+    return plan
+
+
 def tune_pipeline(base, max_b, sched, scale, dev, per_arm=2, small_per_arm=6, small_cap=4096, seed=104):
     """Autotune a pipeline on a twin of the base graph (untimed) and return its plan: for every
     bin of the ladder, batches of sizes inside that bin, two per arm of the tuner (five tile
@@ -726,7 +746,9 @@ def run_streaming(ctx, sched_kind, verify_every=None):
     if a.stream_path == "pipeline":
         max_b = max(s.numel() for s, _, _ in dbat)
         t_tune = time.perf_counter()
-        if not a.no_stream_tune:
+        if a.stream_plan:
+            plan = plan_from_bench(a.stream_plan)
+        elif not a.no_stream_tune:
             plan = tune_pipeline(base, max_b, sched, a.stream_scale, dev)
         tune_s = time.perf_counter() - t_tune
         pipe = api.Pipeline(graph, max_b, sched=sched)
@@ -784,11 +806,16 @@ def run_streaming(ctx, sched_kind, verify_every=None):
         res["path"] = ("tc_pipeline (one captured CUDA graph per batch-size bin; the delta count of each phase one "
                        "persistent kernel)")
         res["bins"] = [{"capacity": int(plan.bin_cap[i]), "served_by_capacity": int(plan.bin_cap[plan.serve[i]]),
-                        "delta_ctas_per_sm": bps, "split_min": int(plan.split_min[i]), "chunk": int(plan.chunk[i])}
+                        "delta_ctas_per_sm": bps, "plan_ctas_per_sm": int(plan.ctas_per_sm[i]),
+                        "split_min": int(plan.split_min[i]), "chunk": int(plan.chunk[i])}
                        for i, (_, bps) in enumerate(pipe.info())]
-        res["autotune"] = ("off: the pipeline's default plan" if a.no_stream_tune else
-                           f"on a twin of the base graph before the timed run ({tune_s:.1f} s, untimed): per bin, "
-                           "two batches per arm (tile shapes, and the next bin's graph)")
+        if a.stream_plan:
+            res["autotune"] = f"off: the plan recorded in {os.path.basename(a.stream_plan)}"
+        elif a.no_stream_tune:
+            res["autotune"] = "off: the pipeline's default plan"
+        else:
+            res["autotune"] = (f"on a twin of the base graph before the timed run ({tune_s:.1f} s, untimed): per "
+                               "bin, two batches per arm (tile shapes, and the next bin's graph)")
         res["delta_kernel_ms"] = round(st["delta_ms"], 3)
         if st["delta_ms"] > 0:
             ach = st["delta_bytes"] / (st["delta_ms"] / 1e3) / 1e9

@@ -5,7 +5,12 @@
   custingeralg_b200/libtcgen.so          seeded graph generators, graph file readers and the binary
                                          CSR cache (host C++/OpenMP)
 
-Usage: python -m custingeralg_b200.build [--force] [--verbose]
+Usage: python -m custingeralg_b200.build [--force] [--verbose] [--define NAME=VALUE ...]
+
+--define passes a preprocessor definition to every CUDA source: the kernels' tuning constants
+(TC_HUB_UNIT, TC_HUB_ITEM_LOG2, TC_HUB_THREADS, TC_DELTA_MIN_BLOCKS) take their defaults unless
+given, which is how their alternatives were measured. Use it with --force, and rebuild with
+--force and no --define to return to the defaults.
 """
 from __future__ import annotations
 
@@ -79,15 +84,17 @@ def build_gen(force=False, verbose=False):
     return LIB_GEN
 
 
-def build_all(force=False, verbose=False):
+def build_all(force=False, verbose=False, defines=()):
     build_gen(force, verbose)
-    build_tc(force, verbose)
+    build_tc(force, verbose, extra=[f"-D{d}" for d in defines])
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--define", action="append", default=[], metavar="NAME=VALUE",
+                    help="preprocessor definition for the CUDA sources (a tuning constant)")
     a = ap.parse_args()
-    build_all(a.force, a.verbose)
+    build_all(a.force, a.verbose, a.define)
     print("built", LIB_TC, LIB_GEN)

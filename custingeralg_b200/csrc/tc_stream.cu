@@ -306,30 +306,53 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
       }
     }
     const int32_t* A = pool + s_old;
-    // New entries first, while A is intact: final position j + #(old < B[j]) (relative).
+    // New entries first, while A is intact: final position j + #(old < B[j]) (relative). The
+    // first five levels of each search come from 32 evenly spaced samples of A held in the lanes.
     int32_t first_new = a;  // old entries below the smallest new entry keep their slots
-    for (int64_t j = i0 + lane; j < i1; j += 32) {
-      const int32_t val = (int32_t)(uint32_t)dk[j];
-      int32_t lo = 0, hi = a;
-      while (lo < hi) {
-        const int32_t mid = (lo + hi) >> 1;
-        if (A[mid] < val) lo = mid + 1;
-        else hi = mid;
+    {
+      const int32_t step = (a + 31) / 32;
+      const int32_t smp = lane * step < a ? A[lane * step] : INT32_MAX;
+      const int32_t s31 = __shfl_sync(kFull, smp, 31);
+      for (int64_t jb = i0; jb < i1; jb += 32) {
+        const int64_t j = jb + lane;
+        const bool act = j < i1;
+        const int32_t val = act ? (int32_t)(uint32_t)dk[j] : INT32_MAX;
+        int pos = 0;  // samples below val (they ascend with the lane)
+#pragma unroll
+        for (int st = 16; st > 0; st >>= 1)
+          if (__shfl_sync(kFull, smp, pos + st - 1) < val) pos += st;
+        if (pos == 31 && s31 < val) pos = 32;
+        int32_t lo = pos > 0 ? (pos - 1) * step + 1 : 0;
+        int32_t hi = pos < 32 ? min(pos * step, a) : a;
+        if (act) {
+          while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (A[mid] < val) lo = mid + 1;
+            else hi = mid;
+          }
+          slot[j] = (j - i0) + lo;
+          if (j == i0) first_new = lo;
+        }
+        __syncwarp();
       }
-      slot[j] = (j - i0) + lo;
-      if (j == i0) first_new = lo;
     }
     __syncwarp();
     // In place, old entries below the first new entry do not move; relocated, all of them do.
     const int32_t keep_below = moved ? 0 : __shfl_sync(kFull, first_new, 0);
     // Old entries: final position i + #(new < A[i]); backwards in chunks so that, in place, no
-    // unread entry is overwritten (targets never precede sources).
-    for (int32_t base = ((a - 1) / 32) * 32; base >= (keep_below / 32) * 32 && a > 0; base -= 32) {
+    // unread entry is overwritten (targets never precede sources). Each chunk's entries are read
+    // one chunk ahead: the writes of a chunk go to slots at or above its own.
+    const int32_t low = (keep_below / 32) * 32;
+    int32_t base = a > 0 ? ((a - 1) / 32) * 32 : -1;
+    int32_t ahead = (base >= low && base + lane < a && base + lane >= keep_below) ? A[base + lane] : 0;
+    for (; base >= low; base -= 32) {
       const int32_t i = base + lane;
-      int32_t val = 0;
+      const bool act = i < a && i >= keep_below;
+      const int32_t val = ahead;
+      const int32_t inext = i - 32;
+      ahead = (base - 32 >= low && inext >= keep_below) ? A[inext] : 0;
       int64_t pos = 0;
-      if (i < a && i >= keep_below) {
-        val = A[i];
+      if (act) {
         int64_t lo = i0, hi = i1;
         while (lo < hi) {
           const int64_t mid = (lo + hi) >> 1;
@@ -339,7 +362,7 @@ __global__ void k_insert_runs(const uint64_t* __restrict__ dk, const int64_t nd_
         pos = i + (lo - i0);
       }
       __syncwarp();
-      if (i < a && i >= keep_below) {
+      if (act) {
         pool[s_new + pos] = val;
         if (mark) mark[s_new + pos] = 0;
       }
@@ -531,6 +554,10 @@ __global__ void __launch_bounds__(kThreads) k_long_stage(
     const uint64_t* __restrict__ dk, const int32_t* __restrict__ pool, const LongPlan* __restrict__ plan,
     const unsigned long long* __restrict__ items, const int64_t item_cap, int32_t* __restrict__ scr,
     uint8_t* __restrict__ smark, int64_t* __restrict__ slot, const BatchStatus* __restrict__ st) {
+  // The new entries whose values fall inside the item's old entries, staged in shared memory,
+  // so that each old entry counts the new ones below it there instead of in global memory.
+  __shared__ int32_t s_run[kLongChunk];
+  __shared__ int32_t s_lo, s_n;
   const int64_t n_items = min((int64_t)st->long_items, item_cap);
   for (int64_t q = blockIdx.x; q < n_items; q += gridDim.x) {
     const unsigned long long item = items[q];
@@ -538,16 +565,57 @@ __global__ void __launch_bounds__(kThreads) k_long_stage(
     const LongPlan P = plan[item >> 32];
     const int32_t k0 = (int32_t)(uint32_t)item * kLongChunk, k1 = min(P.len, k0 + kLongChunk);
     const int32_t suffix = P.a - P.first;
+    const int32_t ko1 = min(k1, suffix);  // the item's old entries: [k0, ko1)
+    int32_t run_lo = 0, run_n = -1;       // run_n < 0: not staged
+    if (k0 < ko1) {
+      if (threadIdx.x == 0) {
+        // new entries below the item's first old value, and below its last: the ones between
+        // are the only ones that tell its old entries apart
+        const int32_t v0 = pool[P.s_old + P.first + k0], v1 = pool[P.s_old + P.first + ko1 - 1];
+        int32_t lo = 0, hi = P.c;
+        while (lo < hi) {
+          const int32_t mid = (lo + hi) >> 1;
+          if ((int32_t)(uint32_t)dk[P.i0 + mid] < v0) lo = mid + 1;
+          else hi = mid;
+        }
+        int32_t lo2 = lo, hi2 = P.c;
+        while (lo2 < hi2) {
+          const int32_t mid = (lo2 + hi2) >> 1;
+          if ((int32_t)(uint32_t)dk[P.i0 + mid] < v1) lo2 = mid + 1;
+          else hi2 = mid;
+        }
+        s_lo = lo;
+        s_n = lo2 - lo;
+      }
+      __syncthreads();
+      run_lo = s_lo;
+      run_n = s_n <= kLongChunk ? s_n : -1;
+      for (int32_t t = threadIdx.x; t < run_n; t += kThreads) s_run[t] = (int32_t)(uint32_t)dk[P.i0 + run_lo + t];
+      __syncthreads();
+    }
     for (int32_t k = k0 + (int32_t)threadIdx.x; k < k1; k += kThreads) {
       int32_t val, pos;
       uint8_t mk;
       if (k < suffix) {  // an old entry: shifts by the new entries below it
         val = pool[P.s_old + P.first + k];
-        int32_t lo = 0, hi = P.c;
-        while (lo < hi) {
-          const int32_t mid = (lo + hi) >> 1;
-          if ((int32_t)(uint32_t)dk[P.i0 + mid] < val) lo = mid + 1;
-          else hi = mid;
+        int32_t lo, hi;
+        if (run_n >= 0) {
+          lo = 0;
+          hi = run_n;
+          while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if (s_run[mid] < val) lo = mid + 1;
+            else hi = mid;
+          }
+          lo += run_lo;
+        } else {
+          lo = 0;
+          hi = P.c;
+          while (lo < hi) {
+            const int32_t mid = (lo + hi) >> 1;
+            if ((int32_t)(uint32_t)dk[P.i0 + mid] < val) lo = mid + 1;
+            else hi = mid;
+          }
         }
         pos = k + lo;
         mk = 0;
@@ -561,6 +629,7 @@ __global__ void __launch_bounds__(kThreads) k_long_stage(
       scr[P.soff + pos] = val;
       smark[P.soff + pos] = mk;
     }
+    __syncthreads();  // the next item restages s_run
   }
 }
 
@@ -1244,7 +1313,10 @@ __global__ void __launch_bounds__(kThreads, 6) k_delta_split(const DeltaArgs A, 
 // grid was not resident, or a test forces it) sets kErrTimeout and the warp leaves the item
 // pass: the batch's count is then incomplete and the host reports TC_ERR_TIMEOUT.
 template <int PRED>
-__global__ void __launch_bounds__(kThreads, 6) k_delta_fused(const DeltaArgs A, uint32_t* __restrict__ pv,
+#ifndef TC_DELTA_MIN_BLOCKS
+#define TC_DELTA_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kThreads, TC_DELTA_MIN_BLOCKS) k_delta_fused(const DeltaArgs A, uint32_t* __restrict__ pv,
                                                           unsigned long long* __restrict__ tri_out) {
   const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -1300,7 +1372,10 @@ constexpr int kHubUnit = TC_HUB_UNIT;
 constexpr int kHubPass = 2 * kHubBucketsMax;  // entries of N(h) per pass (load <= 0.5)
 constexpr int32_t kHubMarkBit = INT32_MIN;    // bit 31 of a stored key: the edge (h, key) is changed
 constexpr int64_t kHubSearchCost = 64;        // an item's estimate of one range search, in probes
-constexpr int64_t kHubItemMin = 1 << 16;      // probes of work per item at least ...
+#ifndef TC_HUB_ITEM_LOG2
+#define TC_HUB_ITEM_LOG2 17
+#endif
+constexpr int64_t kHubItemMin = 1ll << TC_HUB_ITEM_LOG2;  // probes of work per item at least ...
 constexpr int64_t kHubBuildShare = 16;        // ... and at least this many times its table build
 constexpr int64_t kHubItemsPerUpdate = 4;     // item queue capacity per batch update
 constexpr int64_t kHubUnitsPerUpdate = kHubUnit >= 1024 ? 4 : 4 * 1024 / kHubUnit;  // unit slots per update

@@ -97,3 +97,24 @@ def test_ranks_share_one_generated_graph():
     got = dict(q.get(timeout=5) for _ in procs)
     assert got == {0: True, 1: True, 2: True}
     assert not os.path.exists(os.path.join(tempfile.gettempdir(), f"tc_bench_{port}_rmat11_16_3.tccsr"))
+
+
+def test_stream_plan_round_trips_through_a_bench_line(tmp_path):
+    """--stream-plan reads the bins a bench line recorded back into the pipeline plan they came
+    from: capacities, the bin serving each one and its tile shape."""
+    bins = [{"capacity": 1024, "served_by_capacity": 4096, "delta_ctas_per_sm": 6, "plan_ctas_per_sm": 0,
+             "split_min": 128, "chunk": 64},
+            {"capacity": 2048, "served_by_capacity": 4096, "delta_ctas_per_sm": 6, "plan_ctas_per_sm": 0,
+             "split_min": 128, "chunk": 64},
+            {"capacity": 4096, "served_by_capacity": 4096, "delta_ctas_per_sm": 6, "plan_ctas_per_sm": 0,
+             "split_min": 256, "chunk": 128},
+            {"capacity": 8192, "served_by_capacity": 8192, "delta_ctas_per_sm": 6,
+             "split_min": 512, "chunk": 256}]
+    path = tmp_path / "line.json"
+    path.write_text("noise before the line\n" + __import__("json").dumps({"streaming": {"bins": bins}}) + "\n")
+    p = bench.plan_from_bench(str(path))
+    assert p.nbins == 4
+    assert list(p.bin_cap)[:4] == [1024, 2048, 4096, 8192]
+    assert list(p.serve)[:4] == [2, 2, 2, 3]
+    assert list(p.split_min)[:4] == [128, 128, 256, 512] and list(p.chunk)[:4] == [64, 64, 128, 256]
+    assert list(p.ctas_per_sm)[:4] == [0, 0, 0, 0]
