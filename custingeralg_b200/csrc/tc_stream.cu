@@ -37,8 +37,8 @@ constexpr int kDeltaChunk = 1024;   // ... into items of this many entries of th
 constexpr int64_t kDeltaItems = 1 << 20;  // capacity of the split-item queue
 constexpr unsigned long long kNoItem = ~0ull;
 constexpr int kGrab = 4;  // changed edges a warp takes per grab from the delta kernel's queue
-// Bounded wait of the persistent delta kernel's grid barrier (a wait that runs out reports
-// kErrTimeout and the kernel skips the work after the barrier).
+// Bound of the persistent delta kernel's waits for queued split items (a wait that runs out
+// reports kErrTimeout and the warp leaves the item pass).
 constexpr unsigned long long kSpinNs = 2000000000ull;  // 2 s
 constexpr unsigned kSpinMaxIters = 1u << 24;
 
@@ -2110,7 +2110,7 @@ void long_insert(tc_graph* g, StreamWs& w, int64_t nd_cap, uint8_t* mark, cudaSt
 }
 
 // Grid of the persistent delta kernel: ctas_per_sm CTAs per SM (0 = the occupancy limit), never
-// more than can be resident at once (its grid barrier needs every CTA running).
+// more than can be resident at once (its item pass waits for every warp's entry pass).
 tc_status fused_grid(int ctas_per_sm, size_t smem, int* grid) {
   constexpr int kMaxDev = 64;
   static int occ[kMaxDev][2] = {};  // without, with the staging buffers
@@ -2324,7 +2324,7 @@ tc_status tc_apply_batch(tc_graph* g, const int32_t* src, const int32_t* dst, co
     TC_CUDA_TRY(cudaStreamSynchronize(s));
     const BatchStatus& f = *w.st_host;
     if (f.err & (kErrPool | kErrScratch)) return fail(TC_ERR_CAPACITY, "adjacency pool or insertion scratch exhausted");
-    if (f.err & kErrTimeout) return fail(TC_ERR_TIMEOUT, "the delta kernel's grid barrier gave up waiting");
+    if (f.err & kErrTimeout) return fail(TC_ERR_TIMEOUT, "the delta kernel gave up waiting for queued work");
     info->updates = b;
     info->inserted = (int64_t)f.n_ins;
     info->deleted = (int64_t)f.n_del;
@@ -2631,7 +2631,7 @@ tc_status pipe_settle(tc_pipeline* p) {
   }
   if (f.err & kErrTimeout) {
     p->last.status = TC_ERR_TIMEOUT;
-    return fail(TC_ERR_TIMEOUT, "the delta kernel's grid barrier gave up waiting; the batch's count is incomplete");
+    return fail(TC_ERR_TIMEOUT, "the delta kernel gave up waiting for queued work; the batch's count is incomplete");
   }
   return TC_OK;
 }
