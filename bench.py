@@ -85,6 +85,9 @@ def parse(argv=None):
     ap.add_argument("--stream-plan", default=None,
                     help="run the streaming pipeline on the plan (bins and tile shapes) recorded in an "
                          "earlier bench line (a file holding that JSON line) instead of tuning one")
+    ap.add_argument("--stream-hub-min", type=int, default=None,
+                    help="changed edges an endpoint must hold to be counted as a hub (the scheduler's "
+                         "stream_hub_min; default: the library's)")
     ap.add_argument("--stream-scale", type=int, default=22)
     ap.add_argument("--stream-batches", type=int, default=200)
     ap.add_argument("--stream-verify", type=int, default=1, help="recount after every k-th batch (0 = never)")
@@ -742,6 +745,8 @@ def run_streaming(ctx, sched_kind, verify_every=None):
             sched = L.learned_stream_sched(L.load(L.STREAM_WEIGHTS))
             sched_desc = "learned (custingeralg_b200/data/sched_mlp_stream.bin, nominal cell degrees)"
     sched.shard, sched.nshards = ctx.rank, ctx.world
+    if a.stream_hub_min is not None:
+        sched.stream_hub_min = a.stream_hub_min
     pipe, plan, tune_s = None, None, 0.0
     if a.stream_path == "pipeline":
         max_b = max(s.numel() for s, _, _ in dbat)
@@ -794,7 +799,7 @@ def run_streaming(ctx, sched_kind, verify_every=None):
     final = int(ctx.allreduce_(delta.clone()).item()) + T0
     res = {"value": updates / (total_ms / 1e3), "unit": "update edges/s", "batches": len(dbat),
            "updates": updates, "effective": eff if pipe is not None else None, "ms_total": total_ms,
-           "recount_checks": checked, "scheduler": sched_desc,
+           "recount_checks": checked, "scheduler": sched_desc, "hub_min": int(sched.stream_hub_min),
            "workload": f"R-MAT scale {a.stream_scale} ef 16 seed 4 base (slack 0.25), {len(dbat)} batches of "
                        "log-uniform size in [1, 2^20], 70% R-MAT insertions / 30% deletions of distinct present "
                        "edges; timed per batch over sort + classify + structure update + delta count, batches "
