@@ -1736,6 +1736,19 @@ __global__ void k_bump_epoch(unsigned* __restrict__ epoch) {
 
 // Canonical keys of a padded batch: entries [b, cap) (b read on the device) become sentinels,
 // so a launch sequence sized for cap serves every batch of at most cap updates.
+// A device batch into the pipeline's capacity-sized buffers, and its size where the captured
+// graph reads it: one launch in place of three copies and a host-to-device copy of the size.
+__global__ void k_load_batch(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                             const uint8_t* __restrict__ isdel, const int64_t b, int32_t* __restrict__ wsrc,
+                             int32_t* __restrict__ wdst, uint8_t* __restrict__ wdel, int64_t* __restrict__ d_b) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b; i += (int64_t)gridDim.x * blockDim.x) {
+    wsrc[i] = src[i];
+    wdst[i] = dst[i];
+    wdel[i] = isdel ? isdel[i] : (uint8_t)0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_b = b;
+}
+
 __global__ void k_make_keys_cap(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
                                 const uint8_t* __restrict__ is_del, const int64_t* __restrict__ b_dev,
                                 const int64_t cap, const int32_t n, const int L, uint64_t* __restrict__ keys,
@@ -2493,8 +2506,9 @@ tc_status tc_count_batch(tc_graph* g, const int32_t* d_src, const int32_t* d_dst
 // synchronisation) and sizes each launch from them. The pipeline below runs the same steps as
 // one CUDA graph per batch-size bin instead: every launch is sized for the bin's capacity and
 // reads the batch's real counts from device memory (grid-stride loops over device counts, the
-// batch padded with sentinel keys), so a batch is a few copies and one graph launch with no
-// host synchronisation inside. The delta count of each phase (deletions, insertions) is one
+// batch padded with sentinel keys), so a batch is one small launch that loads it and its size
+// into the bin's buffers (k_load_batch) and one graph launch, with no host synchronisation
+// inside. The delta count of each phase (deletions, insertions) is one
 // persistent kernel (k_delta_fused). The pool headroom the relocations of one batch can take is
 // bounded ahead (every touched list moving: (m + 2b)(1 + slack) slots) and reserved before the
 // launch, so the device bump allocator cannot run out. The graphs capture the graph's pool and
@@ -2553,7 +2567,6 @@ struct tc_pipeline {
   unsigned bar_extra = 0;                            // (test hook: arrivals that never come)
   cudaStream_t cs = nullptr;     // capture stream
   int64_t* d_b = nullptr;
-  int64_t* h_b = nullptr;        // pinned
   tc::BatchStatus* h_st = nullptr;          // pinned: status of the last batch
   unsigned long long* h_top = nullptr;      // pinned: pool bump pointer after it
   uint32_t* pv_scratch = nullptr;
@@ -2828,7 +2841,6 @@ tc_status tc_pipeline_create(tc_graph* g, int64_t max_batch, const tc_sched* sch
     if ((rc = ensure_stream_ws(g, p->b_max)) != TC_OK) break;
     if (cudaStreamCreateWithFlags(&p->cs, cudaStreamNonBlocking) != cudaSuccess ||
         ::tc::dev_malloc(&p->d_b, sizeof(int64_t)) != cudaSuccess ||
-        cudaMallocHost(&p->h_b, sizeof(int64_t)) != cudaSuccess ||
         cudaMallocHost(&p->h_st, sizeof(BatchStatus)) != cudaSuccess ||
         cudaMallocHost(&p->h_top, sizeof(unsigned long long)) != cudaSuccess ||
         ::tc::dev_malloc(&p->pv_scratch, sizeof(uint32_t) * ((size_t)g->n + 1)) != cudaSuccess ||
@@ -2858,7 +2870,6 @@ tc_status tc_pipeline_destroy(tc_pipeline* p) {
   drop_graphs(p);
   if (p->cs) cudaStreamDestroy(p->cs);
   cudaFree(p->d_b);
-  cudaFreeHost(p->h_b);
   cudaFreeHost(p->h_st);
   cudaFreeHost(p->h_top);
   cudaFree(p->pv_scratch);
@@ -2909,13 +2920,10 @@ tc_status tc_pipeline_apply(tc_pipeline* p, const int32_t* d_src, const int32_t*
     cand = arm < kPipeCands ? arm : 0;
   }
   if (!p->exec[bin][cand]) TC_TRY(pipe_capture(p, bin, cand, pv, delta));
-  // the batch into the capacity-sized buffers the graph reads
-  TC_CUDA_TRY(cudaMemcpyAsync(w.src, d_src, sizeof(int32_t) * b, cudaMemcpyDeviceToDevice, s));
-  TC_CUDA_TRY(cudaMemcpyAsync(w.dst, d_dst, sizeof(int32_t) * b, cudaMemcpyDeviceToDevice, s));
-  if (d_is_delete) TC_CUDA_TRY(cudaMemcpyAsync(w.isdel, d_is_delete, b, cudaMemcpyDeviceToDevice, s));
-  else TC_CUDA_TRY(cudaMemsetAsync(w.isdel, 0, b, s));
-  *p->h_b = b;
-  TC_CUDA_TRY(cudaMemcpyAsync(p->d_b, p->h_b, sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  // the batch into the capacity-sized buffers the graph reads, and its size
+  k_load_batch<<<grid_for(b, kThreads), kThreads, 0, s>>>(d_src, d_dst, d_is_delete, b, w.src, w.dst, w.isdel,
+                                                         p->d_b);
+  TC_CUDA_TRY(cudaGetLastError());
   p->timing = arm >= 0;
   if (p->timing) TC_CUDA_TRY(cudaEventRecord(p->t0, s));
   TC_CUDA_TRY(cudaGraphLaunch(p->exec[bin][cand], s));
